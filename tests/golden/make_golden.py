@@ -1,0 +1,91 @@
+"""Extract the bempp-cl golden matrices that pin bempp-rs's boundary assembly.
+
+Source: tests/compare_to_bempp_cl.rs of bempp-rs (the eight active tests at lines
+19-206).  Every test assembles on ``regular_sphere(0)`` (the unit octahedron, 8 cells,
+6 vertices) with default options (37-point regular rule, order-4 Duffy rules) and
+compares entry (i, j) of bempp-rs's matrix with ``from_cl[perm[i]][perm[j]]`` (perm is
+the identity for DP0) within an absolute ``epsilon``.
+
+Run in a checkout that has the reference at REFERENCE (default /root/reference):
+
+    python tests/golden/make_golden.py
+
+It writes tests/golden/bempp_cl_octahedron.json.  The fixture is committed; the tests
+never read the reference tree.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+import re
+import sys
+
+REFERENCE = os.environ.get("REFERENCE", "/root/reference")
+SRC = os.path.join(REFERENCE, "tests", "compare_to_bempp_cl.rs")
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "bempp_cl_octahedron.json")
+
+# test name -> (kernel, operator, space degree, continuous)
+TESTS = {
+    "test_laplace_single_layer_dp0_dp0": ("laplace", "single_layer", 0, False),
+    "test_laplace_double_layer_dp0_dp0": ("laplace", "double_layer", 0, False),
+    "test_laplace_adjoint_double_layer_dp0_dp0": ("laplace", "adjoint_double_layer", 0, False),
+    "test_laplace_hypersingular_p1_p1": ("laplace", "hypersingular", 1, True),
+    "test_helmholtz_single_layer_dp0_dp0": ("helmholtz", "single_layer", 0, False),
+    "test_helmholtz_double_layer_dp0_dp0": ("helmholtz", "double_layer", 0, False),
+    "test_helmholtz_adjoint_double_layer_dp0_dp0": ("helmholtz", "adjoint_double_layer", 0, False),
+    "test_helmholtz_hypersingular_p1_p1": ("helmholtz", "hypersingular", 1, True),
+}
+
+
+def parse_matrix(text: str):
+    text = text.strip()
+    assert text.startswith("[[") and text.endswith("]]"), text[:40]
+    rows = []
+    for row in re.findall(r"\[([^\[\]]*)\]", text[1:-1]):
+        if "c64::new" in row:
+            vals = re.findall(r"c64::new\(\s*([-+0-9.eE]+)\s*,\s*([-+0-9.eE]+)\s*\)", row)
+            rows.append([[float(a), float(b)] for a, b in vals])
+        else:
+            rows.append([float(v) for v in row.split(",") if v.strip()])
+    return rows
+
+
+def main():
+    src = open(SRC).read()
+    # only the active (non-commented) tests
+    active = "\n".join(line for line in src.splitlines() if not line.lstrip().startswith("//"))
+    out = {"source": "bempp-rs tests/compare_to_bempp_cl.rs", "cases": []}
+    for m in re.finditer(r"fn (test_\w+)\(\)\s*\{(.*?)\n\}", active, re.S):
+        name, body = m.group(1), m.group(2)
+        if name not in TESTS:
+            continue
+        kernel, op, degree, cont = TESTS[name]
+        mat = parse_matrix(re.search(r"let from_cl = (\[\[.*?\]\]);", body, re.S).group(1))
+        eps = float(re.search(r"epsilon = ([0-9.eE-]+)", body).group(1))
+        perm_m = re.search(r"let perm = \[([0-9, ]+)\];", body)
+        perm = [int(x) for x in perm_m.group(1).split(",")] if perm_m else list(range(len(mat)))
+        k_m = re.search(r"helmholtz::assembler::\w+\(([0-9.]+),", body)
+        line = src[: src.index("fn " + name + "()")].count("\n") + 1
+        out["cases"].append(
+            {
+                "name": name,
+                "line": line,
+                "kernel": kernel,
+                "operator": op,
+                "degree": degree,
+                "continuous": cont,
+                "wavenumber": float(k_m.group(1)) if k_m else None,
+                "epsilon": eps,
+                "perm": perm,
+                "matrix": mat,
+            }
+        )
+    assert len(out["cases"]) == len(TESTS), [c["name"] for c in out["cases"]]
+    with open(OUT, "w") as f:
+        json.dump(out, f, indent=1)
+    print(f"wrote {len(out['cases'])} cases to {OUT}")
+
+
+if __name__ == "__main__":
+    sys.exit(main())
