@@ -1,0 +1,279 @@
+"""Boundary assembly.
+
+Mirrors python/bempp/assembly/boundary.py of bempp-rs: ``BoundaryAssemblerOptions``,
+``BoundaryAssembler.assemble`` (dense, Fortran order), ``assemble_singular`` (SciPy
+CSR) and ``create_laplace_assembler`` keep their names, arguments and errors.
+Additions: ``create_helmholtz_assembler`` (the C function exists in the reference,
+src/bindings/boundary_assemblers.rs:168-210, but had no Python wrapper),
+``set_precision`` (FP64 or mixed FP32/FP64 regular quadrature), ``assemble_into_device``
+(a device buffer, e.g. a torch CUDA tensor, filled on a CUDA stream), and phase timing.
+"""
+
+from __future__ import annotations
+
+import typing
+from enum import Enum
+
+import numpy as np
+import numpy.typing as npt
+from scipy.sparse import csr_matrix
+
+from bempp._lib import check as _check
+from bempp._lib import ffi as _ffi
+from bempp._lib import last_error as _last_error
+from bempp._lib import lib as _lib
+from bempp.function_space import FunctionSpace
+from ndelement.reference_cell import ReferenceCellType
+
+_rtypes = {
+    np.float32: _lib.DType_F32,
+    np.float64: _lib.DType_F64,
+    np.complex64: _lib.DType_C32,
+    np.complex128: _lib.DType_C64,
+}
+_dtypes = {j: i for i, j in _rtypes.items()}
+_real = {np.float32: np.float32, np.float64: np.float64, np.complex64: np.float32,
+         np.complex128: np.float64}
+
+
+def _convert_to_scipy(rs_sparse_mat, dtype: typing.Type[np.floating]) -> csr_matrix:
+    """Convert a library CSR matrix to a SciPy CSR matrix (and free it)."""
+    if rs_sparse_mat == _ffi.NULL:
+        raise RuntimeError(_last_error())
+    shape = (_lib.matrix_shape0(rs_sparse_mat), _lib.matrix_shape1(rs_sparse_mat))
+    data = np.empty(_lib.matrix_csr_data_size(rs_sparse_mat), dtype=dtype)
+    indices = np.empty(_lib.matrix_csr_indices_size(rs_sparse_mat), dtype=np.uintp)
+    indptr = np.empty(_lib.matrix_csr_indptr_size(rs_sparse_mat), dtype=np.uintp)
+    _lib.matrix_csr_data_copy(rs_sparse_mat, _ffi.cast("void*", data.ctypes.data))
+    _lib.matrix_csr_indices_copy(rs_sparse_mat, _ffi.cast("uintptr_t*", indices.ctypes.data))
+    _lib.matrix_csr_indptr_copy(rs_sparse_mat, _ffi.cast("uintptr_t*", indptr.ctypes.data))
+    _lib.matrix_t_free(rs_sparse_mat)
+    return csr_matrix((data, indices, indptr), shape=shape)
+
+
+class OperatorType(Enum):
+    """Operator type."""
+
+    SingleLayer = _lib.OperatorType_SingleLayer
+    DoubleLayer = _lib.OperatorType_DoubleLayer
+    AdjointDoubleLayer = _lib.OperatorType_AdjointDoubleLayer
+    Hypersingular = _lib.OperatorType_Hypersingular
+    ElectricField = _lib.OperatorType_ElectricField
+    MagneticField = _lib.OperatorType_MagneticField
+
+
+class Precision(Enum):
+    """Arithmetic of the regular far-pair quadrature (addition)."""
+
+    FP64 = _lib.Precision_FP64
+    Mixed = _lib.Precision_Mixed
+
+
+class BoundaryAssemblerOptions(object):
+    """Boundary assembler options."""
+
+    def __init__(self):
+        self._read_only = False
+        self._rs_options = _lib.boundary_assembler_options_new()
+
+    def __del__(self):
+        if getattr(self, "_rs_options", None) is not None:
+            _lib.boundary_assembler_options_t_free(self._rs_options)
+            self._rs_options = None
+
+    def set_regular_quadrature_degree(self, cell: ReferenceCellType, degree: int):
+        """Set the (non-singular) quadrature degree for a cell type."""
+        if self._read_only:
+            raise ValueError("Cannot edit options already being used by an assembler")
+        if not _lib.boundary_assembler_options_has_regular_quadrature_degree(
+            self._rs_options, cell.value
+        ):
+            raise ValueError(f"Invalid cell type: {cell}")
+        _lib.boundary_assembler_options_set_regular_quadrature_degree(
+            self._rs_options, cell.value, degree
+        )
+
+    def regular_quadrature_degree(self, cell: ReferenceCellType) -> int:
+        """Get the (non-singular) quadrature degree for a cell type."""
+        if not _lib.boundary_assembler_options_has_regular_quadrature_degree(
+            self._rs_options, cell.value
+        ):
+            raise ValueError(f"Invalid cell type: {cell}")
+        return _lib.boundary_assembler_options_get_regular_quadrature_degree(
+            self._rs_options, cell.value
+        )
+
+    def set_singular_quadrature_degree(
+        self, cell0: ReferenceCellType, cell1: ReferenceCellType, degree: int
+    ):
+        """Set the singular quadrature degree for a cell type."""
+        if self._read_only:
+            raise ValueError("Cannot edit options already being used by an assembler")
+        if not _lib.boundary_assembler_options_has_singular_quadrature_degree(
+            self._rs_options, cell0.value, cell1.value
+        ):
+            raise ValueError(f"Invalid cell pair: {cell0} and {cell1}")
+        _lib.boundary_assembler_options_set_singular_quadrature_degree(
+            self._rs_options, cell0.value, cell1.value, degree
+        )
+
+    def singular_quadrature_degree(self, cell0: ReferenceCellType, cell1: ReferenceCellType) -> int:
+        """Get the singular quadrature degree for a cell type."""
+        if not _lib.boundary_assembler_options_has_singular_quadrature_degree(
+            self._rs_options, cell0.value, cell1.value
+        ):
+            raise ValueError(f"Invalid cell pair: {cell0} and {cell1}")
+        return _lib.boundary_assembler_options_get_singular_quadrature_degree(
+            self._rs_options, cell0.value, cell1.value
+        )
+
+    def set_batch_size(self, batch_size: int):
+        """Set the batch size."""
+        if self._read_only:
+            raise ValueError("Cannot edit options already being used by an assembler")
+        _lib.boundary_assembler_options_set_batch_size(self._rs_options, batch_size)
+
+    def batch_size(self) -> int:
+        """Get the batch size."""
+        return _lib.boundary_assembler_options_get_batch_size(self._rs_options)
+
+    def set_precision(self, precision: Precision):
+        """Set the arithmetic of the regular far-pair quadrature (addition)."""
+        if self._read_only:
+            raise ValueError("Cannot edit options already being used by an assembler")
+        _lib.boundary_assembler_options_set_precision(self._rs_options, precision.value)
+
+    def precision(self) -> Precision:
+        """Arithmetic of the regular far-pair quadrature."""
+        return Precision(_lib.boundary_assembler_options_get_precision(self._rs_options))
+
+
+class BoundaryAssembler(object):
+    """Boundary assembler."""
+
+    def __init__(self, options: BoundaryAssemblerOptions, rs_assembler, owned: bool = True):
+        """Initialise."""
+        if rs_assembler == _ffi.NULL:
+            raise ValueError(_last_error())
+        self.options = options
+        self.options._read_only = True
+        self._rs_assembler = rs_assembler
+        self._owned = owned
+
+    def __del__(self):
+        """Delete."""
+        if getattr(self, "_owned", False):
+            _lib.boundary_assembler_t_free(self._rs_assembler)
+
+    def _check_spaces(self, trial_space: FunctionSpace, test_space: FunctionSpace):
+        ok = (trial_space.dtype, test_space.dtype)
+        allowed = (self.dtype, _real[self.dtype])
+        assert ok[0] in allowed and ok[1] in allowed, "space and assembler dtypes differ"
+
+    def assemble(
+        self, trial_space: FunctionSpace, test_space: FunctionSpace
+    ) -> npt.NDArray[np.floating]:
+        """Assemble operator into a dense matrix."""
+        self._check_spaces(trial_space, test_space)
+        output = np.zeros(
+            (test_space.global_size, trial_space.global_size), dtype=self.dtype, order="F"
+        )
+        _check(
+            _lib.boundary_assembler_assemble_into_memory_ex(
+                self._rs_assembler,
+                trial_space._rs_space,
+                test_space._rs_space,
+                _ffi.cast("void*", output.ctypes.data),
+            ),
+            "assemble",
+        )
+        return output
+
+    def assemble_into_device(self, trial_space: FunctionSpace, test_space: FunctionSpace,
+                             out, stream=None):
+        """Assemble into a device buffer (addition).
+
+        ``out`` is a CUDA tensor (or any object with ``data_ptr()``) holding
+        test.global_size x trial.global_size elements of the assembler's dtype in
+        column-major order (a torch tensor of shape (n_trial, n_test), or the transpose
+        view of an (n_test, n_trial) tensor with Fortran strides).  ``stream`` is a
+        cudaStream_t as an int (e.g. ``torch.cuda.current_stream().cuda_stream``);
+        None uses the legacy default stream.  Returns once the work is enqueued.
+        """
+        self._check_spaces(trial_space, test_space)
+        ptr = out.data_ptr() if hasattr(out, "data_ptr") else int(out)
+        _check(
+            _lib.boundary_assembler_assemble_into_device(
+                self._rs_assembler, trial_space._rs_space, test_space._rs_space,
+                _ffi.cast("void*", ptr), _ffi.cast("void*", int(stream or 0))),
+            "assemble_into_device",
+        )
+
+    def assemble_singular(
+        self, trial_space: FunctionSpace, test_space: FunctionSpace
+    ) -> csr_matrix:
+        """Assemble the singular part of an operator into a CSR matrix."""
+        self._check_spaces(trial_space, test_space)
+        return _convert_to_scipy(
+            _lib.boundary_assembler_assemble_singular(
+                self._rs_assembler,
+                trial_space._rs_space,
+                test_space._rs_space,
+            ),
+            self.dtype,
+        )
+
+    def set_timing(self, enabled: bool = True):
+        """Record CUDA events around the geometry, regular and singular phases."""
+        _lib.boundary_assembler_set_timing(self._rs_assembler, enabled)
+
+    def phase_times(self) -> typing.List[float]:
+        """Milliseconds of the phases of the last timed assembly."""
+        buf = np.zeros(8, dtype=np.float64)
+        n = _lib.boundary_assembler_phase_times(
+            self._rs_assembler, _ffi.cast("double*", buf.ctypes.data), 8)
+        return [float(x) for x in buf[:n]]
+
+    def launch_count(self) -> int:
+        """Kernel launches enqueued by the last assembly."""
+        return _lib.boundary_assembler_last_launch_count(self._rs_assembler)
+
+    @property
+    def dtype(self):
+        """Data type."""
+        return _dtypes[_lib.boundary_assembler_dtype(self._rs_assembler)]
+
+
+def create_laplace_assembler(
+    operator_type: OperatorType,
+    options: typing.Optional[BoundaryAssemblerOptions] = None,
+    dtype: typing.Type[np.floating] = np.float64,
+):
+    """Create a Laplace assembler."""
+    options = BoundaryAssemblerOptions() if options is None else options
+    return BoundaryAssembler(
+        options,
+        _lib.laplace_boundary_assembler_new(
+            options._rs_options, operator_type.value, _rtypes[dtype]
+        ),
+    )
+
+
+def create_helmholtz_assembler(
+    operator_type: OperatorType,
+    wavenumber: float,
+    options: typing.Optional[BoundaryAssemblerOptions] = None,
+    dtype: typing.Type[np.complexfloating] = np.complex128,
+):
+    """Create a Helmholtz assembler (wraps helmholtz_boundary_assembler_new)."""
+    options = BoundaryAssemblerOptions() if options is None else options
+    real = np.float32 if dtype == np.complex64 else np.float64
+    k = np.array([wavenumber], dtype=real)
+    ctype = "float*" if real == np.float32 else "double*"
+    return BoundaryAssembler(
+        options,
+        _lib.helmholtz_boundary_assembler_new(
+            _ffi.cast(ctype, k.ctypes.data), options._rs_options, operator_type.value,
+            _rtypes[dtype]
+        ),
+    )

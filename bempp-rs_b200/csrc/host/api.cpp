@@ -1,0 +1,508 @@
+// extern "C" entry points declared in include/bempp_b200.h.
+//
+// Every function keeps the name, argument order and meaning of the bempp-rs C interface
+// (the src/bindings/ tree).  Where the reference panics (and so aborts across the FFI) these
+// record a message for bempp_last_error() and return a neutral value; the *_ex and
+// device variants return a status code.
+#include <cstring>
+#include <string>
+
+#include "../../../include/bempp_b200.h"
+#include "core.h"
+
+using namespace bempp_b200;
+
+struct BoundaryAssemblerOptionsT {
+  Options options;
+};
+
+namespace {
+thread_local std::string t_last_error;
+}
+
+namespace bempp_b200 {
+void set_last_error(const std::string& msg) { t_last_error = msg; }
+void clear_last_error() { t_last_error.clear(); }
+}  // namespace bempp_b200
+
+namespace {
+
+template <typename F>
+BemppStatus guarded(F&& f) {
+  try {
+    clear_last_error();
+    f();
+    return BemppStatus_Ok;
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    set_last_error("host out of memory");
+    return BemppStatus_OutOfMemory;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return BemppStatus_Internal;
+  }
+}
+
+template <typename T>
+T* require(T* p, const char* what) {
+  if (!p) throw Error(kInvalidArgument, std::string("null ") + what);
+  return p;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bempp_last_error(void) { return t_last_error.c_str(); }
+
+// ----------------------------------------------------------------------- options ---
+BoundaryAssemblerOptionsT* boundary_assembler_options_new(void) {
+  return new BoundaryAssemblerOptionsT();
+}
+
+void boundary_assembler_options_t_free(BoundaryAssemblerOptionsT* ptr) { delete ptr; }
+
+void boundary_assembler_options_set_regular_quadrature_degree(BoundaryAssemblerOptionsT* o,
+                                                              ReferenceCellType cell_type,
+                                                              size_t npoints) {
+  guarded([&] {
+    require(o, "options");
+    // HashMap::entry(..).and_modify(..): only an existing key changes
+    auto it = o->options.regular.find(cell_type);
+    if (it != o->options.regular.end()) it->second = npoints;
+  });
+}
+
+size_t boundary_assembler_options_get_regular_quadrature_degree(BoundaryAssemblerOptionsT* o,
+                                                                ReferenceCellType cell_type) {
+  size_t v = 0;
+  guarded([&] {
+    require(o, "options");
+    auto it = o->options.regular.find(cell_type);
+    if (it == o->options.regular.end())
+      throw Error(kInvalidArgument, "no regular quadrature degree for this cell type");
+    v = it->second;
+  });
+  return v;
+}
+
+bool boundary_assembler_options_has_regular_quadrature_degree(BoundaryAssemblerOptionsT* o,
+                                                              ReferenceCellType cell_type) {
+  return o && o->options.regular.count(cell_type) > 0;
+}
+
+void boundary_assembler_options_set_singular_quadrature_degree(BoundaryAssemblerOptionsT* o,
+                                                               ReferenceCellType c0,
+                                                               ReferenceCellType c1,
+                                                               size_t npoints) {
+  guarded([&] {
+    require(o, "options");
+    auto it = o->options.singular.find({c0, c1});
+    if (it != o->options.singular.end()) it->second = npoints;
+  });
+}
+
+size_t boundary_assembler_options_get_singular_quadrature_degree(BoundaryAssemblerOptionsT* o,
+                                                                 ReferenceCellType c0,
+                                                                 ReferenceCellType c1) {
+  size_t v = 0;
+  guarded([&] {
+    require(o, "options");
+    auto it = o->options.singular.find({c0, c1});
+    if (it == o->options.singular.end())
+      throw Error(kInvalidArgument, "no singular quadrature degree for this cell pair");
+    v = it->second;
+  });
+  return v;
+}
+
+bool boundary_assembler_options_has_singular_quadrature_degree(BoundaryAssemblerOptionsT* o,
+                                                               ReferenceCellType c0,
+                                                               ReferenceCellType c1) {
+  return o && o->options.singular.count({c0, c1}) > 0;
+}
+
+void boundary_assembler_options_set_batch_size(BoundaryAssemblerOptionsT* o, size_t batch_size) {
+  if (o) o->options.batch_size = batch_size;
+}
+
+size_t boundary_assembler_options_get_batch_size(BoundaryAssemblerOptionsT* o) {
+  return o ? o->options.batch_size : 0;
+}
+
+void boundary_assembler_options_set_precision(BoundaryAssemblerOptionsT* o, Precision p) {
+  guarded([&] {
+    require(o, "options");
+    if (p > Precision_Mixed) throw Error(kInvalidArgument, "unknown precision");
+    o->options.precision = p;
+  });
+}
+
+Precision boundary_assembler_options_get_precision(BoundaryAssemblerOptionsT* o) {
+  return o ? o->options.precision : Precision_FP64;
+}
+
+// -------------------------------------------------------------------- assemblers ---
+static BoundaryAssemblerT* new_assembler(const BoundaryAssemblerOptionsT* o, int kernel,
+                                         OperatorType op, DType dtype, double k) {
+  BoundaryAssemblerT* out = nullptr;
+  guarded([&] {
+    require(o, "options");
+    if (op > OperatorType_Hypersingular)
+      throw Error(kUnsupported, std::string("invalid operator for ") +
+                                    (kernel == kLaplace ? "Laplace" : "Helmholtz"));
+    if (kernel == kLaplace && dtype != DType_F32 && dtype != DType_F64)
+      throw Error(kInvalidArgument, "invalid dtype for Laplace");
+    if (kernel == kHelmholtz && dtype != DType_C32 && dtype != DType_C64)
+      throw Error(kInvalidArgument, "invalid dtype for Helmholtz");
+    auto* a = new BoundaryAssemblerT();
+    a->kernel = kernel;
+    a->op = op;
+    a->dtype = dtype;
+    a->k = k;
+    a->options = o->options;
+    out = a;
+  });
+  return out;
+}
+
+BoundaryAssemblerT* laplace_boundary_assembler_new(const BoundaryAssemblerOptionsT* options,
+                                                   OperatorType operator_type, DType dtype) {
+  return new_assembler(options, kLaplace, operator_type, dtype, 0.0);
+}
+
+BoundaryAssemblerT* helmholtz_boundary_assembler_new(const void* k,
+                                                     const BoundaryAssemblerOptionsT* options,
+                                                     OperatorType operator_type, DType dtype) {
+  if (!k) {
+    set_last_error("null wavenumber");
+    return nullptr;
+  }
+  double kv = dtype == DType_C32 ? static_cast<double>(*static_cast<const float*>(k))
+                                 : *static_cast<const double*>(k);
+  return new_assembler(options, kHelmholtz, operator_type, dtype, kv);
+}
+
+void boundary_assembler_t_free(BoundaryAssemblerT* ptr) { delete ptr; }
+
+DType boundary_assembler_dtype(BoundaryAssemblerT* a) { return a ? a->dtype : DType_F64; }
+
+BemppStatus boundary_assembler_assemble_into_device(BoundaryAssemblerT* a, SpaceT* trial,
+                                                    SpaceT* test, void* device_data,
+                                                    void* stream) {
+  return guarded([&] {
+    require(a, "assembler");
+    require(trial, "trial space");
+    require(test, "test space");
+    if (test->ndofs > 0 && trial->ndofs > 0) require(device_data, "output");
+    std::lock_guard<std::mutex> lock(a->mu);
+    assemble_device(*a, *trial, *test, device_data, static_cast<cudaStream_t>(stream));
+  });
+}
+
+BemppStatus boundary_assembler_assemble_into_memory_ex(BoundaryAssemblerT* a, SpaceT* trial,
+                                                       SpaceT* test, void* data) {
+  return guarded([&] {
+    require(a, "assembler");
+    require(trial, "trial space");
+    require(test, "test space");
+    const size_t n = static_cast<size_t>(test->ndofs) * trial->ndofs;
+    if (n == 0) return;
+    require(data, "output");
+    std::lock_guard<std::mutex> lock(a->mu);
+    const size_t bytes = n * dtype_size(a->dtype);
+    a->work.alloc(bytes);
+    assemble_device(*a, *trial, *test, a->work.ptr, nullptr);
+    BEMPP_CUDA(cudaMemcpy(data, a->work.ptr, bytes, cudaMemcpyDeviceToHost));
+  });
+}
+
+void boundary_assembler_assemble_into_memory(BoundaryAssemblerT* a, SpaceT* trial,
+                                             SpaceT* test, void* data) {
+  boundary_assembler_assemble_into_memory_ex(a, trial, test, data);
+}
+
+MatrixT* boundary_assembler_assemble(BoundaryAssemblerT* a, SpaceT* trial, SpaceT* test) {
+  MatrixT* out = nullptr;
+  guarded([&] {
+    require(a, "assembler");
+    require(trial, "trial space");
+    require(test, "test space");
+    auto* m = new MatrixT();
+    m->csr = false;
+    m->dtype = a->dtype;
+    m->rows = test->ndofs;
+    m->cols = trial->ndofs;
+    m->data.resize(m->rows * m->cols * dtype_size(a->dtype));
+    BemppStatus s = boundary_assembler_assemble_into_memory_ex(a, trial, test, m->data.data());
+    if (s != BemppStatus_Ok) {
+      std::string msg = bempp_last_error();
+      delete m;
+      throw Error(static_cast<Status>(s), msg);
+    }
+    out = m;
+  });
+  return out;
+}
+
+MatrixT* boundary_assembler_assemble_singular(BoundaryAssemblerT* a, SpaceT* trial,
+                                              SpaceT* test) {
+  MatrixT* out = nullptr;
+  guarded([&] {
+    require(a, "assembler");
+    require(trial, "trial space");
+    require(test, "test space");
+    std::lock_guard<std::mutex> lock(a->mu);
+    out = assemble_singular_csr(*a, *trial, *test);
+  });
+  return out;
+}
+
+void boundary_assembler_set_timing(BoundaryAssemblerT* a, bool enabled) {
+  if (a) a->timing = enabled;
+}
+
+size_t boundary_assembler_phase_times(BoundaryAssemblerT* a, double* ms, size_t n) {
+  size_t written = 0;
+  guarded([&] {
+    require(a, "assembler");
+    if (a->events_recorded < 2) return;
+    BEMPP_CUDA(cudaEventSynchronize(a->events[a->events_recorded - 1]));
+    for (int i = 1; i < a->events_recorded && written < n; ++i) {
+      float t = 0.f;
+      BEMPP_CUDA(cudaEventElapsedTime(&t, a->events[i - 1], a->events[i]));
+      if (ms) ms[written] = t;
+      ++written;
+    }
+  });
+  return written;
+}
+
+size_t boundary_assembler_last_launch_count(BoundaryAssemblerT* a) { return a ? a->launches : 0; }
+
+BemppStatus bempp_measure_fma_peak(int fp64, int iters, int reps, double* tflops) {
+  return guarded([&] {
+    require(tflops, "output");
+    if (iters <= 0 || reps <= 0) throw Error(kInvalidArgument, "iters and reps must be positive");
+    BEMPP_CUDA(measure_fma_peak(fp64, iters, reps, tflops));
+  });
+}
+
+// ---------------------------------------------------------------------- matrices ---
+size_t matrix_shape0(MatrixT* m) { return m ? m->rows : 0; }
+size_t matrix_shape1(MatrixT* m) { return m ? m->cols : 0; }
+DType matrix_dtype(MatrixT* m) { return m ? m->dtype : DType_F64; }
+bool matrix_is_csr(MatrixT* m) { return m && m->csr; }
+
+const void* matrix_dense_data(MatrixT* m) {
+  if (!m || m->csr) {
+    set_last_error("not a dense matrix");
+    return nullptr;
+  }
+  return m->data.data();
+}
+
+void matrix_dense_data_copy(MatrixT* m, void* data) {
+  if (!m || m->csr || !data) {
+    set_last_error("not a dense matrix or null output");
+    return;
+  }
+  std::memcpy(data, m->data.data(), m->data.size());
+}
+
+size_t matrix_csr_data_size(MatrixT* m) {
+  return (m && m->csr) ? m->indices.size() : 0;
+}
+const void* matrix_csr_data(MatrixT* m) { return (m && m->csr) ? m->data.data() : nullptr; }
+void matrix_csr_data_copy(MatrixT* m, void* data) {
+  if (m && m->csr && data) std::memcpy(data, m->data.data(), m->data.size());
+}
+size_t matrix_csr_indices_size(MatrixT* m) { return (m && m->csr) ? m->indices.size() : 0; }
+const uintptr_t* matrix_csr_indices(MatrixT* m) {
+  return (m && m->csr) ? m->indices.data() : nullptr;
+}
+void matrix_csr_indices_copy(MatrixT* m, uintptr_t* indices) {
+  if (m && m->csr && indices)
+    std::memcpy(indices, m->indices.data(), m->indices.size() * sizeof(uintptr_t));
+}
+size_t matrix_csr_indptr_size(MatrixT* m) { return (m && m->csr) ? m->indptr.size() : 0; }
+const uintptr_t* matrix_csr_indptr(MatrixT* m) {
+  return (m && m->csr) ? m->indptr.data() : nullptr;
+}
+void matrix_csr_indptr_copy(MatrixT* m, uintptr_t* indptr) {
+  if (m && m->csr && indptr)
+    std::memcpy(indptr, m->indptr.data(), m->indptr.size() * sizeof(uintptr_t));
+}
+void matrix_t_free(MatrixT* ptr) { delete ptr; }
+
+// ------------------------------------------------------------------------ spaces ---
+SpaceT* function_space(GridT* grid, ElementFamilyT* e_family) {
+  SpaceT* out = nullptr;
+  guarded([&] {
+    require(grid, "grid");
+    require(e_family, "element family");
+    out = make_space(grid, *e_family);
+  });
+  return out;
+}
+
+void space_t_free(SpaceT* ptr) { delete ptr; }
+
+SpaceT* space_local_space(SpaceT* s) {
+  SpaceT* out = nullptr;
+  guarded([&] {
+    require(s, "space");
+    ElementFamilyT fam{s->degree, static_cast<uint8_t>(s->continuous ? 0 : 1), s->dtype};
+    out = make_space(s->grid, fam);
+  });
+  return out;
+}
+
+bool space_is_serial(SpaceT* s) { return s != nullptr; }
+
+size_t space_get_local_dof_numbers_size(SpaceT* s, size_t dim, size_t entity) {
+  if (!s || dim > 2 || entity >= s->entity_dofs[dim].size()) return 0;
+  return s->entity_dofs[dim][entity].size();
+}
+
+void space_get_local_dof_numbers(SpaceT* s, size_t dim, size_t entity, uintptr_t* dofs) {
+  if (!s || !dofs || dim > 2 || entity >= s->entity_dofs[dim].size()) return;
+  const auto& v = s->entity_dofs[dim][entity];
+  for (size_t i = 0; i < v.size(); ++i) dofs[i] = static_cast<uintptr_t>(v[i]);
+}
+
+size_t space_local_size(SpaceT* s) { return s ? static_cast<size_t>(s->ndofs) : 0; }
+size_t space_global_size(SpaceT* s) { return s ? static_cast<size_t>(s->ndofs) : 0; }
+
+bool space_has_cell_dofs(SpaceT* s, size_t cell) {
+  return s && cell < static_cast<size_t>(s->grid->ncells);
+}
+
+size_t space_cell_dofs_size(SpaceT* s, size_t cell) {
+  return space_has_cell_dofs(s, cell) ? static_cast<size_t>(s->nbasis) : 0;
+}
+
+void space_cell_dofs(SpaceT* s, size_t cell, uintptr_t* dofs) {
+  if (!space_has_cell_dofs(s, cell) || !dofs) return;
+  for (int b = 0; b < s->nbasis; ++b)
+    dofs[b] = static_cast<uintptr_t>(s->cell_dofs[cell * s->nbasis + b]);
+}
+
+size_t space_global_dof_index(SpaceT* s, size_t local_dof_index) {
+  (void)s;
+  return local_dof_index;  // serial space: global numbering = local numbering
+}
+
+bool space_is_owned(SpaceT* s, size_t local_dof_index) {
+  return s && local_dof_index < static_cast<size_t>(s->ndofs);
+}
+
+size_t space_ownership_process(SpaceT* s, size_t local_dof_index) {
+  (void)s;
+  (void)local_dof_index;
+  return 0;
+}
+
+size_t space_ownership_index(SpaceT* s, size_t local_dof_index) {
+  (void)s;
+  return local_dof_index;
+}
+
+DType space_dtype(SpaceT* s) { return s ? s->dtype : DType_F64; }
+
+// ------------------------------------------------------------- grids, elements ---
+static GridT* make_grid(const void* points, size_t npoints, size_t gdim, DType dtype,
+                        const size_t* cells, size_t ncells, size_t points_per_cell) {
+  GridT* out = nullptr;
+  guarded([&] {
+    if (npoints > 0) require(points, "points");
+    if (ncells > 0) require(cells, "cells");
+    if (gdim != 3) throw Error(kUnsupported, "only surface grids in 3D are supported");
+    if (points_per_cell < 3) throw Error(kInvalidArgument, "cells need three vertices");
+    if (dtype != DType_F32 && dtype != DType_F64)
+      throw Error(kInvalidArgument, "grid points must be F32 or F64");
+    auto* g = new GridT();
+    g->dtype = dtype;
+    g->npoints = static_cast<int64_t>(npoints);
+    g->ncells = static_cast<int64_t>(ncells);
+    g->points.resize(3 * npoints);
+    for (size_t i = 0; i < 3 * npoints; ++i)
+      g->points[i] = dtype == DType_F64 ? static_cast<const double*>(points)[i]
+                                        : static_cast<const float*>(points)[i];
+    g->cells.resize(3 * ncells);
+    for (size_t c = 0; c < ncells; ++c)
+      for (int i = 0; i < 3; ++i) {
+        size_t v = cells[c * points_per_cell + i];
+        if (v >= npoints) {
+          delete g;
+          throw Error(kInvalidArgument, "cell vertex index out of range");
+        }
+        g->cells[3 * c + i] = static_cast<int>(v);
+      }
+    out = g;
+  });
+  return out;
+}
+
+GridT* single_element_grid_borrowed_create_bempp(
+    size_t tdim, const size_t* id_sizes, const size_t* const* id_pointers,
+    const ReferenceCellType* entity_types, const size_t* entity_counts,
+    const size_t* const* const* downward_connectivity,
+    const size_t* const* downward_connectivity_shape0,
+    const size_t* const* const* const* upward_connectivity,
+    const size_t* const* const* upward_connectivity_lens, const void* points, size_t gdim,
+    size_t npoints, DType dtype, const size_t* cells, size_t points_per_cell, size_t ncells,
+    size_t geometry_degree) {
+  (void)id_sizes;
+  (void)id_pointers;
+  (void)entity_counts;
+  (void)downward_connectivity;
+  (void)downward_connectivity_shape0;
+  (void)upward_connectivity;
+  (void)upward_connectivity_lens;
+  if (tdim != 2 || (entity_types && entity_types[2] != ReferenceCellType_Triangle)) {
+    set_last_error("only triangle surface grids are supported");
+    return nullptr;
+  }
+  if (geometry_degree != 1) {
+    set_last_error("only flat (degree-1) cells are supported");
+    return nullptr;
+  }
+  return make_grid(points, npoints, gdim, dtype, cells, ncells, points_per_cell);
+}
+
+GridT* bempp_grid_from_points_cells(const void* points, size_t npoints, DType dtype,
+                                    const size_t* cells, size_t ncells) {
+  return make_grid(points, npoints, 3, dtype, cells, ncells, 3);
+}
+
+void grid_t_free_bempp(GridT* ptr) { delete ptr; }
+
+ElementFamilyT* create_lagrange_family_bempp(size_t degree, Continuity continuity, DType dtype) {
+  if (degree > 1) {
+    set_last_error("only Lagrange degree 0 and 1 are supported");
+    return nullptr;
+  }
+  if (continuity > Continuity_Discontinuous || dtype > DType_C64) {
+    set_last_error("invalid continuity or dtype");
+    return nullptr;
+  }
+  // degree 0 is always discontinuous
+  return new ElementFamilyT{degree, static_cast<uint8_t>(degree == 0 ? 1 : continuity), dtype};
+}
+
+ElementFamilyT* create_raviart_thomas_family_bempp(size_t, Continuity, DType) {
+  set_last_error("Raviart-Thomas spaces are not supported");
+  return nullptr;
+}
+
+ElementFamilyT* create_nedelec_family_bempp(size_t, Continuity, DType) {
+  set_last_error("Nedelec spaces are not supported");
+  return nullptr;
+}
+
+void element_family_t_free_bempp(ElementFamilyT* ptr) { delete ptr; }
+
+}  // extern "C"

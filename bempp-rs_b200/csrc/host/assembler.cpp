@@ -1,0 +1,398 @@
+// Assembly driver: device-resident caches and the kernel sequence of one dense assembly.
+//
+// bempp-rs BoundaryAssembler::assemble_into_memory (src/boundary_assemblers.rs:176-214)
+// runs the regular part over coloured 128x128 cell blocks with rayon, then the singular
+// part into COO triplets, then adds the triplets serially.  Here one assembly is a short
+// stream-ordered kernel sequence on the caller's stream:
+//   1. geometry (once per grid and regular rule, cached on the device),
+//   2. regular part: DP0 x DP0 -> direct-store kernel (writes every entry);
+//      otherwise memset + tile-scatter kernel,
+//   3. singular part: one warp per adjacent cell pair, added into the dense output,
+//   4. F32 / C32 outputs: one conversion pass from the FP64 staging buffer.
+// Vertex-sharing pairs are skipped by the regular kernels exactly when test and trial
+// spaces live on the same grid object (pointer equality, as equal_grids at
+// src/boundary_assemblers/helpers.rs:59-64).
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <map>
+
+#include "core.h"
+
+namespace bempp_b200 {
+
+void build_singular_pairs(GridT& g, SingularPairList& out);
+void build_tiles(const SpaceT& s, int tile, std::vector<int>& off, std::vector<int>& dofs,
+                 std::vector<uint8_t>& ldof, int& max_dofs);
+int scatter_tile_cells();
+cudaError_t launch_convert_to_single(const double* src, void* dst, size_t n_reals,
+                                     cudaStream_t stream);
+
+size_t dtype_size(uint8_t dtype) {
+  switch (dtype) {
+    case 0: return 4;
+    case 1: return 8;
+    case 2: return 8;
+    case 3: return 16;
+    default: throw Error(kInvalidArgument, "unknown dtype");
+  }
+}
+
+namespace {
+
+int current_device() {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) throw Error(kNoDevice, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+    throw Error(kNoDevice, "no CUDA device");
+  return dev;
+}
+
+// Duffy rules per (device, order), shared by all assemblers.
+struct DeviceRules {
+  DeviceBuffer offset, test_xi, trial_xi, w;
+  int total = 0;
+};
+std::mutex g_rules_mu;
+std::map<std::pair<int, int>, std::unique_ptr<DeviceRules>> g_rules;
+
+const DeviceRules& device_rules(int device, int order) {
+  std::lock_guard<std::mutex> lock(g_rules_mu);
+  auto& slot = g_rules[{device, order}];
+  if (!slot) {
+    auto r = std::make_unique<DeviceRules>();
+    std::vector<int> off{0};
+    std::vector<double> txi, sxi, w;
+    for (size_t c = 0; c < singular_configurations().size(); ++c) {
+      DuffyRule d = duffy_rule(static_cast<int>(c), order);
+      txi.insert(txi.end(), d.test_xi.begin(), d.test_xi.end());
+      sxi.insert(sxi.end(), d.trial_xi.begin(), d.trial_xi.end());
+      w.insert(w.end(), d.w.begin(), d.w.end());
+      off.push_back(static_cast<int>(w.size()));
+    }
+    r->offset.upload(off);
+    r->test_xi.upload(txi);
+    r->trial_xi.upload(sxi);
+    r->w.upload(w);
+    r->total = static_cast<int>(w.size());
+    slot = std::move(r);
+  }
+  return *slot;
+}
+
+void ensure_grid_device(GridT& g, int device) {
+  if (g.device == device && g.d_points.ptr) return;
+  if (g.device != -1 && g.device != device)
+    throw Error(kUnsupported, "a grid is bound to the device it was first assembled on");
+  if (g.ncells > INT32_MAX / 3 || g.npoints > INT32_MAX)
+    throw Error(kUnsupported, "grid too large for 32-bit cell indices");
+  g.d_points.upload(g.points);
+  g.d_cells.upload(g.cells);
+  g.device = device;
+}
+
+const GridGeometry& grid_geometry(GridT& g, int device, const RegularRule& rule,
+                                  cudaStream_t stream, size_t& launches) {
+  std::lock_guard<std::mutex> lock(g.mu);
+  ensure_grid_device(g, device);
+  auto& slot = g.geometry[rule.npts];
+  if (!slot) {
+    auto geo = std::make_unique<GridGeometry>();
+    const size_t n = g.ncells;
+    geo->npts = rule.npts;
+    geo->geom.alloc(sizeof(double) * kNumGeomFields * n);
+    geo->qpts.alloc(sizeof(double) * 3 * rule.npts * n);
+    geo->qrel.alloc(sizeof(float) * 3 * rule.npts * n);
+    geo->vids.alloc(sizeof(int) * 3 * n);
+    BEMPP_CUDA(launch_geometry(g.d_points.as<double>(), g.d_cells.as<int>(),
+                               static_cast<int>(n), rule, geo->geom.as<double>(),
+                               geo->qpts.as<double>(), geo->qrel.as<float>(),
+                               geo->vids.as<int>(), stream));
+    ++launches;
+    slot = std::move(geo);
+  }
+  return *slot;
+}
+
+SingularPairList& grid_pairs(GridT& g, int device) {
+  std::lock_guard<std::mutex> lock(g.mu);
+  ensure_grid_device(g, device);
+  if (!g.pairs) {
+    g.build_topology();
+    auto p = std::make_unique<SingularPairList>();
+    build_singular_pairs(g, *p);
+    p->d_test.upload(p->test_cell);
+    p->d_trial.upload(p->trial_cell);
+    p->d_config.upload(p->config);
+    p->uploaded = true;
+    g.pairs = std::move(p);
+  }
+  return *g.pairs;
+}
+
+void ensure_space_device(SpaceT& s, int device) {
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (s.device == device && s.d_dofs.ptr) return;
+  if (s.device != -1 && s.device != device)
+    throw Error(kUnsupported, "a space is bound to the device it was first assembled on");
+  if (s.ndofs > INT32_MAX) throw Error(kUnsupported, "too many DOFs for 32-bit indices");
+  std::vector<int> dofs(s.cell_dofs.begin(), s.cell_dofs.end());
+  s.d_dofs.upload(dofs);
+  std::vector<int> off, tdofs;
+  std::vector<uint8_t> ldof;
+  s.tile_cells = scatter_tile_cells();
+  build_tiles(s, s.tile_cells, off, tdofs, ldof, s.max_tile_dofs);
+  s.ntiles = static_cast<int>(off.size()) - 1;
+  s.d_tile_off.upload(off);
+  s.d_tile_dofs.upload(tdofs);
+  s.d_cell_ldof.upload(ldof);
+  s.device = device;
+}
+
+CellSet cell_set(const GridT& g, const GridGeometry& geo) {
+  CellSet c;
+  c.ncells = static_cast<int>(g.ncells);
+  c.geom = geo.geom.as<double>();
+  c.qpts = geo.qpts.as<double>();
+  c.qrel = geo.qrel.as<float>();
+  c.vids = geo.vids.as<int>();
+  return c;
+}
+
+SpaceTiles space_tiles(const SpaceT& s) {
+  SpaceTiles t;
+  t.nbasis = s.nbasis;
+  t.tile_cells = s.tile_cells;
+  t.ntiles = s.ntiles;
+  t.max_tile_dofs = s.max_tile_dofs;
+  t.tile_dof_off = s.d_tile_off.as<int>();
+  t.tile_dofs = s.d_tile_dofs.as<int>();
+  t.cell_ldof = s.d_cell_ldof.as<uint8_t>();
+  return t;
+}
+
+void check_spaces(const BoundaryAssemblerT& a, const SpaceT& trial, const SpaceT& test) {
+  if (!trial.grid || !test.grid) throw Error(kInvalidArgument, "space without grid");
+  (void)a;
+}
+
+struct Timer {
+  BoundaryAssemblerT& a;
+  cudaStream_t stream;
+  int next = 0;
+  Timer(BoundaryAssemblerT& asmb, cudaStream_t s) : a(asmb), stream(s) {
+    if (!a.timing) return;
+    for (auto& e : a.events)
+      if (!e) BEMPP_CUDA(cudaEventCreate(&e));
+    mark();
+  }
+  void mark() {
+    if (a.timing && next < 5) BEMPP_CUDA(cudaEventRecord(a.events[next++], stream));
+  }
+  // Durations are read lazily (boundary_assembler_phase_times) so that timing adds no
+  // host synchronisation to the assembly itself.
+  void finish() { a.events_recorded = a.timing ? next : 0; }
+};
+
+}  // namespace
+
+void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d_out,
+                     cudaStream_t stream) {
+  check_spaces(a, trial, test);
+  const int device = current_device();
+  const auto qit = a.options.regular.find(kTriangle);
+  if (qit == a.options.regular.end())
+    throw Error(kInvalidArgument, "no regular quadrature degree for triangles");
+  const auto sit = a.options.singular.find({kTriangle, kTriangle});
+  if (sit == a.options.singular.end())
+    throw Error(kInvalidArgument, "no singular quadrature degree for triangle pairs");
+  const RegularRule rule = simplex_rule(static_cast<int>(qit->second));
+  const int order = static_cast<int>(sit->second);
+  const bool same_grid = trial.grid == test.grid;
+  const int64_t nt = test.ndofs, ns = trial.ndofs;
+  a.launches = 0;
+
+  ensure_space_device(test, device);
+  ensure_space_device(trial, device);
+  Timer timer(a, stream);
+  const GridGeometry& tgeo = grid_geometry(*test.grid, device, rule, stream, a.launches);
+  const GridGeometry& sgeo = grid_geometry(*trial.grid, device, rule, stream, a.launches);
+  timer.mark();
+
+  const bool single = a.dtype == 0 || a.dtype == 2;
+  const bool cplx = a.kernel == kHelmholtz;
+  void* out = d_out;
+  if (single) {
+    a.convert.alloc(static_cast<size_t>(nt) * ns * (cplx ? 16 : 8));
+    out = a.convert.ptr;
+  }
+  RegularArgs ra;
+  ra.kernel = a.kernel;
+  ra.op = a.op;
+  ra.k = a.k;
+  ra.same_grid = same_grid ? 1 : 0;
+  ra.precision = a.options.precision == 1 ? kRegularMixed : kRegularFP64;
+  ra.out_type = cplx ? kOutC128 : kOutF64;
+  ra.ld = nt;
+  ra.out = out;
+  const CellSet tcs = cell_set(*test.grid, tgeo), scs = cell_set(*trial.grid, sgeo);
+  const bool dp0 = test.nbasis == 1 && trial.nbasis == 1 && a.op != kHS;
+  if (nt > 0 && ns > 0) {
+    if (dp0) {
+      timer.mark();  // no memset phase: the DP0 kernel writes every entry
+      BEMPP_CUDA(launch_regular_dp0(tcs, scs, rule, ra, stream));
+      ++a.launches;
+    } else {
+      BEMPP_CUDA(cudaMemsetAsync(out, 0, static_cast<size_t>(nt) * ns * (cplx ? 16 : 8), stream));
+      timer.mark();
+      BEMPP_CUDA(launch_regular_scatter(tcs, space_tiles(test), scs, space_tiles(trial), rule,
+                                        ra, stream));
+      ++a.launches;
+    }
+  }
+  timer.mark();
+  if (same_grid && nt > 0 && ns > 0) {
+    SingularPairList& pl = grid_pairs(*test.grid, device);
+    const DeviceRules& dr = device_rules(device, order);
+    SingularRules rules{dr.offset.as<int>(), dr.test_xi.as<double>(), dr.trial_xi.as<double>(),
+                        dr.w.as<double>()};
+    SingularPairs pairs{static_cast<int>(pl.test_cell.size()), pl.d_test.as<int>(),
+                        pl.d_trial.as<int>(), pl.d_config.as<int>()};
+    SingularArgs sa;
+    sa.kernel = a.kernel;
+    sa.op = a.op;
+    sa.k = a.k;
+    sa.out_type = ra.out_type;
+    sa.ld = nt;
+    sa.out = out;
+    sa.unique_entries = dp0 ? 1 : 0;
+    sa.pair_values = nullptr;
+    BEMPP_CUDA(launch_singular(tcs, test.d_dofs.as<int>(), test.nbasis, scs,
+                               trial.d_dofs.as<int>(), trial.nbasis, rules, pairs, sa, stream));
+    ++a.launches;
+  }
+  if (single) {
+    BEMPP_CUDA(launch_convert_to_single(static_cast<const double*>(out), d_out,
+                                        static_cast<size_t>(nt) * ns * (cplx ? 2 : 1), stream));
+    ++a.launches;
+  }
+  timer.mark();
+  timer.finish();
+}
+
+MatrixT* assemble_singular_csr(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test) {
+  check_spaces(a, trial, test);
+  const int device = current_device();
+  const bool cplx = a.kernel == kHelmholtz;
+  const bool single = a.dtype == 0 || a.dtype == 2;
+  const size_t es = dtype_size(a.dtype);
+  auto* m = new MatrixT();
+  m->csr = true;
+  m->dtype = a.dtype;
+  m->rows = test.ndofs;
+  m->cols = trial.ndofs;
+  std::vector<int64_t> rows, cols;
+  std::vector<double> vals;  // FP64 (interleaved complex)
+  const int nvals = test.nbasis * trial.nbasis * (cplx ? 2 : 1);
+  if (trial.grid == test.grid && test.ndofs > 0 && trial.ndofs > 0) {
+    const auto sit = a.options.singular.find({kTriangle, kTriangle});
+    if (sit == a.options.singular.end())
+      throw Error(kInvalidArgument, "no singular quadrature degree for triangle pairs");
+    const auto qit = a.options.regular.find(kTriangle);
+    const RegularRule rule = simplex_rule(qit == a.options.regular.end() ? 6 : static_cast<int>(qit->second));
+    ensure_space_device(test, device);
+    ensure_space_device(trial, device);
+    size_t launches = 0;
+    const GridGeometry& geo = grid_geometry(*test.grid, device, rule, nullptr, launches);
+    SingularPairList& pl = grid_pairs(*test.grid, device);
+    const DeviceRules& dr = device_rules(device, static_cast<int>(sit->second));
+    const int np = static_cast<int>(pl.test_cell.size());
+    a.pair_values.alloc(sizeof(double) * std::max(1, np * nvals));
+    SingularRules rules{dr.offset.as<int>(), dr.test_xi.as<double>(), dr.trial_xi.as<double>(),
+                        dr.w.as<double>()};
+    SingularPairs pairs{np, pl.d_test.as<int>(), pl.d_trial.as<int>(), pl.d_config.as<int>()};
+    SingularArgs sa{a.kernel, a.op, a.k, cplx ? kOutC128 : kOutF64, 0, nullptr, 0,
+                    a.pair_values.as<double>()};
+    const CellSet cs = cell_set(*test.grid, geo);
+    BEMPP_CUDA(launch_singular(cs, test.d_dofs.as<int>(), test.nbasis, cs, trial.d_dofs.as<int>(),
+                               trial.nbasis, rules, pairs, sa, nullptr));
+    std::vector<double> pv(static_cast<size_t>(np) * nvals);
+    BEMPP_CUDA(cudaMemcpy(pv.data(), a.pair_values.ptr, pv.size() * sizeof(double),
+                          cudaMemcpyDeviceToHost));
+    // COO triplets in the reference's order: per pair, trial basis outer, test inner
+    // (src/boundary_assemblers.rs:675-681)
+    for (int p = 0; p < np; ++p)
+      for (int b = 0; b < trial.nbasis; ++b)
+        for (int aa = 0; aa < test.nbasis; ++aa) {
+          const int e = aa + test.nbasis * b;
+          rows.push_back(test.cell_dofs[static_cast<int64_t>(pl.test_cell[p]) * test.nbasis + aa]);
+          cols.push_back(trial.cell_dofs[static_cast<int64_t>(pl.trial_cell[p]) * trial.nbasis + b]);
+          if (cplx) {
+            vals.push_back(pv[static_cast<size_t>(p) * nvals + 2 * e]);
+            vals.push_back(pv[static_cast<size_t>(p) * nvals + 2 * e + 1]);
+          } else {
+            vals.push_back(pv[static_cast<size_t>(p) * nvals + e]);
+          }
+        }
+  }
+  // src/boundary_assemblers.rs:130-145: an all-(near-)zero singular part is an empty CSR
+  const double tiny = 1e-10;
+  bool any = false;
+  const size_t nnz_in = rows.size();
+  for (size_t i = 0; i < nnz_in && !any; ++i) {
+    double mag = cplx ? std::hypot(vals[2 * i], vals[2 * i + 1]) : std::fabs(vals[i]);
+    any = mag > tiny;
+  }
+  m->indptr.assign(m->rows + 1, 0);
+  if (!any) return m;
+  // from_aij: sort by (row, col), sum duplicates
+  std::vector<size_t> order(nnz_in);
+  for (size_t i = 0; i < nnz_in; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+    return rows[x] != rows[y] ? rows[x] < rows[y] : cols[x] < cols[y];
+  });
+  std::vector<double> merged;
+  std::vector<int64_t> mrow;
+  for (size_t k = 0; k < nnz_in; ++k) {
+    const size_t i = order[k];
+    if (!m->indices.empty() && mrow.back() == rows[i] &&
+        static_cast<int64_t>(m->indices.back()) == cols[i]) {
+      if (cplx) {
+        merged[merged.size() - 2] += vals[2 * i];
+        merged[merged.size() - 1] += vals[2 * i + 1];
+      } else {
+        merged.back() += vals[i];
+      }
+      continue;
+    }
+    mrow.push_back(rows[i]);
+    m->indices.push_back(static_cast<uintptr_t>(cols[i]));
+    if (cplx) {
+      merged.push_back(vals[2 * i]);
+      merged.push_back(vals[2 * i + 1]);
+    } else {
+      merged.push_back(vals[i]);
+    }
+  }
+  for (int64_t r : mrow) m->indptr[r + 1]++;
+  for (size_t r = 0; r < m->rows; ++r) m->indptr[r + 1] += m->indptr[r];
+  const size_t nnz = m->indices.size();
+  m->data.resize(nnz * es);
+  if (single) {
+    float* d = reinterpret_cast<float*>(m->data.data());
+    for (size_t i = 0; i < merged.size(); ++i) d[i] = static_cast<float>(merged[i]);
+  } else {
+    std::memcpy(m->data.data(), merged.data(), merged.size() * sizeof(double));
+  }
+  return m;
+}
+
+}  // namespace bempp_b200
+
+BoundaryAssemblerT::~BoundaryAssemblerT() {
+  for (auto& e : events)
+    if (e) cudaEventDestroy(e);
+}

@@ -1,0 +1,205 @@
+// Internal host-side objects behind the opaque C-ABI handles.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../kernels/launch.h"
+
+namespace bempp_b200 {
+
+// Status codes (BemppStatus in include/bempp_b200.h).
+enum Status : int32_t {
+  kOk = 0,
+  kInvalidArgument = 1,
+  kUnsupported = 2,
+  kOutOfMemory = 3,
+  kCudaError = 4,
+  kNoDevice = 5,
+  kInternal = 6
+};
+
+struct Error : std::runtime_error {
+  Status status;
+  Error(Status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+void set_last_error(const std::string& msg);
+void clear_last_error();
+
+#define BEMPP_CUDA(call)                                                               \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      throw ::bempp_b200::Error(e_ == cudaErrorMemoryAllocation ? kOutOfMemory           \
+                                                                : kCudaError,            \
+                                std::string(#call) + ": " + cudaGetErrorString(e_));    \
+  } while (0)
+
+// Owning device buffer.
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  ~DeviceBuffer() { reset(); }
+  void reset() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  void alloc(size_t n) {
+    if (n <= bytes && ptr) return;
+    reset();
+    if (n == 0) return;
+    BEMPP_CUDA(cudaMalloc(&ptr, n));
+    bytes = n;
+  }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(ptr);
+  }
+  template <typename T>
+  void upload(const std::vector<T>& v) {
+    alloc(v.size() * sizeof(T));
+    if (!v.empty()) BEMPP_CUDA(cudaMemcpy(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  }
+};
+
+// ------------------------------------------------------------------------ options ---
+enum CellType : uint8_t { kPoint = 0, kInterval = 1, kTriangle = 2, kQuadrilateral = 3 };
+
+struct Options {
+  // src/boundary_assemblers.rs:43-57 defaults
+  std::map<uint8_t, size_t> regular{{kTriangle, 37}, {kQuadrilateral, 37}};
+  std::map<std::pair<uint8_t, uint8_t>, size_t> singular{{{kTriangle, kTriangle}, 4},
+                                                         {{kQuadrilateral, kQuadrilateral}, 4},
+                                                         {{kQuadrilateral, kTriangle}, 4},
+                                                         {{kTriangle, kQuadrilateral}, 4}};
+  size_t batch_size = 128;
+  uint8_t precision = 0;  // Precision_FP64
+};
+
+// --------------------------------------------------------------------------- rules ---
+void gauss_legendre_01(int n, std::vector<double>& x, std::vector<double>& w);
+// Symmetric triangle rule by number of points; throws if no rule has that count.
+RegularRule simplex_rule(int npoints);
+bool has_simplex_rule(int npoints);
+// The 28 (test_local, trial_local) vertex pairings of the reference
+// (src/boundary_assemblers.rs:267-288) and their Duffy rules of 1-D order n.
+const std::vector<std::vector<std::pair<int, int>>>& singular_configurations();
+struct DuffyRule {
+  std::vector<double> test_xi, trial_xi, w;
+};
+DuffyRule duffy_rule(int config, int order);
+
+// --------------------------------------------------------------------- grid/space ---
+struct GridGeometry {  // device geometry for one regular rule
+  int npts = 0;
+  DeviceBuffer geom, qpts, qrel, vids;
+};
+
+struct SingularPairList {
+  std::vector<int> test_cell, trial_cell, config;
+  DeviceBuffer d_test, d_trial, d_config;
+  bool uploaded = false;
+};
+
+}  // namespace bempp_b200
+
+// Handle types of the C-ABI (declared opaque in include/bempp_b200.h).
+using bempp_b200::DeviceBuffer;
+
+struct GridT {
+  std::vector<double> points;  // npoints x 3
+  std::vector<int> cells;      // ncells x 3 (triangle vertices)
+  int64_t npoints = 0, ncells = 0;
+  uint8_t dtype = 1;
+  std::vector<std::vector<int>> vertex_cells;  // upward connectivity, increasing cell index
+  std::vector<std::pair<int, int>> edges;      // unique edges (v0 < v1)
+  std::vector<std::array<int, 3>> cell_edges;  // local edge i opposite local vertex i
+  int device = -1;
+  DeviceBuffer d_points, d_cells;
+  std::map<int, std::unique_ptr<bempp_b200::GridGeometry>> geometry;  // keyed by regular npts
+  std::unique_ptr<bempp_b200::SingularPairList> pairs;
+  std::mutex mu;
+  void build_topology();
+};
+
+struct ElementFamilyT {
+  size_t degree;
+  uint8_t continuity;  // 0 standard, 1 discontinuous
+  uint8_t dtype;
+};
+
+struct SpaceT {
+  GridT* grid = nullptr;
+  size_t degree = 0;
+  bool continuous = false;
+  uint8_t dtype = 1;
+  int nbasis = 1;
+  int64_t ndofs = 0;
+  std::vector<int64_t> cell_dofs;                  // ncells x nbasis
+  std::vector<std::vector<int64_t>> entity_dofs[3];  // [dim][entity] -> dofs
+  // device mirrors
+  int device = -1;
+  DeviceBuffer d_dofs;                                   // int32 ncells x nbasis
+  DeviceBuffer d_tile_off, d_tile_dofs, d_cell_ldof;     // tile-scatter layout
+  int ntiles = 0, max_tile_dofs = 0, tile_cells = 0;
+  std::mutex mu;
+};
+
+// ----------------------------------------------------------------------- matrices ---
+struct MatrixT {
+  bool csr = false;
+  uint8_t dtype = 1;
+  size_t rows = 0, cols = 0;
+  std::vector<unsigned char> data;
+  std::vector<uintptr_t> indices, indptr;
+};
+
+// --------------------------------------------------------------------- assemblers ---
+struct BoundaryAssemblerT {
+  int kernel = bempp_b200::kLaplace;
+  int op = bempp_b200::kSL;
+  double k = 0.0;
+  uint8_t dtype = 1;
+  bempp_b200::Options options;
+  bool timing = false;
+  std::vector<double> phase_ms;
+  size_t launches = 0;
+  cudaEvent_t events[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  int events_recorded = 0;
+  DeviceBuffer work;     // device output for host-memory assembly
+  DeviceBuffer convert;  // FP64 staging for F32 / C32 outputs
+  DeviceBuffer pair_values;
+  std::mutex mu;
+  ~BoundaryAssemblerT();
+};
+
+
+namespace bempp_b200 {
+
+SpaceT* make_space(GridT* grid, const ElementFamilyT& fam);
+// greedy colouring as src/function.rs:281-351 (exposed for tests of the host logic)
+std::vector<std::vector<int64_t>> cell_colouring(const SpaceT& s);
+
+size_t dtype_size(uint8_t dtype);
+
+// Dense assembly into device memory (column-major, assembler dtype) on `stream`.
+void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d_out,
+                     cudaStream_t stream);
+// Singular part as CSR (host).
+MatrixT* assemble_singular_csr(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test);
+
+}  // namespace bempp_b200

@@ -1,0 +1,184 @@
+// Grid topology, DOF maps and the host-side layouts the kernels consume.
+//
+//   make_space:      DOF numbering of Lagrange degree 0/1 spaces exactly as bempp-rs
+//                    assign_dofs (src/function.rs:365-445): cells in order, sub-entities
+//                    of each dimension in local order, the first visit allocates DOFs.
+//   cell_colouring:  greedy colouring of src/function.rs:281-351 (kept for API parity
+//                    and tests; the GPU kernels do not need it).
+//   singular pairs:  make_cell_blocks + get_pairs_if_smallest
+//                    (src/boundary_assemblers.rs:564-606,775-792): each ordered pair of
+//                    cells sharing a vertex, once, with its (test_local, trial_local)
+//                    vertex pairing mapped to one of the 28 configurations.
+//   tiles:           the DOFs touched by each run of 32 consecutive cells, for the
+//                    tile-scatter kernel.
+#include <algorithm>
+#include <cstring>
+
+#include "core.h"
+
+void GridT::build_topology() {
+  if (!vertex_cells.empty() || ncells == 0) return;
+  vertex_cells.assign(npoints, {});
+  for (int64_t c = 0; c < ncells; ++c)
+    for (int i = 0; i < 3; ++i) vertex_cells[cells[3 * c + i]].push_back(static_cast<int>(c));
+  // edges: numbered in first-visit order over cells and local edges [1,2], [0,2], [0,1]
+  std::map<std::pair<int, int>, int> index;
+  cell_edges.resize(ncells);
+  const int local[3][2] = {{1, 2}, {0, 2}, {0, 1}};
+  for (int64_t c = 0; c < ncells; ++c)
+    for (int e = 0; e < 3; ++e) {
+      int a = cells[3 * c + local[e][0]], b = cells[3 * c + local[e][1]];
+      auto key = std::make_pair(std::min(a, b), std::max(a, b));
+      auto it = index.find(key);
+      if (it == index.end()) {
+        it = index.emplace(key, static_cast<int>(edges.size())).first;
+        edges.push_back(key);
+      }
+      cell_edges[c][e] = it->second;
+    }
+}
+
+namespace bempp_b200 {
+
+SpaceT* make_space(GridT* grid, const ElementFamilyT& fam) {
+  if (fam.degree > 1)
+    throw Error(kUnsupported, "only Lagrange degree 0 and 1 spaces are supported");
+  std::lock_guard<std::mutex> lock(grid->mu);
+  grid->build_topology();
+  auto* s = new SpaceT();
+  s->grid = grid;
+  s->degree = fam.degree;
+  s->continuous = fam.continuity == 0 && fam.degree >= 1;
+  s->dtype = fam.dtype;
+  const int64_t nc = grid->ncells;
+  s->entity_dofs[0].assign(grid->npoints, {});
+  s->entity_dofs[1].assign(grid->edges.size(), {});
+  s->entity_dofs[2].assign(nc, {});
+  if (fam.degree == 0) {
+    // DP0: one DOF on the cell itself (Lagrange degree 0 is discontinuous)
+    s->nbasis = 1;
+    s->cell_dofs.resize(nc);
+    for (int64_t c = 0; c < nc; ++c) {
+      s->cell_dofs[c] = c;
+      s->entity_dofs[2][c] = {c};
+    }
+    s->ndofs = nc;
+  } else if (s->continuous) {
+    s->nbasis = 3;
+    s->cell_dofs.resize(3 * nc);
+    int64_t size = 0;
+    for (int64_t c = 0; c < nc; ++c)
+      for (int i = 0; i < 3; ++i) {
+        auto& ed = s->entity_dofs[0][grid->cells[3 * c + i]];
+        if (ed.empty()) ed.push_back(size++);
+        s->cell_dofs[3 * c + i] = ed[0];
+      }
+    s->ndofs = size;
+  } else {
+    // DP1: all three DOFs belong to the cell interior
+    s->nbasis = 3;
+    s->cell_dofs.resize(3 * nc);
+    for (int64_t c = 0; c < nc; ++c) {
+      for (int i = 0; i < 3; ++i) s->cell_dofs[3 * c + i] = 3 * c + i;
+      s->entity_dofs[2][c] = {3 * c, 3 * c + 1, 3 * c + 2};
+    }
+    s->ndofs = 3 * nc;
+  }
+  return s;
+}
+
+std::vector<std::vector<int64_t>> cell_colouring(const SpaceT& s) {
+  const GridT& g = *s.grid;
+  const bool vertex_based = s.continuous;
+  std::vector<std::vector<int64_t>> colours;
+  std::vector<std::vector<int>> entity_colours(vertex_based ? g.npoints : g.ncells);
+  for (int64_t c = 0; c < g.ncells; ++c) {
+    int ents[3];
+    int ne = 0;
+    if (vertex_based)
+      for (int i = 0; i < 3; ++i) ents[ne++] = g.cells[3 * c + i];
+    else
+      ents[ne++] = static_cast<int>(c);
+    int col = 0;
+    for (; col < static_cast<int>(colours.size()); ++col) {
+      bool used = false;
+      for (int e = 0; e < ne && !used; ++e)
+        used = std::find(entity_colours[ents[e]].begin(), entity_colours[ents[e]].end(), col) !=
+               entity_colours[ents[e]].end();
+      if (!used) break;
+    }
+    if (col == static_cast<int>(colours.size())) colours.emplace_back();
+    colours[col].push_back(c);
+    for (int e = 0; e < ne; ++e) entity_colours[ents[e]].push_back(col);
+  }
+  return colours;
+}
+
+// Singular pair enumeration; pairs grouped by configuration (as cell_pairs[config] in
+// make_cell_blocks), vertices visited in increasing order.
+void build_singular_pairs(GridT& g, SingularPairList& out) {
+  const auto& cfgs = singular_configurations();
+  std::vector<std::vector<std::pair<int, int>>> by_cfg(cfgs.size());
+  std::vector<std::pair<int, int>> pairs;
+  for (int64_t v = 0; v < g.npoints; ++v)
+    for (int tc : g.vertex_cells[v])
+      for (int sc : g.vertex_cells[v]) {
+        pairs.clear();
+        bool smallest = true;
+        for (int si = 0; si < 3 && smallest; ++si)
+          for (int ti = 0; ti < 3; ++ti)
+            if (g.cells[3 * tc + ti] == g.cells[3 * sc + si]) {
+              if (g.cells[3 * tc + ti] < v) {
+                smallest = false;
+                break;
+              }
+              pairs.push_back({ti, si});
+            }
+        if (!smallest) continue;
+        auto it = std::find(cfgs.begin(), cfgs.end(), pairs);
+        if (it == cfgs.end()) throw Error(kInternal, "unknown adjacency configuration");
+        by_cfg[it - cfgs.begin()].push_back({tc, sc});
+      }
+  out.test_cell.clear();
+  out.trial_cell.clear();
+  out.config.clear();
+  for (size_t c = 0; c < by_cfg.size(); ++c)
+    for (auto& p : by_cfg[c]) {
+      out.test_cell.push_back(p.first);
+      out.trial_cell.push_back(p.second);
+      out.config.push_back(static_cast<int>(c));
+    }
+}
+
+// Tile layout for the scatter kernel: tiles of `tile` consecutive cells, their sorted
+// unique DOFs, and each cell's DOFs as indices into its tile's list.
+void build_tiles(const SpaceT& s, int tile, std::vector<int>& off, std::vector<int>& dofs,
+                 std::vector<uint8_t>& ldof, int& max_dofs) {
+  const int64_t nc = s.grid->ncells;
+  const int nb = s.nbasis;
+  const int ntiles = static_cast<int>((nc + tile - 1) / tile);
+  off.assign(ntiles + 1, 0);
+  dofs.clear();
+  ldof.assign(nc * nb, 0);
+  max_dofs = 0;
+  std::vector<int> local;
+  for (int t = 0; t < ntiles; ++t) {
+    const int64_t c0 = static_cast<int64_t>(t) * tile, c1 = std::min<int64_t>(c0 + tile, nc);
+    local.clear();
+    for (int64_t c = c0; c < c1; ++c)
+      for (int b = 0; b < nb; ++b) local.push_back(static_cast<int>(s.cell_dofs[c * nb + b]));
+    std::sort(local.begin(), local.end());
+    local.erase(std::unique(local.begin(), local.end()), local.end());
+    for (int64_t c = c0; c < c1; ++c)
+      for (int b = 0; b < nb; ++b) {
+        int d = static_cast<int>(s.cell_dofs[c * nb + b]);
+        ldof[c * nb + b] =
+            static_cast<uint8_t>(std::lower_bound(local.begin(), local.end(), d) - local.begin());
+      }
+    dofs.insert(dofs.end(), local.begin(), local.end());
+    off[t + 1] = static_cast<int>(dofs.size());
+    max_dofs = std::max<int>(max_dofs, static_cast<int>(local.size()));
+  }
+}
+
+}  // namespace bempp_b200

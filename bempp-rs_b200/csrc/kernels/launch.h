@@ -1,0 +1,94 @@
+// Host-side launchers of the assembly kernels (implemented in the .cu files of this
+// directory).  All launches are asynchronous on `stream`; each returns the CUDA error of
+// its launch.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace bempp_b200 {
+
+// Per-cell FP64 geometry, regular quadrature points and vertex ids of a flat-triangle
+// grid (points: npoints x 3 FP64; cells: ncells x 3 int32).
+cudaError_t launch_geometry(const double* points, const int* cells, int ncells,
+                            const RegularRule& rule, double* geom, double* qpts, float* qrel,
+                            int* vids, cudaStream_t stream);
+
+// Arithmetic of the regular far-pair quadrature.
+enum RegularPrecision : int { kRegularFP64 = 0, kRegularMixed = 1 };
+
+// Output element type of a dense matrix.
+enum OutType : int { kOutF64 = 0, kOutC128 = 1, kOutF32 = 2, kOutC64 = 3 };
+
+struct RegularArgs {
+  int kernel;        // KernelKind
+  int op;            // OpKind
+  double k;          // wavenumber (Helmholtz)
+  int same_grid;     // skip vertex-sharing pairs (they belong to the singular part)
+  int precision;     // RegularPrecision
+  int out_type;      // OutType
+  int64_t ld;        // leading dimension = number of test DOFs
+  void* out;         // column-major output
+};
+
+// DP0 test x DP0 trial: every entry is written exactly once (no pre-zeroing needed).
+cudaError_t launch_regular_dp0(const CellSet& test, const CellSet& trial,
+                               const RegularRule& rule, const RegularArgs& a,
+                               cudaStream_t stream);
+
+// DOF layout of a space for the tile-scatter kernel.
+struct SpaceTiles {
+  int nbasis;               // 1 (DP0) or 3 (P1 / DP1)
+  int tile_cells;           // cells per tile
+  int ntiles;
+  int max_tile_dofs;
+  const int* tile_dof_off;  // ntiles + 1
+  const int* tile_dofs;     // global DOF numbers of each tile, ascending
+  const uint8_t* cell_ldof; // ncells * nbasis local (in-tile) DOF indices
+};
+
+// Any pair of spaces: per-tile shared-memory accumulation, then atomic adds into a
+// zero-initialised output.
+cudaError_t launch_regular_scatter(const CellSet& test, const SpaceTiles& ttiles,
+                                   const CellSet& trial, const SpaceTiles& stiles,
+                                   const RegularRule& rule, const RegularArgs& a,
+                                   cudaStream_t stream);
+
+// Singular (Duffy) rules of all 28 adjacency configurations, concatenated.
+struct SingularRules {
+  const int* offset;       // 29 entries: first point of each configuration
+  const double* test_xi;   // 2 * total
+  const double* trial_xi;  // 2 * total
+  const double* w;         // total
+};
+
+// Adjacent cell pairs (test cell, trial cell, configuration), grouped by configuration.
+struct SingularPairs {
+  int npairs;
+  const int* test_cell;
+  const int* trial_cell;
+  const int* config;
+};
+
+struct SingularArgs {
+  int kernel;
+  int op;
+  double k;
+  int out_type;
+  int64_t ld;
+  void* out;          // dense column-major output (added into), or null
+  int unique_entries; // 1 when every pair owns its entries (DP0 x DP0): plain adds
+  double* pair_values;  // if non-null: per-pair local blocks (nbt * nbs [*2 complex])
+};
+
+cudaError_t launch_singular(const CellSet& test, const int* test_dofs, int nbt,
+                            const CellSet& trial, const int* trial_dofs, int nbs,
+                            const SingularRules& rules, const SingularPairs& pairs,
+                            const SingularArgs& a, cudaStream_t stream);
+
+// CUDA-core FMA throughput probe (diag.cu).
+cudaError_t measure_fma_peak(int fp64, int iters, int reps, double* tflops);
+
+}  // namespace bempp_b200

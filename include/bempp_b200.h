@@ -1,0 +1,261 @@
+/*
+ * bempp_b200.h -- C-ABI of the B200 dense boundary-operator assembler.
+ *
+ * Drop-in for the C interface that bempp-rs generates with cbindgen from
+ * the src/bindings/ tree (cbindgen.toml: enums prefixed with their name): every function of
+ * that interface on the dense-assembly path keeps its name, argument order, argument
+ * meaning and ownership rules.  Each declaration cites the reference function it
+ * replaces.  Additions (status-returning variants, device-pointer assembly, precision
+ * selection, timing, batched sweep, adjoint gradient) are marked "Addition".
+ *
+ * Conventions (as in the reference):
+ *   - Opaque heap handles, each released by its *_t_free function (null-safe).
+ *   - Dense outputs are column-major: entry (test dof i, trial dof j) is at
+ *     i + n_test * j (src/boundary_assemblers.rs:766).
+ *   - Functions that return nothing in the reference abort on invalid input there; here
+ *     they record the error (bempp_last_error) and return without writing.  The *_ex
+ *     variants return a status code instead.
+ */
+#ifndef BEMPP_B200_H
+#define BEMPP_B200_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* c-api-tools DType (src/bindings/space.rs:189-198; python/bempp/function_space.py:13-16). */
+enum { DType_F32 = 0, DType_F64 = 1, DType_C32 = 2, DType_C64 = 3 };
+typedef uint8_t DType;
+
+/* ndelement ReferenceCellType (python/bempp/function_space.py:23-35). */
+enum {
+  ReferenceCellType_Point = 0,
+  ReferenceCellType_Interval = 1,
+  ReferenceCellType_Triangle = 2,
+  ReferenceCellType_Quadrilateral = 3,
+  ReferenceCellType_Tetrahedron = 4,
+  ReferenceCellType_Hexahedron = 5,
+  ReferenceCellType_Prism = 6,
+  ReferenceCellType_Pyramid = 7
+};
+typedef uint8_t ReferenceCellType;
+
+/* ndelement Continuity (src/bindings/ndelement.rs:19-25). */
+enum { Continuity_Standard = 0, Continuity_Discontinuous = 1 };
+typedef uint8_t Continuity;
+
+/* src/bindings/boundary_assemblers.rs:15-24 */
+enum {
+  OperatorType_SingleLayer = 0,
+  OperatorType_DoubleLayer = 1,
+  OperatorType_AdjointDoubleLayer = 2,
+  OperatorType_Hypersingular = 3,
+  OperatorType_ElectricField = 4,
+  OperatorType_MagneticField = 5
+};
+typedef uint8_t OperatorType;
+
+/* Addition: arithmetic of the regular far-pair quadrature.  Precision_FP64 computes
+ * everything in FP64 (the reference's f64/c64 semantics).  Precision_Mixed computes
+ * regular pairs whose centroid distance is at least two element diameters in FP32
+ * with compensated accumulation; geometry, near pairs and singular pairs stay FP64. */
+enum { Precision_FP64 = 0, Precision_Mixed = 1 };
+typedef uint8_t Precision;
+
+/* Addition: status codes of the *_ex functions. */
+enum {
+  BemppStatus_Ok = 0,
+  BemppStatus_InvalidArgument = 1,
+  BemppStatus_Unsupported = 2,
+  BemppStatus_OutOfMemory = 3,
+  BemppStatus_CudaError = 4,
+  BemppStatus_NoDevice = 5,
+  BemppStatus_Internal = 6
+};
+typedef int32_t BemppStatus;
+
+typedef struct BoundaryAssemblerOptionsT BoundaryAssemblerOptionsT;
+typedef struct BoundaryAssemblerT BoundaryAssemblerT;
+typedef struct MatrixT MatrixT;
+typedef struct SpaceT SpaceT;
+typedef struct GridT GridT;
+typedef struct ElementFamilyT ElementFamilyT;
+
+/* Addition: message of the last error on this thread ("" if none). */
+const char *bempp_last_error(void);
+
+/* ------------------------------------------------------------------ options ----- */
+/* src/bindings/boundary_assemblers.rs:34-40 */
+BoundaryAssemblerOptionsT *boundary_assembler_options_new(void);
+/* src/bindings/boundary_assemblers.rs:42-50 (null-safe) */
+void boundary_assembler_options_t_free(BoundaryAssemblerOptionsT *ptr);
+/* src/bindings/boundary_assemblers.rs:52-60 (only changes an existing cell type) */
+void boundary_assembler_options_set_regular_quadrature_degree(
+    BoundaryAssemblerOptionsT *options, ReferenceCellType cell_type, size_t npoints);
+/* src/bindings/boundary_assemblers.rs:61-68 (returns 0 and records an error if absent) */
+size_t boundary_assembler_options_get_regular_quadrature_degree(
+    BoundaryAssemblerOptionsT *options, ReferenceCellType cell_type);
+/* src/bindings/boundary_assemblers.rs:69-76 */
+bool boundary_assembler_options_has_regular_quadrature_degree(
+    BoundaryAssemblerOptionsT *options, ReferenceCellType cell_type);
+/* src/bindings/boundary_assemblers.rs:78-87 */
+void boundary_assembler_options_set_singular_quadrature_degree(
+    BoundaryAssemblerOptionsT *options, ReferenceCellType cell_type0,
+    ReferenceCellType cell_type1, size_t npoints);
+/* src/bindings/boundary_assemblers.rs:88-98 */
+size_t boundary_assembler_options_get_singular_quadrature_degree(
+    BoundaryAssemblerOptionsT *options, ReferenceCellType cell_type0,
+    ReferenceCellType cell_type1);
+/* src/bindings/boundary_assemblers.rs:99-109 */
+bool boundary_assembler_options_has_singular_quadrature_degree(
+    BoundaryAssemblerOptionsT *options, ReferenceCellType cell_type0,
+    ReferenceCellType cell_type1);
+/* src/bindings/boundary_assemblers.rs:111-118 */
+void boundary_assembler_options_set_batch_size(BoundaryAssemblerOptionsT *options,
+                                               size_t batch_size);
+/* src/bindings/boundary_assemblers.rs:119-125 */
+size_t boundary_assembler_options_get_batch_size(BoundaryAssemblerOptionsT *options);
+/* Addition: precision of the regular far-pair quadrature (default Precision_FP64). */
+void boundary_assembler_options_set_precision(BoundaryAssemblerOptionsT *options,
+                                              Precision precision);
+Precision boundary_assembler_options_get_precision(BoundaryAssemblerOptionsT *options);
+
+/* --------------------------------------------------------------- assemblers ----- */
+/* src/bindings/boundary_assemblers.rs:127-166 (F32 or F64) */
+BoundaryAssemblerT *laplace_boundary_assembler_new(const BoundaryAssemblerOptionsT *options,
+                                                   OperatorType operator_type, DType dtype);
+/* src/bindings/boundary_assemblers.rs:168-210 (C32 or C64; k points to a float for C32
+ * and a double for C64, as T::Real there) */
+BoundaryAssemblerT *helmholtz_boundary_assembler_new(const void *k,
+                                                     const BoundaryAssemblerOptionsT *options,
+                                                     OperatorType operator_type, DType dtype);
+/* src/bindings/boundary_assemblers.rs:26-27 (#[cfuncs(name = "boundary_assembler_t", free)]) */
+void boundary_assembler_t_free(BoundaryAssemblerT *ptr);
+/* src/bindings/boundary_assemblers.rs:212-233 */
+DType boundary_assembler_dtype(BoundaryAssemblerT *assembler);
+/* src/bindings/boundary_assemblers.rs:272-307: owned dense MatrixT (column-major) */
+MatrixT *boundary_assembler_assemble(BoundaryAssemblerT *assembler, SpaceT *trial_space,
+                                     SpaceT *test_space);
+/* src/bindings/boundary_assemblers.rs:235-270: singular part as an owned CSR MatrixT */
+MatrixT *boundary_assembler_assemble_singular(BoundaryAssemblerT *assembler,
+                                              SpaceT *trial_space, SpaceT *test_space);
+/* src/bindings/boundary_assemblers.rs:309-348: dense assembly into caller memory holding
+ * n_test * n_trial elements of the assembler's dtype, column-major (host memory). */
+void boundary_assembler_assemble_into_memory(BoundaryAssemblerT *assembler,
+                                             SpaceT *trial_space, SpaceT *test_space,
+                                             void *data);
+/* Addition: as boundary_assembler_assemble_into_memory, with a status code. */
+BemppStatus boundary_assembler_assemble_into_memory_ex(BoundaryAssemblerT *assembler,
+                                                       SpaceT *trial_space,
+                                                       SpaceT *test_space, void *data);
+/* Addition: dense assembly into device memory on the current CUDA device, enqueued on
+ * `stream` (a cudaStream_t; NULL = legacy default stream).  Returns after enqueueing;
+ * the matrix is complete when the stream reaches that point. */
+BemppStatus boundary_assembler_assemble_into_device(BoundaryAssemblerT *assembler,
+                                                    SpaceT *trial_space, SpaceT *test_space,
+                                                    void *device_data, void *stream);
+/* Addition: record CUDA events around each phase of the next assemblies and read the
+ * last durations in milliseconds: [geometry, output clear, regular, singular (+ final
+ * conversion)]; returns the number of phases written (at most n).  Reading waits for
+ * the last assembly to finish. */
+void boundary_assembler_set_timing(BoundaryAssemblerT *assembler, bool enabled);
+size_t boundary_assembler_phase_times(BoundaryAssemblerT *assembler, double *ms, size_t n);
+/* Addition: number of kernel launches the last assembly enqueued. */
+size_t boundary_assembler_last_launch_count(BoundaryAssemblerT *assembler);
+/* Addition: measured CUDA-core fused multiply-add throughput of the current device in
+ * TFLOP/s (fp64 != 0: FP64, else FP32), the roofline denominator of the regular
+ * quadrature kernels. */
+BemppStatus bempp_measure_fma_peak(int fp64, int iters, int reps, double *tflops);
+
+/* ------------------------------------------------------------------ matrices ----- */
+/* src/bindings/matrices.rs:6-20 */
+size_t matrix_shape0(MatrixT *matrix);
+size_t matrix_shape1(MatrixT *matrix);
+/* src/bindings/matrices.rs:29-49 (dense only) */
+const void *matrix_dense_data(MatrixT *matrix);
+void matrix_dense_data_copy(MatrixT *matrix, void *data);
+/* src/bindings/matrices.rs:57-137 (CSR only; indices and indptr are uintptr_t) */
+size_t matrix_csr_data_size(MatrixT *matrix);
+const void *matrix_csr_data(MatrixT *matrix);
+void matrix_csr_data_copy(MatrixT *matrix, void *data);
+size_t matrix_csr_indices_size(MatrixT *matrix);
+const uintptr_t *matrix_csr_indices(MatrixT *matrix);
+void matrix_csr_indices_copy(MatrixT *matrix, uintptr_t *indices);
+size_t matrix_csr_indptr_size(MatrixT *matrix);
+const uintptr_t *matrix_csr_indptr(MatrixT *matrix);
+void matrix_csr_indptr_copy(MatrixT *matrix, uintptr_t *indptr);
+/* src/bindings.rs:13-14 (#[cfuncs(name = "matrix_t", free)]) */
+void matrix_t_free(MatrixT *ptr);
+/* Addition: DType of a matrix, and whether it is CSR (true) or dense (false). */
+DType matrix_dtype(MatrixT *matrix);
+bool matrix_is_csr(MatrixT *matrix);
+
+/* -------------------------------------------------------------------- spaces ----- */
+/* src/bindings/space.rs:20-42 */
+SpaceT *function_space(GridT *grid, ElementFamilyT *e_family);
+/* src/bindings/space.rs:17-18 (#[cfuncs(name = "space_t", free)]) */
+void space_t_free(SpaceT *ptr);
+/* src/bindings/space.rs:44-56 (a serial space is its own local space) */
+SpaceT *space_local_space(SpaceT *space);
+/* src/bindings/space.rs:58-67 */
+bool space_is_serial(SpaceT *space);
+/* src/bindings/space.rs:69-106 */
+size_t space_get_local_dof_numbers_size(SpaceT *space, size_t entity_dim,
+                                        size_t entity_number);
+void space_get_local_dof_numbers(SpaceT *space, size_t entity_dim, size_t entity_number,
+                                 uintptr_t *dofs);
+/* src/bindings/space.rs:108-128 */
+size_t space_local_size(SpaceT *space);
+size_t space_global_size(SpaceT *space);
+/* src/bindings/space.rs:130-165 */
+bool space_has_cell_dofs(SpaceT *space, size_t cell);
+size_t space_cell_dofs_size(SpaceT *space, size_t cell);
+void space_cell_dofs(SpaceT *space, size_t cell, uintptr_t *dofs);
+/* src/bindings/space.rs:167-187 */
+size_t space_global_dof_index(SpaceT *space, size_t local_dof_index);
+bool space_is_owned(SpaceT *space, size_t local_dof_index);
+/* python/bempp/function_space.py:95-102 (ghost owner; serial spaces own every DOF) */
+size_t space_ownership_process(SpaceT *space, size_t local_dof_index);
+size_t space_ownership_index(SpaceT *space, size_t local_dof_index);
+/* src/bindings/space.rs:189-198 */
+DType space_dtype(SpaceT *space);
+
+/* ---------------------------------------------------------- grids, elements ----- */
+/* src/bindings/ndgrid.rs:18-56: ndgrid's borrowed single-element grid.  The topology
+ * arrays are accepted for signature compatibility; the grid is rebuilt from `points`
+ * (npoints x gdim, DType_F32 or DType_F64) and `cells` (ncells x points_per_cell point
+ * indices, the first three being the triangle's vertices). */
+GridT *single_element_grid_borrowed_create_bempp(
+    size_t tdim, const size_t *id_sizes, const size_t *const *id_pointers,
+    const ReferenceCellType *entity_types, const size_t *entity_counts,
+    const size_t *const *const *downward_connectivity,
+    const size_t *const *downward_connectivity_shape0,
+    const size_t *const *const *const *upward_connectivity,
+    const size_t *const *const *upward_connectivity_lens, const void *points, size_t gdim,
+    size_t npoints, DType dtype, const size_t *cells, size_t points_per_cell, size_t ncells,
+    size_t geometry_degree);
+/* Addition: flat-triangle grid from points (npoints x 3) and cells (ncells x 3). */
+GridT *bempp_grid_from_points_cells(const void *points, size_t npoints, DType dtype,
+                                    const size_t *cells, size_t ncells);
+/* src/bindings/ndgrid.rs:6-16 (null-safe) */
+void grid_t_free_bempp(GridT *ptr);
+/* src/bindings/ndelement.rs:18-25: Lagrange degree 0 or 1 on triangles */
+ElementFamilyT *create_lagrange_family_bempp(size_t degree, Continuity continuity,
+                                             DType dtype);
+/* src/bindings/ndelement.rs:27-43: not supported (returns NULL, records an error) */
+ElementFamilyT *create_raviart_thomas_family_bempp(size_t degree, Continuity continuity,
+                                                   DType dtype);
+ElementFamilyT *create_nedelec_family_bempp(size_t degree, Continuity continuity,
+                                            DType dtype);
+/* src/bindings/ndelement.rs:9-19 (null-safe) */
+void element_family_t_free_bempp(ElementFamilyT *ptr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BEMPP_B200_H */

