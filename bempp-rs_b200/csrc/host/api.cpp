@@ -12,6 +12,10 @@
 
 using namespace bempp_b200;
 
+namespace bempp_b200 {
+void build_singular_pairs(GridT& g, SingularPairList& out);
+}
+
 struct BoundaryAssemblerOptionsT {
   Options options;
 };
@@ -504,5 +508,58 @@ ElementFamilyT* create_nedelec_family_bempp(size_t, Continuity, DType) {
 }
 
 void element_family_t_free_bempp(ElementFamilyT* ptr) { delete ptr; }
+
+// -------------------------------------------------------------------- inspection ---
+size_t bempp_regular_rule(size_t npoints, double* points, double* weights) {
+  size_t n = 0;
+  guarded([&] {
+    if (!has_simplex_rule(static_cast<int>(npoints))) return;
+    RegularRule r = simplex_rule(static_cast<int>(npoints));
+    for (int i = 0; i < r.npts; ++i) {
+      if (points) {
+        points[2 * i] = r.xi[2 * i];
+        points[2 * i + 1] = r.xi[2 * i + 1];
+      }
+      if (weights) weights[i] = r.w[i];
+    }
+    n = static_cast<size_t>(r.npts);
+  });
+  return n;
+}
+
+size_t bempp_singular_rule(size_t config, size_t order, double* test_points,
+                           double* trial_points, double* weights) {
+  size_t n = 0;
+  guarded([&] {
+    DuffyRule r = duffy_rule(static_cast<int>(config), static_cast<int>(order));
+    n = r.w.size();
+    if (test_points) std::memcpy(test_points, r.test_xi.data(), r.test_xi.size() * sizeof(double));
+    if (trial_points)
+      std::memcpy(trial_points, r.trial_xi.data(), r.trial_xi.size() * sizeof(double));
+    if (weights) std::memcpy(weights, r.w.data(), r.w.size() * sizeof(double));
+  });
+  return n;
+}
+
+size_t bempp_grid_singular_pairs(GridT* grid, size_t* test_cells, size_t* trial_cells,
+                                 size_t* configs) {
+  size_t n = 0;
+  guarded([&] {
+    require(grid, "grid");
+    SingularPairList pl;
+    {
+      std::lock_guard<std::mutex> lock(grid->mu);
+      grid->build_topology();
+      build_singular_pairs(*grid, pl);
+    }
+    n = pl.test_cell.size();
+    for (size_t i = 0; i < n; ++i) {
+      if (test_cells) test_cells[i] = static_cast<size_t>(pl.test_cell[i]);
+      if (trial_cells) trial_cells[i] = static_cast<size_t>(pl.trial_cell[i]);
+      if (configs) configs[i] = static_cast<size_t>(pl.config[i]);
+    }
+  });
+  return n;
+}
 
 }  // extern "C"

@@ -79,6 +79,15 @@ RegularRule simplex_rule(int npoints) {
       r.w[i] = e.weights[i];
       r.xi[2 * i] = e.points[2 * i];
       r.xi[2 * i + 1] = e.points[2 * i + 1];
+      r.wf[i] = static_cast<float>(e.weights[i]);
+      r.uf[i] = static_cast<float>(e.points[2 * i] - 1.0 / 3.0);
+      r.vf[i] = static_cast<float>(e.points[2 * i + 1] - 1.0 / 3.0);
+      const double x = e.points[2 * i], y = e.points[2 * i + 1];
+      const double phi[3] = {1.0 - x - y, x, y};
+      for (int b = 0; b < 3; ++b) {
+        r.phi[b][i] = phi[b];
+        r.phif[b][i] = static_cast<float>(phi[b]);
+      }
     }
     return r;
   }

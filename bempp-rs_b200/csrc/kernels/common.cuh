@@ -34,6 +34,14 @@ struct RegularRule {
   int npts;
   double w[kMaxRegularPoints];
   double xi[2 * kMaxRegularPoints];
+  // FP32 copies for the mixed-precision kernels: weights, and the point offsets from
+  // the centroid in reference coordinates, (u, v) = xi - (1/3, 1/3).
+  float wf[kMaxRegularPoints];
+  float uf[kMaxRegularPoints];
+  float vf[kMaxRegularPoints];
+  // P1 basis values phi_b(xi_q) = (1 - x - y, x, y) at each point, FP64 and FP32
+  double phi[3][kMaxRegularPoints];
+  float phif[3][kMaxRegularPoints];
 };
 
 struct CellSet {
@@ -60,6 +68,18 @@ __device__ __forceinline__ double g(const double* geom, int field, int n, int c)
 __device__ __forceinline__ bool share_vertex(int a0, int a1, int a2, int b0, int b1, int b2) {
   return a0 == b0 || a0 == b1 || a0 == b2 || a1 == b0 || a1 == b1 || a1 == b2 || a2 == b0 ||
          a2 == b1 || a2 == b2;
+}
+
+// 1/sqrt(a) for normal positive FP64 a without a special-case branch: the hardware
+// approximation rsqrt.approx.ftz.f64 (PTX) refined by one step of the binomial series
+// (1 - e)^(-1/2) = 1 + e/2 + 3e^2/8 + O(e^3) with e = 1 - a y^2, which cubes the
+// relative error of the seed.  Only used for distances between distinct quadrature
+// points (a > 0, far from the subnormal range).
+__device__ __forceinline__ double rsqrt_refined(double a) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+  const double e = fma(-a * y, y, 1.0);
+  return fma(y * e, fma(e, 0.375, 0.5), y);
 }
 
 // P1 basis on the reference triangle: phi0 = 1 - x - y, phi1 = x, phi2 = y.

@@ -1,13 +1,21 @@
 """Benchmark: dense boundary-operator assembly on B200.
 
-Workload (default): Laplace double-layer, adjoint double-layer and hypersingular
-operators, continuous P1 trial and test spaces, f64, on the unit icosphere refined 5
-times (20,480 flat triangles, 10,242 vertices) with a seeded radial perturbation
-U(-0.02, 0.02) (numpy default_rng(20480)); regular pairs use the 6-point symmetric rule,
-singular pairs order-4 Duffy rules.  One step assembles all three 10,242 x 10,242
-matrices (314.7 M entries).  The metric is dense entries per second.
+Headline workload (default, ``--workload p1``): Laplace double-layer, adjoint
+double-layer and hypersingular operators, continuous P1 trial and test spaces, f64, on
+the unit icosphere refined 5 times (20,480 flat triangles, 10,242 vertices) with a seeded
+radial perturbation U(-0.02, 0.02) (numpy default_rng(20480)); regular pairs use the
+6-point symmetric rule, singular pairs order-4 Duffy rules.  One step assembles all three
+10,242 x 10,242 matrices (314.7 M entries).  The metric is dense entries per second.
+
+Other workloads: ``helmholtz_sl`` (Helmholtz single layer, k = 8, DP0, complex128, same
+perturbed 20,480-triangle sphere, 419 M entries) and ``laplace_sl`` (Laplace single layer,
+DP0, f64, 1,280-triangle icosphere).  The default run also measures the Helmholtz
+single-layer FP64 and mixed-precision assemblies and reports their speed ratio and the
+mixed result's relative Frobenius error against the FP64 result (``north_star`` key).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload p1|helmholtz_sl|laplace_sl] [--precision fp64|mixed]
+                  [--level L] [--once]
 
 value: device-resident assembly (geometry cached, output in HBM), max over ranks.
 e2e:   the same step through the C-ABI host path a user calls (grid and spaces built
@@ -15,6 +23,7 @@ e2e:   the same step through the C-ABI host path a user calls (grid and spaces b
 --impl reference: the CPU FP64 oracle (a restatement of the bempp-rs algorithm, which
        cannot be compiled here: no Rust toolchain) timed on a bounded sample of the same
        workload on all host cores.
+--once: assemble each operator once and exit (the command used under ncu).
 Multi-GPU (torchrun): every rank assembles its own copy of the workload (weak scaling,
 no collective on the data path).
 """
@@ -38,22 +47,43 @@ for _p in (ROOT, PKG):
 
 import numpy as np  # noqa: E402
 
-LEVEL = 5
-SEED = 20480
 Q_REGULAR = 6
 ORDER = 4
-OPERATORS = ["double_layer", "adjoint_double_layer", "hypersingular"]
-# Algorithmic FLOPs per regular P1 x P1 cell pair at Q = 6 (36 point pairs): kernel +
-# factorised basis accumulation, transcendental = 1, per-cell constants hoisted.
-FLOPS_PER_PAIR = {"double_layer": 990, "adjoint_double_layer": 990, "hypersingular": 459}
-METRIC = "dense entries/s (Laplace DL+ADL+HS, P1, f64, 20480-triangle icosphere)"
+SEED = 20480
+
+# Algorithmic FLOPs per regular cell pair at Q = 6 (36 point pairs): kernel evaluation
+# plus basis accumulation, transcendental functions counted as 1, per-cell constants
+# hoisted (P1 x P1 uses the factorised sum U_b(p) = sum_q K psi_b w_q).
+FLOPS_PER_PAIR = {
+    ("laplace", "single_layer", "dp0"): 396,
+    ("laplace", "double_layer", "p1"): 990,
+    ("laplace", "adjoint_double_layer", "p1"): 990,
+    ("laplace", "hypersingular", "p1"): 459,
+    ("helmholtz", "single_layer", "dp0"): 720,
+}
+
+WORKLOADS = {
+    "p1": dict(name="laplace_dl_adl_hs_p1_ico5_f64", kernel="laplace", space="p1", level=5,
+               perturb=True, k=0.0,
+               ops=["double_layer", "adjoint_double_layer", "hypersingular"],
+               metric="dense entries/s (Laplace DL+ADL+HS, P1, f64, 20480-triangle icosphere)"),
+    "helmholtz_sl": dict(name="helmholtz_sl_dp0_ico5_k8_c128", kernel="helmholtz", space="dp0",
+                         level=5, perturb=True, k=8.0, ops=["single_layer"],
+                         metric="dense entries/s (Helmholtz SL k=8, DP0, c128, 20480-triangle "
+                                "icosphere)"),
+    "laplace_sl": dict(name="laplace_sl_dp0_ico3_f64", kernel="laplace", space="dp0", level=3,
+                       perturb=False, k=0.0, ops=["single_layer"],
+                       metric="dense entries/s (Laplace SL, DP0, f64, 1280-triangle icosphere)"),
+}
 
 
-def workload_mesh():
+def workload_mesh(w, level=None):
     from bempp import shapes
 
-    pts, cells = shapes.icosphere(LEVEL)
-    return shapes.radial_perturbation(pts, SEED), cells
+    pts, cells = shapes.icosphere(w["level"] if level is None else level)
+    if w["perturb"]:
+        pts = shapes.radial_perturbation(pts, SEED)
+    return pts, cells
 
 
 def dist_env():
@@ -121,186 +151,39 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_spaces(points, cells):
+def build_space(points, cells, space):
     from bempp.function_space import function_space
     from ndelement.ciarlet import Continuity, Family, create_family
     from ndgrid.grid import Grid
 
     grid = Grid(points, cells)
-    p1 = function_space(grid, create_family(Family.Lagrange, 1, Continuity.Standard))
-    return grid, p1
+    if space == "p1":
+        fam = create_family(Family.Lagrange, 1, Continuity.Standard)
+    else:
+        fam = create_family(Family.Lagrange, 0, Continuity.Discontinuous)
+    return grid, function_space(grid, fam)
 
 
-def make_assemblers(precision_name="FP64"):
+def make_assemblers(w, precision="fp64"):
     from bempp.assembly.boundary import (BoundaryAssemblerOptions, OperatorType, Precision,
-                                         create_laplace_assembler)
+                                         create_helmholtz_assembler, create_laplace_assembler)
     from ndelement.reference_cell import ReferenceCellType
 
-    ops = {"double_layer": OperatorType.DoubleLayer,
+    ops = {"single_layer": OperatorType.SingleLayer, "double_layer": OperatorType.DoubleLayer,
            "adjoint_double_layer": OperatorType.AdjointDoubleLayer,
            "hypersingular": OperatorType.Hypersingular}
     out = []
-    for name in OPERATORS:
+    for name in w["ops"]:
         o = BoundaryAssemblerOptions()
         o.set_regular_quadrature_degree(ReferenceCellType.Triangle, Q_REGULAR)
         o.set_singular_quadrature_degree(ReferenceCellType.Triangle, ReferenceCellType.Triangle,
                                          ORDER)
-        o.set_precision(getattr(Precision, precision_name))
-        out.append((name, create_laplace_assembler(ops[name], o)))
+        o.set_precision(Precision.Mixed if precision == "mixed" else Precision.FP64)
+        if w["kernel"] == "laplace":
+            out.append((name, create_laplace_assembler(ops[name], o)))
+        else:
+            out.append((name, create_helmholtz_assembler(ops[name], w["k"], o)))
     return out
-
-
-def run_ours(args):
-    import torch
-
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-
-            dist.barrier()
-
-    from bempp import _lib
-
-    points, cells = workload_mesh()
-    grid, space = build_spaces(points, cells)
-    n = space.global_size
-    assemblers = make_assemblers("FP64")
-    outs = [torch.empty((n, n), dtype=torch.float64, device="cuda") for _ in assemblers]
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    stream = torch.cuda.current_stream().cuda_stream
-
-    def step(timing=False):
-        launches = 0
-        for (name, a), out in zip(assemblers, outs):
-            a.set_timing(timing)
-            a.assemble_into_device(space, space, out, stream)
-            launches += a.launch_count()
-        flush.fill_(1.0)  # L2 flush between steps (256 MiB > 126 MB L2)
-        return launches + 1
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-
-    # kernel-level timing of the regular (dominant) kernel, live, on the same stream
-    regular_ms = {}
-    for name, a in assemblers:
-        a.set_timing(True)
-    step(timing=True)
-    torch.cuda.synchronize()
-    for name, a in assemblers:
-        ph = a.phase_times()  # geometry, clear, regular, singular
-        regular_ms[name] = ph[2] if len(ph) > 2 else float("nan")
-        a.set_timing(False)
-
-    sampler = ClockSampler(local)
-    sampler.start()
-    time.sleep(0.3)
-    barrier()
-    torch.cuda.synchronize()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    t0.record()
-    launches = 0
-    for _ in range(args.steps):
-        launches += step()
-    t1.record()
-    torch.cuda.synchronize()
-    barrier()
-    clocks = sampler.stop()
-    ms = t0.elapsed_time(t1)
-    if world > 1:
-        import torch.distributed as dist
-
-        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-    ms_per_step = ms / args.steps
-    entries_per_step = len(assemblers) * n * n
-    value = world * entries_per_step / (ms_per_step * 1e-3)
-
-    # end-to-end through the public API with host buffers (one replica per rank)
-    e2e = None
-    if not args.skip_e2e:
-        torch.cuda.synchronize()
-        pts_h = np.ascontiguousarray(points)
-        cells_h = np.ascontiguousarray(cells)
-        e2e_steps = max(1, min(args.steps, 3))
-        barrier()
-        t = time.perf_counter()
-        for _ in range(e2e_steps):
-            g2, s2 = build_spaces(pts_h, cells_h)
-            for name, a in assemblers:
-                a.assemble(s2, s2)
-            del s2, g2
-        e2e_s = (time.perf_counter() - t) / e2e_steps
-        if world > 1:
-            import torch.distributed as dist
-
-            tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_s = float(tt.item())
-        e2e = {"value": world * entries_per_step / e2e_s, "unit": "entries/s",
-               "h2d_bytes_per_step": int(pts_h.nbytes + cells_h.astype(np.uintp).nbytes),
-               "d2h_bytes_per_step": int(entries_per_step * 8),
-               "ms_per_step": e2e_s * 1e3,
-               "path": "function_space(grid) + BoundaryAssembler.assemble x3 (C-ABI "
-                       "boundary_assembler_assemble_into_memory, host numpy output)"}
-
-    # roofline of the dominant kernel (regular tile-scatter kernel, FP64 CUDA cores)
-    peak = ctypes_peak(_lib)
-    from bempp._lib import ffi as _ffi  # noqa: F401
-
-    nsing = singular_pair_count(cells)
-    nregular = len(cells) ** 2 - nsing
-    achieved = {k: FLOPS_PER_PAIR[k] * nregular / (v * 1e-3) / 1e12 for k, v in regular_ms.items()}
-    dl = "double_layer"
-    roofline = {
-        "bound": "fp64",
-        "kernel": "regular_scatter_fp64 (Laplace double layer, P1 x P1)",
-        "achieved": achieved[dl], "peak": peak, "unit": "TFLOP/s",
-        "frac": achieved[dl] / peak if peak else None,
-        "traffic": None,
-        "peak_source": "measured FP64 FMA-chain probe (bempp_measure_fma_peak) on this GPU",
-        "per_operator_tflops": achieved, "regular_ms": regular_ms,
-        "flops_per_regular_pair": FLOPS_PER_PAIR, "regular_pairs": nregular,
-    }
-
-    if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": "entries/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded perturbed icosphere)",
-            "config": {"workload": "laplace_dl_adl_hs_p1_ico5_f64", "triangles": len(cells),
-                       "dofs": n, "operators": OPERATORS, "regular_points": Q_REGULAR,
-                       "duffy_order": ORDER, "entries_per_step": entries_per_step,
-                       "parallelism": f"replicas{world}", "l2": "flushed between steps "
-                       "(256 MiB write); outputs (3 x 839 MB) exceed L2"},
-            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "clocks": clocks,
-        }
-        if not args.skip_cpu:
-            line["cpu_baseline"] = cpu_baseline(points, cells, n, args)
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.destroy_process_group()
-
-
-def ctypes_peak(_lib_mod):
-    from bempp._lib import ffi, lib
-
-    out = ffi.new("double*")
-    st = lib.bempp_measure_fma_peak(1, 4096, 5, out)
-    return float(out[0]) if st == 0 else None
 
 
 def singular_pair_count(cells):
@@ -312,7 +195,7 @@ def singular_pair_count(cells):
         for v in tri:
             vc[v].append(c)
     count = 0
-    for c, tri in enumerate(cells):
+    for tri in cells:
         nb = set()
         for v in tri:
             nb.update(vc[v])
@@ -320,33 +203,251 @@ def singular_pair_count(cells):
     return count
 
 
-def cpu_baseline(points, cells, n, args):
+def fma_peak():
+    from bempp._lib import ffi, lib
+
+    out = ffi.new("double*")
+    st = lib.bempp_measure_fma_peak(1, 4096, 5, out)
+    return float(out[0]) if st == 0 else None
+
+
+class Workload:
+    """Assemblers, device outputs and the step function of one workload on one GPU."""
+
+    def __init__(self, w, precision, level=None):
+        import torch
+
+        self.w = w
+        self.points, self.cells = workload_mesh(w, level)
+        self.grid, self.space = build_space(self.points, self.cells, w["space"])
+        self.n = self.space.global_size
+        self.assemblers = make_assemblers(w, precision)
+        dt = torch.complex128 if w["kernel"] == "helmholtz" else torch.float64
+        self.outs = [torch.empty((self.n, self.n), dtype=dt, device="cuda")
+                     for _ in self.assemblers]
+        self.flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        self.stream = torch.cuda.current_stream().cuda_stream
+        self.entries_per_step = len(self.assemblers) * self.n * self.n
+
+    def step(self, flush=True):
+        launches = 0
+        for (_, a), out in zip(self.assemblers, self.outs):
+            a.assemble_into_device(self.space, self.space, out, self.stream)
+            launches += a.launch_count()
+        if flush:
+            self.flush.fill_(1.0)  # L2 flush between steps (256 MiB > 126 MB L2)
+        return launches
+
+    def phase_ms(self):
+        import torch
+
+        for _, a in self.assemblers:
+            a.set_timing(True)
+        self.step(flush=False)
+        torch.cuda.synchronize()
+        out = {}
+        for name, a in self.assemblers:
+            out[name] = a.phase_times()  # geometry, clear, regular, singular
+            a.set_timing(False)
+        return out
+
+    def timed(self, steps, warmup, barrier=lambda: None):
+        import torch
+
+        for _ in range(warmup):
+            self.step()
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        launches = 0
+        for _ in range(steps):
+            launches += self.step()
+        t1.record()
+        torch.cuda.synchronize()
+        barrier()
+        return t0.elapsed_time(t1) / steps, launches
+
+
+def north_star(args):
+    """Helmholtz SL (k=8, DP0, 20,480 triangles): FP64 vs mixed assembly time and error."""
+    import torch
+
+    w = WORKLOADS["helmholtz_sl"]
+    res = {}
+    outs = {}
+    for prec in ("fp64", "mixed"):
+        wl = Workload(w, prec)
+        ms, _ = wl.timed(max(2, args.steps // 2), 2)
+        ph = wl.phase_ms()["single_layer"]
+        res[prec] = {"ms_per_assembly": ms, "entries_per_s": wl.entries_per_step / (ms * 1e-3),
+                     "regular_ms": ph[2] if len(ph) > 2 else None, "phase_ms": ph}
+        outs[prec] = wl.outs[0]
+        del wl
+        torch.cuda.empty_cache()
+    err = (torch.linalg.norm(outs["mixed"] - outs["fp64"]) / torch.linalg.norm(outs["fp64"])).item()
+    res["speedup_mixed_vs_fp64"] = res["fp64"]["ms_per_assembly"] / res["mixed"]["ms_per_assembly"]
+    res["mixed_rel_frobenius_error_vs_fp64"] = err
+    res["workload"] = w["name"]
+    del outs
+    torch.cuda.empty_cache()
+    return res
+
+
+def run_ours(args):
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    w = WORKLOADS[args.workload]
+    wl = Workload(w, args.precision, args.level)
+    if args.once:
+        wl.step(flush=False)
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"once": w["name"], "precision": args.precision,
+                              "cells": len(wl.cells), "n": wl.n}))
+        return
+
+    for _ in range(args.warmup):
+        wl.step()
+    phases = wl.phase_ms()  # live CUDA-event timing of each phase on the launching stream
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    ms_per_step, launches = wl.timed(args.steps, 1, barrier)
+    clocks = sampler.stop()
+    if world > 1:
+        import torch.distributed as dist
+
+        tt = torch.tensor([ms_per_step], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_per_step = float(tt.item())
+    value = world * wl.entries_per_step / (ms_per_step * 1e-3)
+
+    e2e = None
+    if not args.skip_e2e:
+        pts_h = np.ascontiguousarray(wl.points)
+        cells_h = np.ascontiguousarray(wl.cells)
+        e2e_steps = max(1, min(args.steps, 3))
+        torch.cuda.synchronize()
+        barrier()
+        t = time.perf_counter()
+        for _ in range(e2e_steps):
+            _, s2 = build_space(pts_h, cells_h, w["space"])
+            for _, a in wl.assemblers:
+                a.assemble(s2, s2)
+            del s2
+        e2e_s = (time.perf_counter() - t) / e2e_steps
+        if world > 1:
+            import torch.distributed as dist
+
+            tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_s = float(tt.item())
+        esize = 16 if w["kernel"] == "helmholtz" else 8
+        e2e = {"value": world * wl.entries_per_step / e2e_s, "unit": "entries/s",
+               "h2d_bytes_per_step": int(pts_h.nbytes + cells_h.astype(np.uintp).nbytes),
+               "d2h_bytes_per_step": int(wl.entries_per_step * esize),
+               "ms_per_step": e2e_s * 1e3,
+               "path": "function_space(grid) + BoundaryAssembler.assemble per operator (C-ABI "
+                       "boundary_assembler_assemble_into_memory_ex, host numpy output)"}
+
+    peak = fma_peak()
+    nreg = len(wl.cells) ** 2 - singular_pair_count(wl.cells)
+    per_op = {}
+    for name, ph in phases.items():
+        key = (w["kernel"], name, w["space"])
+        reg_ms = ph[2] if len(ph) > 2 else float("nan")
+        fl = FLOPS_PER_PAIR.get(key)
+        per_op[name] = {"regular_ms": reg_ms, "phase_ms": ph,
+                        "tflops": fl * nreg / (reg_ms * 1e-3) / 1e12 if fl else None}
+    dom = max(per_op, key=lambda n: per_op[n]["regular_ms"])
+    ach = per_op[dom]["tflops"]
+    roofline = {
+        "bound": "fp64", "kernel": f"regular kernel, {w['kernel']} {dom} ({w['space']})",
+        "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+        "frac": (ach / peak) if (ach and peak) else None, "traffic": None,
+        "peak_source": "measured FP64 FMA-chain probe (bempp_measure_fma_peak) on this GPU; "
+                       "MEASURED_PEAKS.json has no FP64 CUDA-core figure",
+        "regular_pairs": nreg, "per_operator": per_op,
+    }
+
+    ns = None
+    if rank == 0 and args.workload == "p1" and not args.skip_north_star:
+        del wl.outs
+        torch.cuda.empty_cache()
+        ns = north_star(args)
+
+    if rank == 0:
+        line = {
+            "metric": w["metric"], "value": value, "unit": "entries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128" if w["kernel"] == "helmholtz" else "f64",
+            "data": "synthetic (seeded icosphere)",
+            "config": {"workload": w["name"], "triangles": len(wl.cells), "dofs": wl.n,
+                       "operators": w["ops"], "precision": args.precision,
+                       "regular_points": Q_REGULAR, "duffy_order": ORDER,
+                       "entries_per_step": wl.entries_per_step,
+                       "parallelism": f"replicas{world}",
+                       "l2": "flushed between steps (256 MiB write); outputs exceed L2"},
+            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "clocks": clocks,
+        }
+        if ns is not None:
+            line["north_star"] = ns
+        if not args.skip_cpu:
+            line["cpu_baseline"] = cpu_baseline(w, wl.points, wl.cells, wl.n, args)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def cpu_baseline(w, points, cells, n, args):
     """CPU FP64 oracle on a bounded sample: the regular part for a subset of test cells
     (all trial cells) plus the full singular part, scaled to the whole workload."""
     from oracle import oracle
 
     threads = os.cpu_count() or 1
-    nsub = args.cpu_sample_cells
+    nsub = min(args.cpu_sample_cells, len(cells))
     rng = np.random.default_rng(0)
     subset = np.sort(rng.choice(len(cells), size=nsub, replace=False))
+    deg = 1 if w["space"] == "p1" else 0
+    kw = dict(k=w["k"], test_degree=deg, test_continuous=bool(deg), trial_degree=deg,
+              trial_continuous=bool(deg), q_regular=Q_REGULAR, q_singular=ORDER,
+              nthreads=threads)
     t_reg = t_sing = 0.0
-    for op in OPERATORS:
+    for op in w["ops"]:
         t = time.perf_counter()
-        oracle.assemble(points, cells, "laplace", op, test_degree=1, test_continuous=True,
-                        trial_degree=1, trial_continuous=True, q_regular=Q_REGULAR,
-                        q_singular=ORDER, nthreads=threads, parts=1, test_subset=subset)
+        oracle.assemble(points, cells, w["kernel"], op, parts=1, test_subset=subset, **kw)
         t_reg += time.perf_counter() - t
         t = time.perf_counter()
-        oracle.assemble(points, cells, "laplace", op, test_degree=1, test_continuous=True,
-                        trial_degree=1, trial_continuous=True, q_regular=Q_REGULAR,
-                        q_singular=ORDER, nthreads=threads, parts=2)
+        oracle.assemble(points, cells, w["kernel"], op, parts=2, **kw)
         t_sing += time.perf_counter() - t
     est = t_reg * len(cells) / nsub + t_sing
-    return {"value": len(OPERATORS) * n * n / est, "unit": "entries/s", "cores": threads,
+    return {"value": len(w["ops"]) * n * n / est, "unit": "entries/s", "cores": threads,
             "kind": "port",
-            "sample": f"regular part of all 3 operators for {nsub} of {len(cells)} test cells "
-                      f"(x all trial cells) scaled by {len(cells) / nsub:.1f}, plus the full "
-                      "singular part; CPU FP64 restatement of the bempp-rs algorithm "
+            "sample": f"regular part of {len(w['ops'])} operator(s) for {nsub} of {len(cells)} "
+                      f"test cells (x all trial cells) scaled by {len(cells) / nsub:.1f}, plus "
+                      "the full singular part; CPU FP64 restatement of the bempp-rs algorithm "
                       "(OpenMP over 128x128 blocks, -O3 -march=native)",
             "seconds_estimated_full_step": est}
 
@@ -355,28 +456,27 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    points, cells = workload_mesh()
+    w = WORKLOADS[args.workload]
+    points, cells = workload_mesh(w, args.level)
     from oracle import oracle
 
-    n = oracle.space_size(points, cells, 1, True)
-    for _ in range(args.warmup):
-        pass  # the oracle has no warm-up state; warm-up steps are not timed anyway
-    vals = []
-    base = None
+    deg = 1 if w["space"] == "p1" else 0
+    n = oracle.space_size(points, cells, deg, bool(deg))
+    vals, base = [], None
     for _ in range(args.steps):
-        base = cpu_baseline(points, cells, n, args)
+        base = cpu_baseline(w, points, cells, n, args)
         vals.append(base["value"])
     value = statistics.median(vals)
+    eps = len(w["ops"]) * n * n
     line = {
-        "metric": METRIC, "value": value, "unit": "entries/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": len(OPERATORS) * n * n / value * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded perturbed icosphere)", "impl": "reference",
-        "config": {"workload": "laplace_dl_adl_hs_p1_ico5_f64", "triangles": len(cells),
-                   "dofs": n, "operators": OPERATORS, "regular_points": Q_REGULAR,
-                   "duffy_order": ORDER, "entries_per_step": len(OPERATORS) * n * n,
-                   "parallelism": "host cores"},
+        "metric": w["metric"], "value": value, "unit": "entries/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": eps / value * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c128" if w["kernel"] == "helmholtz" else "f64",
+        "data": "synthetic (seeded icosphere)", "impl": "reference",
+        "config": {"workload": w["name"], "triangles": len(cells), "dofs": n,
+                   "operators": w["ops"], "regular_points": Q_REGULAR, "duffy_order": ORDER,
+                   "entries_per_step": eps, "parallelism": "host cores"},
         "cpu_baseline": {**base, "value": value},
         "e2e": {"value": value, "unit": "entries/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -390,9 +490,14 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--cpu-sample-cells", type=int, default=48)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="p1")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--level", type=int, default=None, help="icosphere refinement override")
+    ap.add_argument("--once", action="store_true")
+    ap.add_argument("--cpu-sample-cells", type=int, default=160)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-north-star", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -254,6 +254,22 @@ ElementFamilyT *create_nedelec_family_bempp(size_t degree, Continuity continuity
 /* src/bindings/ndelement.rs:9-19 (null-safe) */
 void element_family_t_free_bempp(ElementFamilyT *ptr);
 
+/* ------------------------------------------------------- inspection (host) ----- */
+/* Addition: the regular (non-singular) rule with `npoints` points on the reference
+ * triangle: points as x0,y0,x1,y1,... and weights summing to 1/2.  Returns npoints, or
+ * 0 if no rule has that many points.  Either array may be NULL. */
+size_t bempp_regular_rule(size_t npoints, double *points, double *weights);
+/* Addition: the Duffy rule of adjacency configuration `config` (0..27 in the order of
+ * src/boundary_assemblers.rs:267-288: 9 vertex, 18 edge, 1 identical) with 1-D order
+ * `order`.  Returns the number of points (arrays of 2n, 2n, n; NULL to query), or 0. */
+size_t bempp_singular_rule(size_t config, size_t order, double *test_points,
+                           double *trial_points, double *weights);
+/* Addition: the ordered cell pairs of a grid that share a vertex (the singular part),
+ * grouped by configuration as src/boundary_assemblers.rs:564-606 groups them.  Returns
+ * the number of pairs; arrays may be NULL to query. */
+size_t bempp_grid_singular_pairs(GridT *grid, size_t *test_cells, size_t *trial_cells,
+                                 size_t *configs);
+
 #ifdef __cplusplus
 }
 #endif

