@@ -509,6 +509,51 @@ ElementFamilyT* create_nedelec_family_bempp(size_t, Continuity, DType) {
 
 void element_family_t_free_bempp(ElementFamilyT* ptr) { delete ptr; }
 
+// ------------------------------------------------------- allocation-free assembly ---
+BemppStatus bempp_assemble_regular_dp0_noalloc(
+    int32_t kernel, OperatorType operator_type, double k, Precision precision,
+    size_t regular_points, const double* test_points, size_t test_npoints,
+    const int32_t* test_cells, size_t test_ncells, const double* trial_points,
+    size_t trial_npoints, const int32_t* trial_cells, size_t trial_ncells, void* out,
+    void* stream) {
+  return guarded([&] {
+    if (kernel != kLaplace && kernel != kHelmholtz) throw Error(kInvalidArgument, "kernel must be 0 or 1");
+    if (operator_type > OperatorType_AdjointDoubleLayer)
+      throw Error(kInvalidArgument, "operator must be single, double or adjoint double layer");
+    if (precision > Precision_Mixed) throw Error(kInvalidArgument, "unknown precision");
+    const size_t maxc = static_cast<size_t>(noalloc_max_cells());
+    if (test_ncells > maxc || trial_ncells > maxc)
+      throw Error(kInvalidArgument, "more than " + std::to_string(maxc) +
+                                        " cells in a mesh (the scratch array's limit)");
+    if (regular_points > static_cast<size_t>(noalloc_max_points()) ||
+        !has_simplex_rule(static_cast<int>(regular_points)))
+      throw Error(kInvalidArgument, "regular rule must have at most " +
+                                        std::to_string(noalloc_max_points()) +
+                                        " points and exist (1, 3, 6, 7 or 12)");
+    if (test_ncells == 0 || trial_ncells == 0) return;
+    require(test_points, "test points");
+    require(test_cells, "test cells");
+    require(trial_points, "trial points");
+    require(trial_cells, "trial cells");
+    require(out, "output");
+    if (test_npoints == 0 || trial_npoints == 0) throw Error(kInvalidArgument, "empty point set");
+    const RegularRule rule = simplex_rule(static_cast<int>(regular_points));
+    RegularArgs ra;
+    ra.kernel = kernel;
+    ra.op = operator_type;
+    ra.k = k;
+    ra.same_grid = 0;
+    ra.precision = precision == Precision_Mixed ? kRegularMixed : kRegularFP64;
+    ra.out_type = kernel == kHelmholtz ? kOutC128 : kOutF64;
+    ra.ld = static_cast<int64_t>(test_ncells);
+    ra.out = out;
+    BEMPP_CUDA(assemble_regular_dp0_noalloc(ra, rule, test_points, test_cells,
+                                            static_cast<int>(test_ncells), trial_points,
+                                            trial_cells, static_cast<int>(trial_ncells),
+                                            static_cast<cudaStream_t>(stream)));
+  });
+}
+
 // -------------------------------------------------------------------- inspection ---
 size_t bempp_regular_rule(size_t npoints, double* points, double* weights) {
   size_t n = 0;

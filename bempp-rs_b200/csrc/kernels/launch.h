@@ -88,6 +88,17 @@ cudaError_t launch_singular(const CellSet& test, const int* test_dofs, int nbt,
                             const SingularRules& rules, const SingularPairs& pairs,
                             const SingularArgs& a, cudaStream_t stream);
 
+// Allocation-free regular DP0 assembly between two distinct meshes (noalloc.cu); the
+// scratch lives in a static device array of noalloc_max_cells() cells per mesh and
+// noalloc_max_points() regular points.
+int noalloc_max_cells();
+int noalloc_max_points();
+cudaError_t assemble_regular_dp0_noalloc(const RegularArgs& args, const RegularRule& rule,
+                                         const double* test_points, const int* test_cells,
+                                         int test_ncells, const double* trial_points,
+                                         const int* trial_cells, int trial_ncells,
+                                         cudaStream_t stream);
+
 // CUDA-core FMA throughput probe (diag.cu).
 cudaError_t measure_fma_peak(int fp64, int iters, int reps, double* tflops);
 

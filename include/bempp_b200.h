@@ -254,6 +254,28 @@ ElementFamilyT *create_nedelec_family_bempp(size_t degree, Continuity continuity
 /* src/bindings/ndelement.rs:9-19 (null-safe) */
 void element_family_t_free_bempp(ElementFamilyT *ptr);
 
+/* Addition, with no counterpart in the reference: dense regular-quadrature assembly of a
+ * DP0 x DP0 Laplace (kernel 0) or Helmholtz (kernel 1) single-layer, double-layer or
+ * adjoint double-layer operator between two distinct meshes, for callers that cannot
+ * allocate GPU memory.  It allocates nothing: every input and the output are the
+ * caller's device buffers, and the scratch it needs (per-cell geometry and quadrature
+ * points) is a fixed static device array held by each GPU that loads the library.
+ * Inputs: points (n x 3 FP64) and cells (n x 3 int32, indices < npoints) of each mesh,
+ * in device memory.  Output: n_test_cells x n_trial_cells column-major, FP64 (Laplace)
+ * or interleaved complex128 (Helmholtz).  Every pair uses the regular rule of
+ * `regular_points` points and there is no singular part (the two meshes are treated as
+ * different grids), as in boundary_assembler_assemble_into_device with spaces on two
+ * grid objects.  Limits: at most 8192 cells per mesh and 12 regular points; larger
+ * sizes are rejected with BemppStatus_InvalidArgument.  The first call on a device looks
+ * up the array's device address; make that call before any stream capture.  Calls share
+ * the array: calls that overlap on the GPU race and must be serialised by the caller. */
+BemppStatus bempp_assemble_regular_dp0_noalloc(
+    int32_t kernel, OperatorType operator_type, double k, Precision precision,
+    size_t regular_points, const double *test_points, size_t test_npoints,
+    const int32_t *test_cells, size_t test_ncells, const double *trial_points,
+    size_t trial_npoints, const int32_t *trial_cells, size_t trial_ncells, void *out,
+    void *stream);
+
 /* ------------------------------------------------------- inspection (host) ----- */
 /* Addition: the regular (non-singular) rule with `npoints` points on the reference
  * triangle: points as x0,y0,x1,y1,... and weights summing to 1/2.  Returns npoints, or
