@@ -4,6 +4,7 @@
 // (the src/bindings/ tree).  Where the reference panics (and so aborts across the FFI) these
 // record a message for bempp_last_error() and return a neutral value; the *_ex and
 // device variants return a status code.
+#include <atomic>
 #include <cstring>
 #include <string>
 
@@ -14,6 +15,12 @@ using namespace bempp_b200;
 
 namespace bempp_b200 {
 void build_singular_pairs(GridT& g, SingularPairList& out);
+struct SweepTuning {
+  int kchunk = 8;
+  int blocks_per_sm = 4;
+  double probe_ms = 0.0;
+};
+SweepTuning last_sweep_tuning();
 }
 
 struct BoundaryAssemblerOptionsT {
@@ -22,6 +29,7 @@ struct BoundaryAssemblerOptionsT {
 
 namespace {
 thread_local std::string t_last_error;
+std::atomic<uint64_t> g_grid_uid{1};
 }
 
 namespace bempp_b200 {
@@ -428,6 +436,7 @@ static GridT* make_grid(const void* points, size_t npoints, size_t gdim, DType d
     if (dtype != DType_F32 && dtype != DType_F64)
       throw Error(kInvalidArgument, "grid points must be F32 or F64");
     auto* g = new GridT();
+    g->uid = g_grid_uid.fetch_add(1);
     g->dtype = dtype;
     g->npoints = static_cast<int64_t>(npoints);
     g->ncells = static_cast<int64_t>(ncells);
@@ -508,6 +517,88 @@ ElementFamilyT* create_nedelec_family_bempp(size_t, Continuity, DType) {
 }
 
 void element_family_t_free_bempp(ElementFamilyT* ptr) { delete ptr; }
+
+// ---------------------------------------------------------------- adjoint gradient ---
+BemppStatus bempp_helmholtz_single_layer_dp0_gradient_device(
+    GridT* grid, const BoundaryAssemblerOptionsT* options, double k, const void* lambda,
+    const void* mu, double* value_and_grad_k, double* grad_points, void* stream) {
+  return guarded([&] {
+    require(grid, "grid");
+    require(options, "options");
+    if (grid->ncells == 0) return;
+    require(lambda, "lambda");
+    require(mu, "mu");
+    require(value_and_grad_k, "value");
+    require(grad_points, "grad_points");
+    helmholtz_sl_gradient_device(*grid, options->options, k, static_cast<const double*>(lambda),
+                                 static_cast<const double*>(mu), value_and_grad_k, grad_points,
+                                 static_cast<cudaStream_t>(stream));
+  });
+}
+
+BemppStatus bempp_helmholtz_single_layer_dp0_gradient(GridT* grid,
+                                                      const BoundaryAssemblerOptionsT* options,
+                                                      double k, const void* lambda,
+                                                      const void* mu, double* value,
+                                                      double* grad_k, double* grad_points) {
+  return guarded([&] {
+    require(grid, "grid");
+    require(options, "options");
+    require(value, "value");
+    require(grad_k, "grad_k");
+    require(grad_points, "grad_points");
+    const size_t nc = static_cast<size_t>(grid->ncells), np = static_cast<size_t>(grid->npoints);
+    if (nc == 0) {
+      *value = *grad_k = 0.0;
+      std::memset(grad_points, 0, sizeof(double) * 3 * np);
+      return;
+    }
+    require(lambda, "lambda");
+    require(mu, "mu");
+    DeviceBuffer d_lam, d_mu, d_out, d_grad;
+    d_lam.alloc(16 * nc);
+    d_mu.alloc(16 * nc);
+    d_out.alloc(16);
+    d_grad.alloc(sizeof(double) * 3 * np);
+    BEMPP_CUDA(cudaMemcpy(d_lam.ptr, lambda, 16 * nc, cudaMemcpyHostToDevice));
+    BEMPP_CUDA(cudaMemcpy(d_mu.ptr, mu, 16 * nc, cudaMemcpyHostToDevice));
+    helmholtz_sl_gradient_device(*grid, options->options, k, d_lam.as<double>(),
+                                 d_mu.as<double>(), d_out.as<double>(), d_grad.as<double>(),
+                                 nullptr);
+    double tot[2];
+    BEMPP_CUDA(cudaMemcpy(tot, d_out.ptr, sizeof(tot), cudaMemcpyDeviceToHost));
+    BEMPP_CUDA(cudaMemcpy(grad_points, d_grad.ptr, sizeof(double) * 3 * np,
+                          cudaMemcpyDeviceToHost));
+    *value = tot[0];
+    *grad_k = tot[1];
+  });
+}
+
+// ------------------------------------------------------------------------- sweep ---
+BemppStatus bempp_helmholtz_single_layer_dp0_sweep_device(GridT* const* grids, size_t ngrids,
+                                                          const double* wavenumbers, size_t nk,
+                                                          const BoundaryAssemblerOptionsT* options,
+                                                          void* const* outputs, void* stream) {
+  return guarded([&] {
+    require(options, "options");
+    if (ngrids == 0 || nk == 0) return;
+    require(grids, "grids");
+    require(wavenumbers, "wavenumbers");
+    require(outputs, "outputs");
+    for (size_t i = 0; i < ngrids; ++i) require(grids[i], "grid");
+    helmholtz_sl_sweep_device(grids, ngrids, wavenumbers, nk, options->options, outputs,
+                              static_cast<cudaStream_t>(stream));
+  });
+}
+
+BemppStatus bempp_sweep_last_tuning(int32_t* kchunk, int32_t* blocks_per_sm, double* probe_ms) {
+  return guarded([&] {
+    const SweepTuning t = last_sweep_tuning();
+    if (kchunk) *kchunk = t.kchunk;
+    if (blocks_per_sm) *blocks_per_sm = t.blocks_per_sm;
+    if (probe_ms) *probe_ms = t.probe_ms;
+  });
+}
 
 // ------------------------------------------------------- allocation-free assembly ---
 BemppStatus bempp_assemble_regular_dp0_noalloc(

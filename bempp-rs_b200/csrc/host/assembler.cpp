@@ -283,6 +283,45 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
   timer.finish();
 }
 
+const GridGeometry& sweep_geometry(GridT& g, int device, const RegularRule& rule) {
+  size_t launches = 0;
+  return grid_geometry(g, device, rule, nullptr, launches);
+}
+
+SingularRules sweep_rules(int device, int order) {
+  const DeviceRules& dr = device_rules(device, order);
+  return SingularRules{dr.offset.as<int>(), dr.test_xi.as<double>(), dr.trial_xi.as<double>(),
+                       dr.w.as<double>()};
+}
+
+void helmholtz_sl_gradient_device(GridT& g, const Options& opts, double k, const double* d_lam,
+                                  const double* d_mu, double* d_totals, double* d_grad_points,
+                                  cudaStream_t stream) {
+  const int device = current_device();
+  const auto qit = opts.regular.find(kTriangle);
+  const auto sit = opts.singular.find({kTriangle, kTriangle});
+  if (qit == opts.regular.end() || sit == opts.singular.end())
+    throw Error(kInvalidArgument, "options lack triangle quadrature degrees");
+  if (opts.precision != 0)
+    throw Error(kUnsupported, "the adjoint gradient is computed in FP64 only");
+  const RegularRule rule = simplex_rule(static_cast<int>(qit->second));
+  size_t launches = 0;
+  const GridGeometry& geo = grid_geometry(g, device, rule, stream, launches);
+  SingularPairList& pl = grid_pairs(g, device);
+  const DeviceRules& dr = device_rules(device, static_cast<int>(sit->second));
+  SingularRules rules{dr.offset.as<int>(), dr.test_xi.as<double>(), dr.trial_xi.as<double>(),
+                      dr.w.as<double>()};
+  SingularPairs pairs{static_cast<int>(pl.test_cell.size()), pl.d_test.as<int>(),
+                      pl.d_trial.as<int>(), pl.d_config.as<int>()};
+  {
+    std::lock_guard<std::mutex> lock(g.mu);
+    g.adjoint_scratch.alloc(sizeof(double) * 9 * static_cast<size_t>(std::max<int64_t>(1, g.ncells)));
+  }
+  BEMPP_CUDA(launch_adjoint_sl(cell_set(g, geo), rule, rules, pairs, k, d_lam, d_mu,
+                               g.adjoint_scratch.as<double>(), d_grad_points,
+                               static_cast<int>(g.npoints), d_totals, stream));
+}
+
 MatrixT* assemble_singular_csr(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test) {
   check_spaces(a, trial, test);
   const int device = current_device();

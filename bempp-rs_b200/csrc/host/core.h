@@ -121,6 +121,7 @@ struct SingularPairList {
 using bempp_b200::DeviceBuffer;
 
 struct GridT {
+  uint64_t uid = 0;            // unique per grid object (plans keyed by it)
   std::vector<double> points;  // npoints x 3
   std::vector<int> cells;      // ncells x 3 (triangle vertices)
   int64_t npoints = 0, ncells = 0;
@@ -132,6 +133,7 @@ struct GridT {
   DeviceBuffer d_points, d_cells;
   std::map<int, std::unique_ptr<bempp_b200::GridGeometry>> geometry;  // keyed by regular npts
   std::unique_ptr<bempp_b200::SingularPairList> pairs;
+  DeviceBuffer adjoint_scratch;  // per-cell vertex gradients of the adjoint kernel
   std::mutex mu;
   void build_topology();
 };
@@ -199,6 +201,16 @@ size_t dtype_size(uint8_t dtype);
 // Dense assembly into device memory (column-major, assembler dtype) on `stream`.
 void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d_out,
                      cudaStream_t stream);
+// Adjoint gradient of Re(lambda^H A mu), Helmholtz single layer, DP0 x DP0 on one grid;
+// device inputs (complex128 lambda, mu per cell) and outputs ({J, dJ/dk}, npoints x 3).
+void helmholtz_sl_gradient_device(GridT& g, const Options& opts, double k, const double* d_lam,
+                                  const double* d_mu, double* d_totals, double* d_grad_points,
+                                  cudaStream_t stream);
+// Batched Helmholtz single-layer DP0 sweep (sweep.cpp): outs[i] holds nk complex64
+// column-major ncells_i^2 matrices, wavenumber-major.
+void helmholtz_sl_sweep_device(GridT* const* grids, size_t ngrids, const double* ks, size_t nk,
+                               const Options& opts, void* const* outs, cudaStream_t stream);
+struct SweepTuning;
 // Singular part as CSR (host).
 MatrixT* assemble_singular_csr(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test);
 

@@ -1,0 +1,343 @@
+// Adjoint gradient of J = Re(lambda^H A(x, k) mu) for the Helmholtz single-layer operator
+// on DP0 x DP0, with respect to every vertex coordinate and the wavenumber, without
+// forming dA.
+//
+// A_ij = (1/4pi) jdet_i jdet_j sum_n w_n e^{ik r_n} / r_n over the rule of the pair
+// (regular tensor rule, or the Duffy rule of an adjacent pair), r_n = |x_n - y_n| with
+// x_n = sum_a phi_a(xi_n) V_{i,a} and y_n = sum_b phi_b(eta_n) V_{j,b} (phi the P1
+// barycentric weights, V the cell vertices).  The discrete sum is differentiated
+// exactly:
+//   dA_ij/dV_{i,a} = (1/4pi) [ djdet_i/dV_a jdet_j sum_n w_n G_n
+//                              + jdet_i jdet_j sum_n w_n phi_a(xi_n) grad_x G_n ],
+//   grad_x (e^{ikr}/r) = e^{ikr} (ikr - 1) (x - y) / r^3,  grad_y = -grad_x,
+//   djdet/dV1 = t1 x n, djdet/dV2 = n x t0, djdet/dV0 = -(t1 x n + n x t0),
+//   dA_ij/dk = (1/4pi) jdet_i jdet_j sum_n w_n i e^{ikr_n}.
+// Each pair contributes Re(conj(lambda_i) mu_j dA_ij) to 9 + 9 vertex coordinates of
+// its two cells and to dJ/dk; contributions are reduced per CTA (test side in
+// registers and shared memory, trial side by warp shuffles) and added per cell, then a
+// last kernel scatters the per-cell-vertex gradients to the vertices.
+//
+// Regular pairs use the tiled mapping of regular.cu (32 x 32 cell tiles, lane = test
+// cell); adjacent pairs use one warp per pair over their Duffy rule.  FP64 throughout.
+#include "launch.h"
+#include "tiles.cuh"
+
+namespace bempp_b200 {
+namespace {
+
+using namespace tiles;
+
+// d jdet / d V_a of a flat cell, a = 0, 1, 2 (3-vectors)
+__device__ __forceinline__ void jdet_gradient(const double t0[3], const double t1[3],
+                                              const double n[3], double g[3][3]) {
+  const double a[3] = {t1[1] * n[2] - t1[2] * n[1], t1[2] * n[0] - t1[0] * n[2],
+                       t1[0] * n[1] - t1[1] * n[0]};  // t1 x n
+  const double b[3] = {n[1] * t0[2] - n[2] * t0[1], n[2] * t0[0] - n[0] * t0[2],
+                       n[0] * t0[1] - n[1] * t0[0]};  // n x t0
+  for (int d = 0; d < 3; ++d) {
+    g[1][d] = a[d];
+    g[2][d] = b[d];
+    g[0][d] = -(a[d] + b[d]);
+  }
+}
+
+template <int QT>
+__global__ void __launch_bounds__(kThreads, 3)
+    adjoint_sl_regular(CellSet cs, RegularRule rule, double k, const double2* __restrict__ lam,
+                       const double2* __restrict__ mu, double* __restrict__ grad_cell,
+                       double* __restrict__ totals) {
+  const int Q = QT > 0 ? QT : rule.npts;
+  const int ti0 = blockIdx.x * kTile, sj0 = blockIdx.y * kTile;
+  const int nti = min(kTile, cs.ncells - ti0), nsj = min(kTile, cs.ncells - sj0);
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned char* cursor = smem;
+  const Tile T = carve_tile(cursor, Q, false, 1);
+  const Tile S = carve_tile(cursor, Q, false, 1);
+  double* s_test = reinterpret_cast<double*>(cursor);  // [kTile][9] test-cell gradients
+  double* s_trial = s_test + kTile * 9;                // [kTile][9] trial-cell gradients
+  double* s_tot = s_trial + kTile * 9;                 // J, dJ/dk
+  for (int e = threadIdx.x; e < 2 * kTile * 9 + 2; e += kThreads) s_test[e] = 0.0;
+  load_tile(T, cs, ti0, nti, Q, false, nullptr, 1);
+  load_tile(S, cs, sj0, nsj, Q, false, nullptr, 1);
+  __syncthreads();
+
+  const int it = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool valid = it < nti;
+  const double2 li = valid ? lam[ti0 + it] : make_double2(0.0, 0.0);
+  const int a0 = T.vid[it], a1 = T.vid[kTile + it], a2 = T.vid[2 * kTile + it];
+  const double jdet_i = T.G(fJdet, it);
+
+  double gt[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};  // test-cell vertex gradients
+  double jval = 0.0, dk = 0.0;
+  for (int js = warp; js < nsj; js += kWarps) {
+    const bool adjacent = share_vertex(a0, a1, a2, S.vid[js], S.vid[kTile + js],
+                                       S.vid[2 * kTile + js]);
+    const bool active = valid && !adjacent;
+    // c = conj(lambda_i) mu_j
+    const double2 mj = mu[sj0 + js];
+    const double c_re = li.x * mj.x + li.y * mj.y, c_im = li.x * mj.y - li.y * mj.x;
+    double S0_re = 0.0, S0_im = 0.0, Sk_re = 0.0, Sk_im = 0.0;
+    double uq[QT > 0 ? QT : kMaxRegularPoints][3];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) uq[q][0] = uq[q][1] = uq[q][2] = 0.0;
+    double vt[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    if (active) {
+#pragma unroll 1
+      for (int p = 0; p < Q; ++p) {
+        const double x0 = T.P(p, 0, it), x1 = T.P(p, 1, it), x2 = T.P(p, 2, it);
+        double vp[3] = {0.0, 0.0, 0.0};
+        double g_re = 0.0, g_im = 0.0, e_re = 0.0, e_im = 0.0;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+          const double dx = x0 - S.P(q, 0, js), dy = x1 - S.P(q, 1, js), dz = x2 - S.P(q, 2, js);
+          const double r2 = dx * dx + dy * dy + dz * dz;
+          const double rinv = rsqrt_refined(r2);
+          const double r = r2 * rinv, kr = k * r;
+          double sn, csn;
+          sincos(kr, &sn, &csn);
+          const double wq = rule.w[q];
+          g_re = fma(wq * rinv, csn, g_re);
+          g_im = fma(wq * rinv, sn, g_im);
+          e_re = fma(wq, csn, e_re);
+          e_im = fma(wq, sn, e_im);
+          // Re(c e^{ikr} (ikr - 1)) / r^3
+          const double f_re = -csn - kr * sn, f_im = kr * csn - sn;
+          const double gs = wq * (c_re * f_re - c_im * f_im) * rinv * rinv * rinv;
+          vp[0] = fma(gs, dx, vp[0]);
+          vp[1] = fma(gs, dy, vp[1]);
+          vp[2] = fma(gs, dz, vp[2]);
+          const double wgs = rule.w[p] * gs;
+          uq[q][0] = fma(wgs, dx, uq[q][0]);
+          uq[q][1] = fma(wgs, dy, uq[q][1]);
+          uq[q][2] = fma(wgs, dz, uq[q][2]);
+        }
+        const double wp = rule.w[p];
+        S0_re = fma(wp, g_re, S0_re);
+        S0_im = fma(wp, g_im, S0_im);
+        Sk_re = fma(wp, e_re, Sk_re);
+        Sk_im = fma(wp, e_im, Sk_im);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const double f = wp * rule.phi[a][p];
+          vt[a][0] = fma(f, vp[0], vt[a][0]);
+          vt[a][1] = fma(f, vp[1], vt[a][1]);
+          vt[a][2] = fma(f, vp[2], vt[a][2]);
+        }
+      }
+    }
+    const double jdet_j = S.G(fJdet, js);
+    const double jj = jdet_i * jdet_j * kInv4Pi;
+    const double R0 = c_re * S0_re - c_im * S0_im;  // Re(c S0)
+    // trial-side contributions of this lane, then a warp reduction over the test cells
+    double gs_[3][3];
+    {
+      double tj_t0[3], tj_t1[3], tj_n[3], djj[3][3];
+      for (int d = 0; d < 3; ++d) {
+        tj_t0[d] = S.G(fT0x + d, js);
+        tj_t1[d] = S.G(fT1x + d, js);
+      }
+      tj_n[0] = S.G(fNx, js);
+      tj_n[1] = S.G(fNy, js);
+      tj_n[2] = S.G(fNz, js);
+      jdet_gradient(tj_t0, tj_t1, tj_n, djj);
+      const double rj = R0 * jdet_i * kInv4Pi;
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          double acc = 0.0;
+#pragma unroll
+          for (int q = 0; q < Q; ++q) acc = fma(rule.phi[b][q], uq[q][d], acc);
+          gs_[b][d] = active ? (-jj * acc + rj * djj[b][d]) : 0.0;
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      double v = gs_[e / 3][e % 3];
+#pragma unroll
+      for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
+      if (it == 0) s_trial[js * 9 + e] += v;  // each js belongs to one warp
+    }
+    if (active) {
+      double ti_t0[3], ti_t1[3], ti_n[3], dji[3][3];
+      for (int d = 0; d < 3; ++d) {
+        ti_t0[d] = T.G(fT0x + d, it);
+        ti_t1[d] = T.G(fT1x + d, it);
+      }
+      ti_n[0] = T.G(fNx, it);
+      ti_n[1] = T.G(fNy, it);
+      ti_n[2] = T.G(fNz, it);
+      jdet_gradient(ti_t0, ti_t1, ti_n, dji);
+      const double ri = R0 * jdet_j * kInv4Pi;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) gt[a][d] += jj * vt[a][d] + ri * dji[a][d];
+      jval += R0 * jj;
+      dk += (c_re * (-Sk_im) - c_im * Sk_re) * jj;  // Re(c i Sk)
+    }
+  }
+  if (valid) {
+#pragma unroll
+    for (int e = 0; e < 9; ++e) atomicAdd(s_test + it * 9 + e, gt[e / 3][e % 3]);
+  }
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    jval += __shfl_xor_sync(0xffffffffu, jval, s);
+    dk += __shfl_xor_sync(0xffffffffu, dk, s);
+  }
+  if (it == 0) {
+    atomicAdd(s_tot, jval);
+    atomicAdd(s_tot + 1, dk);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < kTile * 9; e += kThreads) {
+    const int c = e / 9;
+    if (c < nti) atomicAdd(grad_cell + static_cast<int64_t>(ti0 + c) * 9 + (e % 9), s_test[e]);
+    if (c < nsj) atomicAdd(grad_cell + static_cast<int64_t>(sj0 + c) * 9 + (e % 9), s_trial[e]);
+  }
+  if (threadIdx.x == 0) {
+    atomicAdd(totals, s_tot[0]);
+    atomicAdd(totals + 1, s_tot[1]);
+  }
+}
+
+struct CellGeo {
+  double v0[3], t0[3], t1[3], n[3], jdet;
+};
+
+__device__ __forceinline__ void load_geo(const CellSet& cs, int c, CellGeo& g) {
+  const int N = cs.ncells;
+  for (int d = 0; d < 3; ++d) {
+    g.v0[d] = bempp_b200::g(cs.geom, kV0x + d, N, c);
+    g.t0[d] = bempp_b200::g(cs.geom, kT0x + d, N, c);
+    g.t1[d] = bempp_b200::g(cs.geom, kT1x + d, N, c);
+    g.n[d] = bempp_b200::g(cs.geom, kNx + d, N, c);
+  }
+  g.jdet = bempp_b200::g(cs.geom, kJdet, N, c);
+}
+
+// One warp per adjacent pair over its Duffy rule.
+__global__ void __launch_bounds__(256)
+    adjoint_sl_singular(CellSet cs, SingularRules rules, SingularPairs pairs, double k,
+                        const double2* __restrict__ lam, const double2* __restrict__ mu,
+                        double* __restrict__ grad_cell, double* __restrict__ totals) {
+  const int lane = threadIdx.x & 31;
+  const int pair = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (pair >= pairs.npairs) return;
+  const int tc = pairs.test_cell[pair], sc = pairs.trial_cell[pair], cfg = pairs.config[pair];
+  CellGeo x, y;
+  load_geo(cs, tc, x);
+  load_geo(cs, sc, y);
+  const double2 li = lam[tc], mj = mu[sc];
+  const double c_re = li.x * mj.x + li.y * mj.y, c_im = li.x * mj.y - li.y * mj.x;
+  const int off = rules.offset[cfg], npts = rules.offset[cfg + 1] - off;
+  double S0_re = 0.0, S0_im = 0.0, Sk_re = 0.0, Sk_im = 0.0;
+  double gx[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, gy[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  for (int ii = lane; ii < npts; ii += 32) {
+    const int i = off + ii;
+    const double xi0 = rules.test_xi[2 * i], xi1 = rules.test_xi[2 * i + 1];
+    const double et0 = rules.trial_xi[2 * i], et1 = rules.trial_xi[2 * i + 1];
+    const double w = rules.w[i];
+    double d[3];
+    for (int c = 0; c < 3; ++c)
+      d[c] = (x.v0[c] + xi0 * x.t0[c] + xi1 * x.t1[c]) - (y.v0[c] + et0 * y.t0[c] + et1 * y.t1[c]);
+    const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    const double rinv = rsqrt(r2);
+    const double r = r2 * rinv, kr = k * r;
+    double sn, csn;
+    sincos(kr, &sn, &csn);
+    S0_re = fma(w * rinv, csn, S0_re);
+    S0_im = fma(w * rinv, sn, S0_im);
+    Sk_re = fma(w, csn, Sk_re);
+    Sk_im = fma(w, sn, Sk_im);
+    const double f_re = -csn - kr * sn, f_im = kr * csn - sn;
+    const double gs = w * (c_re * f_re - c_im * f_im) * rinv * rinv * rinv;
+    const double phi[3] = {1.0 - xi0 - xi1, xi0, xi1};
+    const double psi[3] = {1.0 - et0 - et1, et0, et1};
+    for (int a = 0; a < 3; ++a)
+      for (int c = 0; c < 3; ++c) {
+        gx[a][c] = fma(gs * phi[a], d[c], gx[a][c]);
+        gy[a][c] = fma(-gs * psi[a], d[c], gy[a][c]);
+      }
+  }
+  for (int s = 16; s > 0; s >>= 1) {
+    S0_re += __shfl_xor_sync(0xffffffffu, S0_re, s);
+    S0_im += __shfl_xor_sync(0xffffffffu, S0_im, s);
+    Sk_re += __shfl_xor_sync(0xffffffffu, Sk_re, s);
+    Sk_im += __shfl_xor_sync(0xffffffffu, Sk_im, s);
+    for (int a = 0; a < 3; ++a)
+      for (int c = 0; c < 3; ++c) {
+        gx[a][c] += __shfl_xor_sync(0xffffffffu, gx[a][c], s);
+        gy[a][c] += __shfl_xor_sync(0xffffffffu, gy[a][c], s);
+      }
+  }
+  if (lane != 0) return;
+  const double jj = x.jdet * y.jdet * kInv4Pi;
+  const double R0 = c_re * S0_re - c_im * S0_im;
+  double djx[3][3], djy[3][3];
+  jdet_gradient(x.t0, x.t1, x.n, djx);
+  jdet_gradient(y.t0, y.t1, y.n, djy);
+  for (int a = 0; a < 3; ++a)
+    for (int c = 0; c < 3; ++c) {
+      atomicAdd(grad_cell + static_cast<int64_t>(tc) * 9 + a * 3 + c,
+                jj * gx[a][c] + R0 * y.jdet * kInv4Pi * djx[a][c]);
+      atomicAdd(grad_cell + static_cast<int64_t>(sc) * 9 + a * 3 + c,
+                jj * gy[a][c] + R0 * x.jdet * kInv4Pi * djy[a][c]);
+    }
+  atomicAdd(totals, R0 * jj);
+  atomicAdd(totals + 1, (c_re * (-Sk_im) - c_im * Sk_re) * jj);
+}
+
+// Per-cell-vertex gradients -> per-point gradients (npoints x 3).
+__global__ void cell_to_point_gradient(CellSet cs, const double* __restrict__ grad_cell,
+                                       double* __restrict__ grad_points) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cs.ncells) return;
+  for (int a = 0; a < 3; ++a) {
+    const int v = cs.vids[a * cs.ncells + c];
+    for (int d = 0; d < 3; ++d)
+      atomicAdd(grad_points + 3 * static_cast<int64_t>(v) + d,
+                grad_cell[static_cast<int64_t>(c) * 9 + a * 3 + d]);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_adjoint_sl(const CellSet& cs, const RegularRule& rule,
+                              const SingularRules& rules, const SingularPairs& pairs, double k,
+                              const double* lam, const double* mu, double* grad_cell,
+                              double* grad_points, int npoints, double* totals,
+                              cudaStream_t stream) {
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(grad_cell, 0, sizeof(double) * 9 * cs.ncells, stream)) != cudaSuccess)
+    return e;
+  if ((e = cudaMemsetAsync(grad_points, 0, sizeof(double) * 3 * npoints, stream)) != cudaSuccess)
+    return e;
+  if ((e = cudaMemsetAsync(totals, 0, sizeof(double) * 2, stream)) != cudaSuccess) return e;
+  if (cs.ncells <= 0) return cudaSuccess;
+  const size_t smem = 2 * (sizeof(double) * tile_doubles(rule.npts) + sizeof(int) * tile_ints(1) + 16) +
+                      sizeof(double) * (2 * kTile * 9 + 2) + 16;
+  dim3 grid((cs.ncells + kTile - 1) / kTile, (cs.ncells + kTile - 1) / kTile);
+  const double2* l2 = reinterpret_cast<const double2*>(lam);
+  const double2* m2 = reinterpret_cast<const double2*>(mu);
+  if (rule.npts == 6) {
+    auto fn = adjoint_sl_regular<6>;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    fn<<<grid, kThreads, smem, stream>>>(cs, rule, k, l2, m2, grad_cell, totals);
+  } else {
+    auto fn = adjoint_sl_regular<0>;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    fn<<<grid, kThreads, smem, stream>>>(cs, rule, k, l2, m2, grad_cell, totals);
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (pairs.npairs > 0) {
+    adjoint_sl_singular<<<(pairs.npairs + 7) / 8, 256, 0, stream>>>(cs, rules, pairs, k, l2, m2,
+                                                                   grad_cell, totals);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  cell_to_point_gradient<<<(cs.ncells + 255) / 256, 256, 0, stream>>>(cs, grad_cell, grad_points);
+  return cudaGetLastError();
+}
+
+}  // namespace bempp_b200

@@ -99,6 +99,36 @@ cudaError_t assemble_regular_dp0_noalloc(const RegularArgs& args, const RegularR
                                          const int* trial_cells, int trial_ncells,
                                          cudaStream_t stream);
 
+// Adjoint gradient of Re(lambda^H A mu) for the Helmholtz single layer on DP0 (adjoint.cu):
+// grad_points (npoints x 3) and totals = {J, dJ/dk}; grad_cell is F x 9 scratch.
+cudaError_t launch_adjoint_sl(const CellSet& cs, const RegularRule& rule,
+                              const SingularRules& rules, const SingularPairs& pairs, double k,
+                              const double* lam, const double* mu, double* grad_cell,
+                              double* grad_points, int npoints, double* totals,
+                              cudaStream_t stream);
+
+// Batched Helmholtz single-layer DP0 sweep (regular.cu): one persistent launch over
+// every (mesh, test tile, trial tile, wavenumber chunk) item; complex64 outputs.
+constexpr int kMaxSweepMeshes = 8;
+struct SweepMesh {
+  CellSet cells;          // geometry for the 6-point rule, with FP32 offsets
+  float2* out;            // nk column-major ncells x ncells matrices, wavenumber-major
+  int ntiles;             // ceil(ncells / 32)
+  long long item_begin;   // first work item of this mesh
+};
+struct SweepArgs {
+  SweepMesh mesh[kMaxSweepMeshes];
+  int nmesh;
+  const double* ks;       // device array of nk wavenumbers
+  int nk;
+  int kchunk;             // wavenumbers per work item
+  long long nitems;
+  unsigned long long* counter;  // work counter, zeroed before each launch
+};
+size_t sweep_smem_bytes();
+cudaError_t launch_sweep_sl(const SweepArgs& args, const RegularRule& rule,
+                            const SingularRules& rules, int blocks, cudaStream_t stream);
+
 // CUDA-core FMA throughput probe (diag.cu).
 cudaError_t measure_fma_peak(int fp64, int iters, int reps, double* tflops);
 

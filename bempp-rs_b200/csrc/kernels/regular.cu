@@ -33,83 +33,19 @@
 //   * Helmholtz: e^{ikr} = e^{ik r0} e^{ik delta}, r0 = |dc| in FP64, delta = r - r0 =
 //     (2 dc.D + D.D) / (r + r0), D = dx_p - dy_q, free of cancellation; e^{ik delta} from
 //     the Taylor series of cos / sin (degree 10 / 9, truncation < 3e-8) when
-//     |k delta| <= k (rad_x + rad_y) <= 0.8, else CUDA's sincosf; e^{ik r0} from an FP64
-//     reduction of k r0 modulo 2 pi followed by sincosf;
+//     |k delta| <= k (rad_x + rad_y) <= 0.8, else the same series after a Cody-Waite
+//     reduction by pi/2;
+//     e^{ik r0} from the same series after an FP64 reduction of k r0 by pi/2;
 //   * DP0 entries sum their 6 inner sums with Kahan compensation; P1 blocks are formed
 //     in FP32 and accumulated into the matrix in FP64.
 #include "launch.h"
+#include "tiles.cuh"
 
 namespace bempp_b200 {
 namespace {
 
-constexpr int kTile = 32;
-constexpr int kThreads = 128;
-constexpr int kWarps = kThreads / 32;
 constexpr float kTaylorMax = 0.8f;
-
-enum TileField : int {
-  fJdet = 0, fNx, fNy, fNz, fH, fT0x, fT0y, fT0z, fT1x, fT1y, fT1z, fCx, fCy, fCz, fDiam,
-  fRad, kTileFields
-};
-
-// Shared-memory image of a tile of kTile cells.
-struct Tile {
-  double* pts;  // [(q*3+d) * kTile + c] absolute FP64 points
-  float* rel;   // [(q*3+d) * kTile + c] FP32 offsets from the centroid (mixed only)
-  double* geo;  // [f * kTile + c]
-  int* vid;     // [v * kTile + c]
-  int* ldof;    // [b * kTile + c]
-  __device__ __forceinline__ double P(int q, int d, int c) const { return pts[(q * 3 + d) * kTile + c]; }
-  __device__ __forceinline__ float R(int q, int d, int c) const { return rel[(q * 3 + d) * kTile + c]; }
-  __device__ __forceinline__ double G(int f, int c) const { return geo[f * kTile + c]; }
-};
-
-__host__ __device__ inline size_t tile_doubles(int q) { return (3 * q + kTileFields) * kTile; }
-__host__ __device__ inline size_t tile_floats(int q, bool mixed) { return mixed ? 3 * q * kTile : 0; }
-__host__ __device__ inline size_t tile_ints(int nb) { return (3 + nb) * kTile; }
-
-// Carves a tile out of shared memory starting at *cursor (8-byte aligned).
-__device__ Tile carve_tile(unsigned char*& cursor, int q, bool mixed, int nb) {
-  Tile t;
-  t.pts = reinterpret_cast<double*>(cursor);
-  t.geo = t.pts + 3 * q * kTile;
-  cursor = reinterpret_cast<unsigned char*>(t.geo + kTileFields * kTile);
-  t.rel = reinterpret_cast<float*>(cursor);
-  cursor += sizeof(float) * tile_floats(q, mixed);
-  t.vid = reinterpret_cast<int*>(cursor);
-  t.ldof = t.vid + 3 * kTile;
-  cursor += sizeof(int) * tile_ints(nb);
-  cursor = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(cursor) + 15) & ~uintptr_t(15));
-  return t;
-}
-
-__device__ void load_tile(const Tile& t, const CellSet& cs, int c0, int n, int q, bool mixed,
-                          const uint8_t* cell_ldof, int nb) {
-  const int N = cs.ncells;
-  for (int idx = threadIdx.x; idx < 3 * q * kTile; idx += kThreads) {
-    const int c = idx % kTile, pd = idx / kTile;
-    const int64_t src = static_cast<int64_t>(pd) * N + c0 + min(c, n - 1);
-    t.pts[idx] = __ldg(cs.qpts + src);
-    if (mixed) t.rel[idx] = __ldg(cs.qrel + src);
-  }
-  for (int c = threadIdx.x; c < kTile; c += kThreads) {
-    const int cell = c0 + min(c, n - 1);
-    const double nx = g(cs.geom, kNx, N, cell), ny = g(cs.geom, kNy, N, cell),
-                 nz = g(cs.geom, kNz, N, cell);
-    t.geo[fJdet * kTile + c] = g(cs.geom, kJdet, N, cell);
-    t.geo[fNx * kTile + c] = nx;
-    t.geo[fNy * kTile + c] = ny;
-    t.geo[fNz * kTile + c] = nz;
-    t.geo[fH * kTile + c] = g(cs.geom, kV0x, N, cell) * nx + g(cs.geom, kV0y, N, cell) * ny +
-                            g(cs.geom, kV0z, N, cell) * nz;
-    for (int f = 0; f < 6; ++f) t.geo[(fT0x + f) * kTile + c] = g(cs.geom, kT0x + f, N, cell);
-    for (int f = 0; f < 3; ++f) t.geo[(fCx + f) * kTile + c] = g(cs.geom, kCx + f, N, cell);
-    t.geo[fDiam * kTile + c] = g(cs.geom, kDiam, N, cell);
-    t.geo[fRad * kTile + c] = g(cs.geom, kRad, N, cell);
-    for (int v = 0; v < 3; ++v) t.vid[v * kTile + c] = c < n ? __ldg(cs.vids + v * N + cell) : -1 - v;
-    for (int b = 0; b < nb; ++b) t.ldof[b * kTile + c] = cell_ldof ? cell_ldof[cell * nb + b] : 0;
-  }
-}
+using namespace tiles;
 
 __device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
   const float y = v - comp;
@@ -118,7 +54,8 @@ __device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
   sum = t;
 }
 
-// cos(t), sin(t) for |t| <= 0.8 from their Taylor series (degree 10 and 9).
+// cos(t), sin(t) for |t| <= pi/4 from their Taylor series (degree 10 and 9; the first
+// omitted terms are below 3e-8 there).
 __device__ __forceinline__ void taylor_cos_sin(float t, float& c, float& s) {
   const float z = t * t;
   c = fmaf(z, fmaf(z, fmaf(z, fmaf(z, fmaf(z, -2.7557319e-7f, 2.4801587e-5f), -1.3888889e-3f),
@@ -186,7 +123,7 @@ __device__ __forceinline__ void finish_block(const Tile& T, int it, const Tile& 
 }
 
 // FP64 local block of test cell `it` (tile T) and trial cell `js` (tile S).
-template <int QT, int KER, int OP, int NBT, int NBS>
+template <int QT, int KER, int OP, int NBT, int NBS, bool kUnroll = true>
 __device__ __forceinline__ void block_fp64(const Tile& T, int it, const Tile& S, int js,
                                         const RegularRule& rule, double k,
                                         double ore[NBT][NBS], double oim[NBT][NBS]) {
@@ -208,7 +145,7 @@ __device__ __forceinline__ void block_fp64(const Tile& T, int it, const Tile& S,
     double u_re[NBS], u_im[NBS], g_re = 0.0, g_im = 0.0;
 #pragma unroll
     for (int b = 0; b < NBS; ++b) u_re[b] = u_im[b] = 0.0;
-#pragma unroll 6
+#pragma unroll(kUnroll ? 6 : 1)
     for (int q = 0; q < Q; ++q) {
       const double y0 = S.P(q, 0, js), y1 = S.P(q, 1, js), y2 = S.P(q, 2, js);
       const double dx = x0 - y0, dy = x1 - y1, dz = x2 - y2;
@@ -270,99 +207,113 @@ __device__ __forceinline__ void block_fp64(const Tile& T, int it, const Tile& S,
   finish_block<KER, OP, NBT, NBS>(T, it, S, js, k, blk_re, blk_im, S_re, S_im, ore, oim);
 }
 
-// FP32 local block of a far pair (see the file comment for the formulation).
-template <int QT, int KER, int OP, int NBT, int NBS>
-__device__ __forceinline__ void block_fp32(const Tile& T, int it, const Tile& S, int js,
-                                           const RegularRule& rule, double k,
-                                           double ore[NBT][NBS], double oim[NBT][NBS]) {
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// cos and sin of an argument of any moderate size: Cody-Waite reduction by multiples of
+// pi/2 (two-part constant) to |r| <= pi/4, Taylor series there (truncation < 3e-8), and
+// the quadrant's exchange of sine and cosine.  FP32 arguments up to a few hundred.
+__device__ __forceinline__ void reduced_cos_sin(float t, float& c, float& s) {
+  const float n = rintf(t * 0.636619772f);
+  float r = fmaf(-n, 1.57079637f, t);
+  r = fmaf(-n, -4.37113883e-8f, r);
+  float cr, sr;
+  taylor_cos_sin(r, cr, sr);
+  const int q = static_cast<int>(n) & 3;
+  c = (q == 0) ? cr : (q == 1) ? -sr : (q == 2) ? -cr : sr;
+  s = (q == 0) ? sr : (q == 1) ? cr : (q == 2) ? -sr : -cr;
+}
+
+// e^{i theta} for an FP64 angle: the reduction by pi/2 in FP64 (two-part constant), the
+// series and the quadrant in FP32; absolute error ~1e-7.
+__device__ __forceinline__ void phase_cos_sin(double theta, float& c, float& s) {
+  const double n = rint(theta * 0.63661977236758134308);
+  double r = fma(-n, 1.5707963267948966192, theta);
+  r = fma(-n, 6.1232339957367660359e-17, r);
+  float cr, sr;
+  taylor_cos_sin(static_cast<float>(r), cr, sr);
+  const int q = static_cast<int>(static_cast<long long>(n) & 3);
+  c = (q == 0) ? cr : (q == 1) ? -sr : (q == 2) ? -cr : sr;
+  s = (q == 0) ? sr : (q == 1) ? cr : (q == 2) ? -sr : -cr;
+}
+
+// Per-pair constants of the FP32 far-pair quadrature.
+template <int QT>
+struct FarPair {
+  static constexpr int kCap = QT > 0 ? QT : kMaxRegularPoints;
+  float fdx, fdy, fdz;      // dc = c_x - c_y in FP32
+  float fa0, fa1, fa2;      // normal-derivative factors in tangent coordinates
+  float r0f, r0sq, kf;      // Helmholtz: reference distance and wavenumber
+  float yx[kCap], yy[kCap], yz[kCap];  // trial points relative to c_y
+  float wq[kCap];           // trial weights (times the ADL factor)
+  float beta[kCap];         // 2 dc . dy_q (Helmholtz)
+};
+
+// Sums of one far pair in FP32: blk[a][b] and S (see block_fp64 for their meaning),
+// without the reference phase e^{ik r0}.
+template <int QT, int KER, int OP, int NBT, int NBS, bool kTaylorOnly>
+__device__ __forceinline__ void far_sums(const Tile& T, int it, const Tile& S, int js,
+                                         const RegularRule& rule, const FarPair<QT>& fp,
+                                         float blk_re[NBT][NBS],
+                                         float blk_im[NBT][NBS], float& S_re, float& S_im) {
   constexpr bool kC = KER == kHelmholtz;
   constexpr bool kNeedBasis = OP != kHS || kC;
   constexpr bool kKahan = NBT == 1 && NBS == 1;
   const int Q = QT > 0 ? QT : rule.npts;
-  const double dcx = T.G(fCx, it) - S.G(fCx, js), dcy = T.G(fCy, it) - S.G(fCy, js),
-               dcz = T.G(fCz, it) - S.G(fCz, js);
-  const float fdx = static_cast<float>(dcx), fdy = static_cast<float>(dcy),
-              fdz = static_cast<float>(dcz);
-  // normal-derivative factors in tangent coordinates
-  float fa0 = 0.f, fa1 = 0.f, fa2 = 0.f;
-  if (OP == kDL) {
-    const double nx = S.G(fNx, js), ny = S.G(fNy, js), nz = S.G(fNz, js);
-    fa0 = static_cast<float>(dcx * nx + dcy * ny + dcz * nz);
-    fa1 = static_cast<float>(T.G(fT0x, it) * nx + T.G(fT0y, it) * ny + T.G(fT0z, it) * nz);
-    fa2 = static_cast<float>(T.G(fT1x, it) * nx + T.G(fT1y, it) * ny + T.G(fT1z, it) * nz);
-  } else if (OP == kADL) {
-    const double nx = T.G(fNx, it), ny = T.G(fNy, it), nz = T.G(fNz, it);
-    fa0 = static_cast<float>(-(dcx * nx + dcy * ny + dcz * nz));
-    fa1 = static_cast<float>(S.G(fT0x, js) * nx + S.G(fT0y, js) * ny + S.G(fT0z, js) * nz);
-    fa2 = static_cast<float>(S.G(fT1x, js) * nx + S.G(fT1y, js) * ny + S.G(fT1z, js) * nz);
-  }
-  float r0f = 0.f, r0sq = 0.f, kf = 0.f, ph_c = 1.f, ph_s = 0.f;
-  bool taylor = false;
-  if (kC) {
-    const double r0 = sqrt(dcx * dcx + dcy * dcy + dcz * dcz);
-    r0f = static_cast<float>(r0);
-    r0sq = r0f * r0f;
-    kf = static_cast<float>(k);
-    // e^{ik r0}: k r0 reduced modulo 2 pi in FP64, then FP32 sincos of the remainder
-    const double theta = k * r0;
-    const double turns = rint(theta * 0.15915494309189533577);
-    const double red = fma(-turns, 6.28318530717958647692, theta);
-    sincosf(static_cast<float>(red), &ph_s, &ph_c);
-    taylor = k * (T.G(fRad, it) + S.G(fRad, js)) <= static_cast<double>(kTaylorMax);
-  }
-  // per-pair factors of each trial point: ADL weight factor and 2 dc.dy_q
-  constexpr int kCap = QT > 0 ? QT : kMaxRegularPoints;
-  float wq_s[kCap], beta_s[kCap];
-#pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    wq_s[q] = OP == kADL ? rule.wf[q] * fmaf(rule.uf[q], fa1, fmaf(rule.vf[q], fa2, fa0))
-                         : rule.wf[q];
-    if (kC) beta_s[q] = 2.f * fmaf(fdx, S.R(q, 0, js), fmaf(fdy, S.R(q, 1, js), fdz * S.R(q, 2, js)));
-  }
-  float blk_re[NBT][NBS], blk_im[NBT][NBS], cmp_re = 0.f, cmp_im = 0.f;
-  float S_re = 0.f, S_im = 0.f;
-#pragma unroll
-  for (int a = 0; a < NBT; ++a)
-#pragma unroll
-    for (int b = 0; b < NBS; ++b) blk_re[a][b] = blk_im[a][b] = 0.f;
+  float cmp_re = 0.f, cmp_im = 0.f;
 #pragma unroll 1
   for (int p = 0; p < Q; ++p) {
     const float ax = T.R(p, 0, it), ay = T.R(p, 1, it), az = T.R(p, 2, it);
-    const float apf = OP == kDL ? fmaf(rule.uf[p], fa1, fmaf(rule.vf[p], fa2, fa0)) : 1.f;
-    const float alpha = kC ? 2.f * fmaf(fdx, ax, fmaf(fdy, ay, fdz * az)) : 0.f;
-    const float px = fdx + ax, py = fdy + ay, pz = fdz + az;
+    const float apf = OP == kDL ? fmaf(rule.uf[p], fp.fa1, fmaf(rule.vf[p], fp.fa2, fp.fa0)) : 1.f;
+    const float alpha = kC ? 2.f * fmaf(fp.fdx, ax, fmaf(fp.fdy, ay, fp.fdz * az)) : 0.f;
+    const float px = fp.fdx + ax, py = fp.fdy + ay, pz = fp.fdz + az;
     float u_re[NBS], u_im[NBS], g_re = 0.f, g_im = 0.f;
 #pragma unroll
     for (int b = 0; b < NBS; ++b) u_re[b] = u_im[b] = 0.f;
-#pragma unroll 6
+#pragma unroll(kTaylorOnly ? 6 : 1)
     for (int q = 0; q < Q; ++q) {
-      const float yx = S.R(q, 0, js), yy = S.R(q, 1, js), yz = S.R(q, 2, js);
-      const float wq = wq_s[q];
+      // the general (rare) path reads the trial data from shared memory so that the
+      // per-pair register arrays are only indexed by compile-time constants
+      const float yq0 = kTaylorOnly ? fp.yx[q] : S.R(q, 0, js);
+      const float yq1 = kTaylorOnly ? fp.yy[q] : S.R(q, 1, js);
+      const float yq2 = kTaylorOnly ? fp.yz[q] : S.R(q, 2, js);
+      const float wq = kTaylorOnly ? fp.wq[q]
+                       : (OP == kADL ? rule.wf[q] * fmaf(rule.uf[q], fp.fa1, fmaf(rule.vf[q], fp.fa2, fp.fa0))
+                                     : rule.wf[q]);
+      const float beta_q = kTaylorOnly ? fp.beta[q]
+                           : 2.f * fmaf(fp.fdx, yq0, fmaf(fp.fdy, yq1, fp.fdz * yq2));
       float kre, kim = 0.f;
       if (!kC) {
-        const float dx = px - yx, dy = py - yy, dz = pz - yz;
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        const float rinv = rsqrtf(r2);
+        const float dx = px - yq0, dy = py - yq1, dz = pz - yq2;
+        const float rinv = rsqrt_approx(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
         kre = (OP == kSL || OP == kHS) ? wq * rinv : wq * (rinv * rinv * rinv);
       } else {
-        const float Dx = ax - yx, Dy = ay - yy, Dz = az - yz;
-        const float s = (alpha - beta_s[q]) + fmaf(Dx, Dx, fmaf(Dy, Dy, Dz * Dz));  // r^2 - r0^2
-        const float r2 = r0sq + s;
-        const float rinv = rsqrtf(r2);
+        const float Dx = ax - yq0, Dy = ay - yq1, Dz = az - yq2;
+        const float s = (alpha - beta_q) + fmaf(Dx, Dx, fmaf(Dy, Dy, Dz * Dz));
+        const float r2 = fp.r0sq + s;
+        const float rinv = rsqrt_approx(r2);
         const float r = r2 * rinv;
-        const float t = kf * __fdividef(s, r + r0f);
+        const float t = fp.kf * s * rcp_approx(r + fp.r0f);  // k (r - r0)
         float cs, sn;
-        if (taylor)
+        if (kTaylorOnly)
           taylor_cos_sin(t, cs, sn);
         else
-          sincosf(t, &sn, &cs);
+          reduced_cos_sin(t, cs, sn);
         if (OP == kSL || OP == kHS) {
           const float f = wq * rinv;
           kre = f * cs;
           kim = f * sn;
         } else {
-          const float f = wq * (rinv * rinv * rinv), kr = kf * r;
-          // (1 - ik r) e^{ik r} = (1 - ik r) e^{ik r0} e^{ik delta}; e^{ik r0} applied below
+          // (1 - ik r) e^{ik r} / r^3 with e^{ik r0} applied per pair
+          const float f = wq * (rinv * rinv * rinv), kr = fp.kf * r;
           kre = f * fmaf(kr, sn, cs);
           kim = f * fmaf(-kr, cs, sn);
         }
@@ -406,12 +357,68 @@ __device__ __forceinline__ void block_fp32(const Tile& T, int it, const Tile& S,
       }
     }
   }
+}
+
+// FP32 local block of a far pair (see the file comment for the formulation).
+template <int QT, int KER, int OP, int NBT, int NBS>
+__device__ __forceinline__ void block_fp32(const Tile& T, int it, const Tile& S, int js,
+                                           const RegularRule& rule, double k,
+                                           double ore[NBT][NBS], double oim[NBT][NBS]) {
+  constexpr bool kC = KER == kHelmholtz;
+  const int Q = QT > 0 ? QT : rule.npts;
+  FarPair<QT> fp;
+  const double dcx = T.G(fCx, it) - S.G(fCx, js), dcy = T.G(fCy, it) - S.G(fCy, js),
+               dcz = T.G(fCz, it) - S.G(fCz, js);
+  fp.fdx = static_cast<float>(dcx);
+  fp.fdy = static_cast<float>(dcy);
+  fp.fdz = static_cast<float>(dcz);
+  fp.fa0 = fp.fa1 = fp.fa2 = 0.f;
+  if (OP == kDL) {
+    const double nx = S.G(fNx, js), ny = S.G(fNy, js), nz = S.G(fNz, js);
+    fp.fa0 = static_cast<float>(dcx * nx + dcy * ny + dcz * nz);
+    fp.fa1 = static_cast<float>(T.G(fT0x, it) * nx + T.G(fT0y, it) * ny + T.G(fT0z, it) * nz);
+    fp.fa2 = static_cast<float>(T.G(fT1x, it) * nx + T.G(fT1y, it) * ny + T.G(fT1z, it) * nz);
+  } else if (OP == kADL) {
+    const double nx = T.G(fNx, it), ny = T.G(fNy, it), nz = T.G(fNz, it);
+    fp.fa0 = static_cast<float>(-(dcx * nx + dcy * ny + dcz * nz));
+    fp.fa1 = static_cast<float>(S.G(fT0x, js) * nx + S.G(fT0y, js) * ny + S.G(fT0z, js) * nz);
+    fp.fa2 = static_cast<float>(S.G(fT1x, js) * nx + S.G(fT1y, js) * ny + S.G(fT1z, js) * nz);
+  }
+  float ph_c = 1.f, ph_s = 0.f;
+  bool taylor = true;
+  fp.r0f = fp.r0sq = fp.kf = 0.f;
+  if (kC) {
+    const double r0 = sqrt(dcx * dcx + dcy * dcy + dcz * dcz);
+    fp.r0f = static_cast<float>(r0);
+    fp.r0sq = fp.r0f * fp.r0f;
+    fp.kf = static_cast<float>(k);
+    phase_cos_sin(k * r0, ph_c, ph_s);
+    taylor = k * (T.G(fRad, it) + S.G(fRad, js)) <= static_cast<double>(kTaylorMax);
+  }
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    fp.yx[q] = S.R(q, 0, js);
+    fp.yy[q] = S.R(q, 1, js);
+    fp.yz[q] = S.R(q, 2, js);
+    fp.wq[q] = OP == kADL ? rule.wf[q] * fmaf(rule.uf[q], fp.fa1, fmaf(rule.vf[q], fp.fa2, fp.fa0))
+                          : rule.wf[q];
+    if (kC) fp.beta[q] = 2.f * fmaf(fp.fdx, fp.yx[q], fmaf(fp.fdy, fp.yy[q], fp.fdz * fp.yz[q]));
+  }
+  float blk_re[NBT][NBS], blk_im[NBT][NBS], S_re = 0.f, S_im = 0.f;
+#pragma unroll
+  for (int a = 0; a < NBT; ++a)
+#pragma unroll
+    for (int b = 0; b < NBS; ++b) blk_re[a][b] = blk_im[a][b] = 0.f;
+  if (!kC || taylor)
+    far_sums<QT, KER, OP, NBT, NBS, true>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
+  else
+    far_sums<QT, KER, OP, NBT, NBS, false>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
   // back to FP64, applying the reference phase e^{ik r0}
   double bre[NBT][NBS], bim[NBT][NBS];
   double Sre = S_re, Sim = S_im;
+  const double pc = ph_c, ps = ph_s;
   if (kC) {
-    const double c = ph_c, s = ph_s;
-    const double re = Sre * c - Sim * s, im = Sre * s + Sim * c;
+    const double re = Sre * pc - Sim * ps, im = Sre * ps + Sim * pc;
     Sre = re;
     Sim = im;
   }
@@ -421,8 +428,7 @@ __device__ __forceinline__ void block_fp32(const Tile& T, int it, const Tile& S,
     for (int b = 0; b < NBS; ++b) {
       double re = blk_re[a][b], im = blk_im[a][b];
       if (kC) {
-        const double c = ph_c, s = ph_s;
-        const double r2 = re * c - im * s, i2 = re * s + im * c;
+        const double r2 = re * pc - im * ps, i2 = re * ps + im * pc;
         re = r2;
         im = i2;
       }
@@ -537,7 +543,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     for (int e = threadIdx.x; e < nq; e += kThreads) {
       const int pi = queue[e] & 0xff, pj = queue[e] >> 8;
       double ore[NBT][NBS], oim[NBT][NBS];
-      block_fp64<QT, KER, OP, NBT, NBS>(T, pi, S, pj, rule, k, ore, oim);
+      block_fp64<QT, KER, OP, NBT, NBS, false>(T, pi, S, pj, rule, k, ore, oim);
       if (DIRECT) {
         const int64_t o = static_cast<int64_t>(sj0 + pj) * ld + ti0 + pi;
         if (kC)
@@ -567,6 +573,164 @@ __global__ void __launch_bounds__(kThreads, 4)
         atomicAdd(out + o, re);
       }
     }
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Batched Helmholtz single-layer DP0 sweep over many wavenumbers and meshes.
+//
+// One persistent launch: every CTA repeatedly takes the next work item (mesh, test tile,
+// trial tile, chunk of wavenumbers) from a global counter (items of the largest mesh
+// first), stages the two tiles once, and for each wavenumber of its chunk writes the
+// complete 32 x 32 block of complex64 entries: far pairs in FP32 (block_fp32), near pairs
+// in FP64 (block_fp64), vertex-sharing pairs by their Duffy rule in FP64 (one warp per
+// pair).  No two items write the same entry, so the launch needs no ordering or atomics
+// on the output; the only shared state is the item counter (reset before every launch).
+
+// Adjacency configuration (0..27, the order of singular_configurations()) of two cells
+// with vertex ids a[3] (test) and b[3] (trial) that share at least one vertex.
+__device__ __forceinline__ int adjacency_config(const int a[3], const int b[3], bool same) {
+  if (same) return 27;
+  int ts[3], ss[3], n = 0;
+  for (int si = 0; si < 3; ++si)
+    for (int ti = 0; ti < 3; ++ti)
+      if (a[ti] == b[si]) {
+        ts[n] = ti;
+        ss[n] = si;
+        ++n;
+      }
+  if (n == 1) return ts[0] * 3 + ss[0];
+  // edge: test edge opposite vertex 3 - t0 - t1, trial edge opposite 3 - s0 - s1
+  const int et = 3 - ts[0] - ts[1], es = 3 - ss[0] - ss[1];
+  return 9 + (et * 3 + es) * 2 + (ts[0] < ts[1] ? 0 : 1);
+}
+
+// Single-layer integral of one vertex-sharing pair over its Duffy rule (FP64), summed by
+// a warp; every lane returns the total.
+__device__ void duffy_sl_dp0_warp(const Tile& T, int it, const Tile& S, int js, int cfg,
+                                  const SingularRules& rules, double k, double& re, double& im) {
+  const int lane = threadIdx.x & 31;
+  double v0x[3], t0x[3], t1x[3], v0y[3], t0y[3], t1y[3];
+  for (int d = 0; d < 3; ++d) {
+    t0x[d] = T.G(fT0x + d, it);
+    t1x[d] = T.G(fT1x + d, it);
+    v0x[d] = T.G(fCx + d, it) - (t0x[d] + t1x[d]) / 3.0;
+    t0y[d] = S.G(fT0x + d, js);
+    t1y[d] = S.G(fT1x + d, js);
+    v0y[d] = S.G(fCx + d, js) - (t0y[d] + t1y[d]) / 3.0;
+  }
+  const int off = __ldg(rules.offset + cfg), npts = __ldg(rules.offset + cfg + 1) - off;
+  double sr = 0.0, si = 0.0;
+  for (int ii = lane; ii < npts; ii += 32) {
+    const int i = off + ii;
+    const double xi0 = __ldg(rules.test_xi + 2 * i), xi1 = __ldg(rules.test_xi + 2 * i + 1);
+    const double et0 = __ldg(rules.trial_xi + 2 * i), et1 = __ldg(rules.trial_xi + 2 * i + 1);
+    const double w = __ldg(rules.w + i);
+    double r2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      const double dd = (v0x[d] + xi0 * t0x[d] + xi1 * t1x[d]) - (v0y[d] + et0 * t0y[d] + et1 * t1y[d]);
+      r2 += dd * dd;
+    }
+    const double rinv = rsqrt(r2);
+    double sn, cs;
+    sincos(k * r2 * rinv, &sn, &cs);
+    sr = fma(w * rinv, cs, sr);
+    si = fma(w * rinv, sn, si);
+  }
+  for (int s = 16; s > 0; s >>= 1) {
+    sr += __shfl_xor_sync(0xffffffffu, sr, s);
+    si += __shfl_xor_sync(0xffffffffu, si, s);
+  }
+  const double sc = T.G(fJdet, it) * S.G(fJdet, js) * kInv4Pi;
+  re = sr * sc;
+  im = si * sc;
+}
+
+__global__ void __launch_bounds__(kThreads)
+    sweep_sl_dp0(SweepArgs a, RegularRule rule, SingularRules rules) {
+  const int Q = 6;
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned char* cursor = smem;
+  const Tile T = carve_tile(cursor, Q, true, 1);
+  const Tile S = carve_tile(cursor, Q, true, 1);
+  unsigned short* nearq = reinterpret_cast<unsigned short*>(cursor);
+  unsigned short* adjq = nearq + kTile * kTile;
+  unsigned char* adjc = reinterpret_cast<unsigned char*>(adjq + kTile * kTile);
+  int* counts = reinterpret_cast<int*>(adjc + kTile * kTile);  // near, adjacent
+  long long* s_item = reinterpret_cast<long long*>(counts + 2);
+  const int it = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      *s_item = static_cast<long long>(atomicAdd(a.counter, 1ull));
+      counts[0] = counts[1] = 0;
+    }
+    __syncthreads();
+    const long long item = *s_item;
+    if (item >= a.nitems) break;
+    int m = 0;
+    while (m + 1 < a.nmesh && item >= a.mesh[m + 1].item_begin) ++m;
+    const SweepMesh& M = a.mesh[m];
+    const long long local = item - M.item_begin;
+    const int nchunks = (a.nk + a.kchunk - 1) / a.kchunk;
+    const int kc = static_cast<int>(local % nchunks);
+    const long long tp = local / nchunks;
+    const int tt = static_cast<int>(tp / M.ntiles), st = static_cast<int>(tp % M.ntiles);
+    const int nc = M.cells.ncells;
+    const int ti0 = tt * kTile, sj0 = st * kTile;
+    const int nti = min(kTile, nc - ti0), nsj = min(kTile, nc - sj0);
+    load_tile(T, M.cells, ti0, nti, Q, true, nullptr, 1);
+    load_tile(S, M.cells, sj0, nsj, Q, true, nullptr, 1);
+    __syncthreads();
+    // classify the tile pair once: vertex-sharing and near pairs are queued
+    if (it < nti) {
+      const int av[3] = {T.vid[it], T.vid[kTile + it], T.vid[2 * kTile + it]};
+      for (int js = warp; js < nsj; js += kWarps) {
+        const int bv[3] = {S.vid[js], S.vid[kTile + js], S.vid[2 * kTile + js]};
+        if (share_vertex(av[0], av[1], av[2], bv[0], bv[1], bv[2])) {
+          const int slot = atomicAdd(counts + 1, 1);
+          adjq[slot] = static_cast<unsigned short>(it | (js << 8));
+          adjc[slot] = static_cast<unsigned char>(adjacency_config(av, bv, ti0 + it == sj0 + js));
+        } else if (near_pair(T, it, S, js)) {
+          const int slot = atomicAdd(counts, 1);
+          nearq[slot] = static_cast<unsigned short>(it | (js << 8));
+        }
+      }
+    }
+    __syncthreads();
+    const int nnear = counts[0], nadj = counts[1];
+    const int k0 = kc * a.kchunk, k1 = min(a.nk, k0 + a.kchunk);
+    for (int kk = k0; kk < k1; ++kk) {
+      const double k = a.ks[kk];
+      float2* out = M.out + static_cast<long long>(kk) * nc * nc;
+      if (it < nti) {
+        const int a0 = T.vid[it], a1 = T.vid[kTile + it], a2 = T.vid[2 * kTile + it];
+        for (int js = warp; js < nsj; js += kWarps) {
+          if (share_vertex(a0, a1, a2, S.vid[js], S.vid[kTile + js], S.vid[2 * kTile + js]) ||
+              near_pair(T, it, S, js))
+            continue;
+          double ore[1][1], oim[1][1];
+          block_fp32<6, kHelmholtz, kSL, 1, 1>(T, it, S, js, rule, k, ore, oim);
+          out[static_cast<long long>(sj0 + js) * nc + ti0 + it] =
+              make_float2(static_cast<float>(ore[0][0]), static_cast<float>(oim[0][0]));
+        }
+      }
+      for (int e = threadIdx.x; e < nnear; e += kThreads) {
+        const int pi = nearq[e] & 0xff, pj = nearq[e] >> 8;
+        double ore[1][1], oim[1][1];
+        block_fp64<6, kHelmholtz, kSL, 1, 1, false>(T, pi, S, pj, rule, k, ore, oim);
+        out[static_cast<long long>(sj0 + pj) * nc + ti0 + pi] =
+            make_float2(static_cast<float>(ore[0][0]), static_cast<float>(oim[0][0]));
+      }
+      for (int e = warp; e < nadj; e += kWarps) {
+        const int pi = adjq[e] & 0xff, pj = adjq[e] >> 8;
+        double re, im;
+        duffy_sl_dp0_warp(T, pi, S, pj, adjc[e], rules, k, re, im);
+        if (it == 0)
+          out[static_cast<long long>(sj0 + pj) * nc + ti0 + pi] =
+              make_float2(static_cast<float>(re), static_cast<float>(im));
+      }
+    }
+    __syncthreads();  // the tiles and queues are reused by the next item
   }
 }
 
@@ -655,6 +819,28 @@ cudaError_t dispatch(const CellSet& test, const SpaceTiles& tt, const CellSet& t
 }  // namespace
 
 int scatter_tile_cells() { return kTile; }
+
+size_t sweep_smem_bytes() {
+  size_t b = 0;
+  for (int t = 0; t < 2; ++t) {
+    b += sizeof(double) * tile_doubles(6) + sizeof(float) * tile_floats(6, true) +
+         sizeof(int) * tile_ints(1);
+    b = (b + 15) & ~size_t(15);
+  }
+  return b + 2 * sizeof(unsigned short) * kTile * kTile + kTile * kTile + 2 * sizeof(int) +
+         sizeof(long long) + 32;
+}
+
+cudaError_t launch_sweep_sl(const SweepArgs& args, const RegularRule& rule,
+                            const SingularRules& rules, int blocks, cudaStream_t stream) {
+  if (rule.npts != 6) return cudaErrorInvalidValue;
+  const size_t smem = sweep_smem_bytes();
+  cudaError_t e = cudaFuncSetAttribute(sweep_sl_dp0, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  sweep_sl_dp0<<<blocks, kThreads, smem, stream>>>(args, rule, rules);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_regular_dp0(const CellSet& test, const CellSet& trial,
                                const RegularRule& rule, const RegularArgs& a,

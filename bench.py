@@ -86,6 +86,20 @@ def workload_mesh(w, level=None):
     return pts, cells
 
 
+def max_over_ranks(x: float, world: int) -> float:
+    """The maximum of x over all ranks (device time of a multi-rank run is the slowest
+    rank's); a no-op for one rank.  Works on NCCL (CUDA tensor) and gloo (CPU tensor)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -296,6 +310,117 @@ def north_star(args):
     return res
 
 
+def adjoint_timing(args):
+    """Config 5: gradient of Re(lambda^H A mu) (Helmholtz SL, DP0, k = 5, perturbed
+    5,120-triangle icosphere) against one FP64 forward assembly, device times."""
+    import torch
+
+    from bempp import shapes
+    from bempp._lib import check, ffi, lib
+    from bempp.assembly.boundary import (BoundaryAssemblerOptions, OperatorType,
+                                         create_helmholtz_assembler)
+    from bempp.function_space import recreate_grid
+    from ndelement.reference_cell import ReferenceCellType
+
+    k = 5.0
+    pts, cells = shapes.icosphere(4)
+    pts = shapes.radial_perturbation(pts, 5120)
+    rng = np.random.default_rng(5)
+    n = len(cells)
+    lam = torch.as_tensor(rng.standard_normal(n) + 1j * rng.standard_normal(n), device="cuda")
+    mu = torch.as_tensor(rng.standard_normal(n) + 1j * rng.standard_normal(n), device="cuda")
+    grid, space = build_space(pts, cells, "dp0")
+    opts = BoundaryAssemblerOptions()
+    opts.set_regular_quadrature_degree(ReferenceCellType.Triangle, Q_REGULAR)
+    a = create_helmholtz_assembler(OperatorType.SingleLayer, k, opts)
+    out = torch.empty((n, n), dtype=torch.complex128, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    gopts = BoundaryAssemblerOptions()
+    gopts.set_regular_quadrature_degree(ReferenceCellType.Triangle, Q_REGULAR)
+    g = grid._bempp_rs_grid  # the grid handle shared by the space
+    tot = torch.zeros(2, dtype=torch.float64, device="cuda")
+    grad = torch.zeros((len(pts), 3), dtype=torch.float64, device="cuda")
+
+    def forward():
+        a.assemble_into_device(space, space, out, stream)
+        return torch.real(torch.vdot(lam, out.T @ mu))
+
+    def gradient():
+        check(lib.bempp_helmholtz_single_layer_dp0_gradient_device(
+            g, gopts._rs_options, k, ffi.cast("void*", lam.data_ptr()),
+            ffi.cast("void*", mu.data_ptr()), ffi.cast("double*", tot.data_ptr()),
+            ffi.cast("double*", grad.data_ptr()), ffi.cast("void*", stream)), "gradient")
+
+    def timed(fn, reps):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(reps):
+            fn()
+        t1.record()
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1) / reps
+
+    f_ms = timed(forward, 5)
+    g_ms = timed(gradient, 5)
+    jf = forward().item()
+    gradient()
+    torch.cuda.synchronize()
+    return {"workload": "helmholtz_sl_dp0_ico4_k5_gradient", "forward_ms": f_ms,
+            "gradient_ms": g_ms, "gradient_over_forward": g_ms / f_ms,
+            "J_forward": jf, "J_adjoint": tot[0].item(),
+            "note": "forward = dense FP64 assembly into HBM + Re(lambda^H A mu); gradient = "
+                    "one adjoint pass (all 7686 coordinates and k)"}
+
+
+def sweep_timing(args):
+    """Config 4: Helmholtz SL DP0 sweep, 32 wavenumbers in [1, 20], three stretched
+    icospheres (1,280 / 5,120 / 20,480 triangles, axes U(0.8, 1.2) with seeds 1280 / 5120 /
+    20480); complex64 outputs (114 GB) resident in HBM; one graph launch per sweep."""
+    import torch
+
+    from bempp import shapes
+    from bempp.sweep import helmholtz_single_layer_sweep, last_tuning
+    from ndgrid.grid import Grid
+
+    ks = np.linspace(1.0, 20.0, 32)
+    grids = []
+    for level, seed in ((3, 1280), (4, 5120), (5, 20480)):
+        pts, cells = shapes.icosphere(level)
+        grids.append(Grid(shapes.ellipsoidal_stretch(pts, seed), cells))
+    need = sum(len(ks) * len(g.cells) ** 2 * 8 for g in grids)
+    free, _ = torch.cuda.mem_get_info()
+    if free < need + (8 << 30):
+        return {"skipped": f"needs {need / 1e9:.1f} GB of free device memory, {free / 1e9:.1f} GB free"}
+    outs = [torch.empty((len(ks), len(g.cells), len(g.cells)), dtype=torch.complex64,
+                        device="cuda") for g in grids]
+    t = time.perf_counter()
+    helmholtz_single_layer_sweep(grids, ks, outs)  # autotune + capture + first launch
+    torch.cuda.synchronize()
+    first_s = time.perf_counter() - t
+    reps = 2
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        helmholtz_single_layer_sweep(grids, ks, outs)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    entries = sum(len(ks) * len(g.cells) ** 2 for g in grids)
+    kc, bps, probe = last_tuning()
+    del outs
+    torch.cuda.empty_cache()
+    return {"workload": "helmholtz_sl_dp0_sweep_32k_ico3_4_5_c64", "entries": entries,
+            "ms_per_sweep": ms, "entries_per_s": entries / (ms * 1e-3),
+            "first_call_s": first_s, "tuning": {"k_per_item": kc, "ctas_per_sm": bps,
+                                                "probe_ms_per_item": probe},
+            "launches_per_sweep": 1}
+
+
 def run_ours(args):
     import torch
 
@@ -333,12 +458,7 @@ def run_ours(args):
     time.sleep(0.3)
     ms_per_step, launches = wl.timed(args.steps, 1, barrier)
     clocks = sampler.stop()
-    if world > 1:
-        import torch.distributed as dist
-
-        tt = torch.tensor([ms_per_step], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_per_step = float(tt.item())
+    ms_per_step = max_over_ranks(ms_per_step, world)
     value = world * wl.entries_per_step / (ms_per_step * 1e-3)
 
     e2e = None
@@ -355,12 +475,7 @@ def run_ours(args):
                 a.assemble(s2, s2)
             del s2
         e2e_s = (time.perf_counter() - t) / e2e_steps
-        if world > 1:
-            import torch.distributed as dist
-
-            tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_s = float(tt.item())
+        e2e_s = max_over_ranks(e2e_s, world)
         esize = 16 if w["kernel"] == "helmholtz" else 8
         e2e = {"value": world * wl.entries_per_step / e2e_s, "unit": "entries/s",
                "h2d_bytes_per_step": int(pts_h.nbytes + cells_h.astype(np.uintp).nbytes),
@@ -389,11 +504,14 @@ def run_ours(args):
         "regular_pairs": nreg, "per_operator": per_op,
     }
 
-    ns = None
+    ns = adj = swp = None
     if rank == 0 and args.workload == "p1" and not args.skip_north_star:
         del wl.outs
         torch.cuda.empty_cache()
         ns = north_star(args)
+        adj = adjoint_timing(args)
+        torch.cuda.empty_cache()
+        swp = None if args.skip_sweep else sweep_timing(args)
 
     if rank == 0:
         line = {
@@ -412,6 +530,10 @@ def run_ours(args):
         }
         if ns is not None:
             line["north_star"] = ns
+        if adj is not None:
+            line["adjoint"] = adj
+        if swp is not None:
+            line["sweep"] = swp
         if not args.skip_cpu:
             line["cpu_baseline"] = cpu_baseline(w, wl.points, wl.cells, wl.n, args)
         print(json.dumps(line), flush=True)
@@ -498,6 +620,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-north-star", action="store_true")
+    ap.add_argument("--skip-sweep", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -254,6 +254,38 @@ ElementFamilyT *create_nedelec_family_bempp(size_t degree, Continuity continuity
 /* src/bindings/ndelement.rs:9-19 (null-safe) */
 void element_family_t_free_bempp(ElementFamilyT *ptr);
 
+/* Addition: adjoint gradient of J = Re(lambda^H A mu) for the Helmholtz single-layer
+ * operator A(x, k) on DP0 x DP0 spaces of `grid` (test = trial), with respect to every
+ * point coordinate and to k, without forming dA (FP64; options give the regular rule and
+ * the singular order).  lambda, mu: complex128 arrays of ncells; outputs J, dJ/dk and
+ * grad_points (npoints x 3).  Host pointers: */
+BemppStatus bempp_helmholtz_single_layer_dp0_gradient(GridT *grid,
+                                                      const BoundaryAssemblerOptionsT *options,
+                                                      double k, const void *lambda,
+                                                      const void *mu, double *value,
+                                                      double *grad_k, double *grad_points);
+/* Addition: the same with device pointers, enqueued on `stream`; value_and_grad_k holds
+ * {J, dJ/dk}. */
+BemppStatus bempp_helmholtz_single_layer_dp0_gradient_device(
+    GridT *grid, const BoundaryAssemblerOptionsT *options, double k, const void *lambda,
+    const void *mu, double *value_and_grad_k, double *grad_points, void *stream);
+
+/* Addition: batched Helmholtz single-layer DP0 frequency sweep.  For every grid i and
+ * every wavenumber k_j, writes the ncells_i x ncells_i complex64 matrix (column-major) at
+ * outputs[i] + j * ncells_i^2 (device memory, nk matrices per grid): regular far pairs in
+ * FP32, near and singular pairs in FP64, all in one persistent launch replayed from a
+ * captured CUDA graph.  `wavenumbers` is a host array; the options must select the
+ * 6-point regular rule.  The launch parameters (wavenumbers per work item, CTAs per SM)
+ * are chosen by a timing autotuner on the first call for a set of mesh sizes; calls with
+ * the same grids, wavenumbers and outputs replay the same graph.  Enqueued on `stream`. */
+BemppStatus bempp_helmholtz_single_layer_dp0_sweep_device(GridT *const *grids, size_t ngrids,
+                                                          const double *wavenumbers, size_t nk,
+                                                          const BoundaryAssemblerOptionsT *options,
+                                                          void *const *outputs, void *stream);
+/* Addition: parameters the autotuner chose for the last sweep (probe_ms: its measured
+ * milliseconds per wavenumber-item on the probe slice). */
+BemppStatus bempp_sweep_last_tuning(int32_t *kchunk, int32_t *blocks_per_sm, double *probe_ms);
+
 /* Addition, with no counterpart in the reference: dense regular-quadrature assembly of a
  * DP0 x DP0 Laplace (kernel 0) or Helmholtz (kernel 1) single-layer, double-layer or
  * adjoint double-layer operator between two distinct meshes, for callers that cannot
