@@ -234,6 +234,15 @@ class BoundaryAssembler(object):
             self._rs_assembler, _ffi.cast("double*", buf.ctypes.data), 8)
         return [float(x) for x in buf[:n]]
 
+    def host_copy_stats(self) -> typing.Dict[str, float]:
+        """Host side of the last host-memory assembly: DMA wait and host copy times (ms),
+        copy groups, assembly chunks and copy threads."""
+        buf = np.zeros(5, dtype=np.float64)
+        n = _lib.boundary_assembler_host_copy_stats(
+            self._rs_assembler, _ffi.cast("double*", buf.ctypes.data), 5)
+        keys = ("dma_wait_ms", "host_copy_ms", "groups", "chunks", "threads")
+        return {k: float(v) for k, v in zip(keys[:n], buf[:n])}
+
     def launch_count(self) -> int:
         """Kernel launches enqueued by the last assembly."""
         return _lib.boundary_assembler_last_launch_count(self._rs_assembler)

@@ -38,8 +38,11 @@ def _grid(points: np.ndarray, cells: np.ndarray):
 
 
 def energy_and_gradient(points, cells, k, lam, mu, regular_points=6, singular_order=4,
-                        device=None):
-    """J, dJ/dk and dJ/dpoints (npoints x 3) as torch float64 tensors on `device`."""
+                        device=None, mixed=False):
+    """J, dJ/dk and dJ/dpoints (npoints x 3) as torch float64 tensors on `device`; with
+    mixed=True far pairs are integrated in FP32 (near and singular pairs stay FP64)."""
+    from bempp.assembly.boundary import Precision
+
     device = torch.device("cuda") if device is None else torch.device(device)
     pts = points.detach().cpu().numpy() if torch.is_tensor(points) else np.asarray(points)
     cls = cells.cpu().numpy() if torch.is_tensor(cells) else np.asarray(cells)
@@ -47,6 +50,7 @@ def energy_and_gradient(points, cells, k, lam, mu, regular_points=6, singular_or
     opts.set_regular_quadrature_degree(ReferenceCellType.Triangle, regular_points)
     opts.set_singular_quadrature_degree(ReferenceCellType.Triangle, ReferenceCellType.Triangle,
                                         singular_order)
+    opts.set_precision(Precision.Mixed if mixed else Precision.FP64)
     g = _grid(pts, cls)
     try:
         lam_d = torch.as_tensor(lam, dtype=torch.complex128, device=device).contiguous()

@@ -224,10 +224,7 @@ BemppStatus boundary_assembler_assemble_into_memory_ex(BoundaryAssemblerT* a, Sp
     if (n == 0) return;
     require(data, "output");
     std::lock_guard<std::mutex> lock(a->mu);
-    const size_t bytes = n * dtype_size(a->dtype);
-    a->work.alloc(bytes);
-    assemble_device(*a, *trial, *test, a->work.ptr, nullptr);
-    BEMPP_CUDA(cudaMemcpy(data, a->work.ptr, bytes, cudaMemcpyDeviceToHost));
+    assemble_host(*a, *trial, *test, data);
   });
 }
 
@@ -274,6 +271,14 @@ MatrixT* boundary_assembler_assemble_singular(BoundaryAssemblerT* a, SpaceT* tri
 
 void boundary_assembler_set_timing(BoundaryAssemblerT* a, bool enabled) {
   if (a) a->timing = enabled;
+}
+
+size_t boundary_assembler_host_copy_stats(BoundaryAssemblerT* a, double* out, size_t n) {
+  if (!a || !out) return 0;
+  std::lock_guard<std::mutex> lock(a->mu);
+  const size_t m = std::min(n, a->host_copy_stats.size());
+  for (size_t i = 0; i < m; ++i) out[i] = a->host_copy_stats[i];
+  return m;
 }
 
 size_t boundary_assembler_phase_times(BoundaryAssemblerT* a, double* ms, size_t n) {

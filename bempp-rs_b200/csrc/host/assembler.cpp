@@ -112,6 +112,11 @@ const GridGeometry& grid_geometry(GridT& g, int device, const RegularRule& rule,
                                geo->qpts.as<double>(), geo->qrel.as<float>(),
                                geo->vids.as<int>(), stream));
     ++launches;
+    // the cache is shared by every stream that assembles on this grid: finish it now
+    // (unless the stream is being captured, where later nodes of the graph order after it)
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    BEMPP_CUDA(cudaStreamIsCapturing(stream, &cap));
+    if (cap == cudaStreamCaptureStatusNone) BEMPP_CUDA(cudaStreamSynchronize(stream));
     slot = std::move(geo);
   }
   return *slot;
@@ -183,24 +188,59 @@ struct Timer {
   BoundaryAssemblerT& a;
   cudaStream_t stream;
   int next = 0;
-  Timer(BoundaryAssemblerT& asmb, cudaStream_t s) : a(asmb), stream(s) {
-    if (!a.timing) return;
+  bool on;
+  Timer(BoundaryAssemblerT& asmb, cudaStream_t s, bool enable = true)
+      : a(asmb), stream(s), on(asmb.timing && enable) {
+    if (!on) return;
     for (auto& e : a.events)
       if (!e) BEMPP_CUDA(cudaEventCreate(&e));
     mark();
   }
   void mark() {
-    if (a.timing && next < 5) BEMPP_CUDA(cudaEventRecord(a.events[next++], stream));
+    if (on && next < 5) BEMPP_CUDA(cudaEventRecord(a.events[next++], stream));
   }
   // Durations are read lazily (boundary_assembler_phase_times) so that timing adds no
   // host synchronisation to the assembly itself.
-  void finish() { a.events_recorded = a.timing ? next : 0; }
+  void finish() { a.events_recorded = on ? next : 0; }
 };
 
 }  // namespace
 
+int effective_chunks(const SpaceT& trial, int want) {
+  const int tiles = static_cast<int>((trial.grid->ncells + 31) / 32);
+  return std::max(1, std::min(want, tiles));
+}
+
+const ColumnRuns& chunk_columns(SpaceT& trial, int nchunks) {
+  std::lock_guard<std::mutex> lock(trial.mu);
+  auto& slot = trial.chunk_runs[nchunks];
+  if (slot.empty()) {
+    const int64_t nc = trial.grid->ncells;
+    const int tiles = static_cast<int>((nc + 31) / 32);
+    // chunk c holds trial tiles [c * tiles / nchunks, (c + 1) * tiles / nchunks)
+    std::vector<int> last(static_cast<size_t>(trial.ndofs), -1);
+    for (int64_t c = 0; c < nc; ++c) {
+      const int tile = static_cast<int>(c / 32);
+      const int chunk = static_cast<int>((static_cast<int64_t>(tile + 1) * nchunks - 1) / tiles);
+      for (int b = 0; b < trial.nbasis; ++b) {
+        int& l = last[trial.cell_dofs[c * trial.nbasis + b]];
+        l = std::max(l, chunk);
+      }
+    }
+    slot.assign(nchunks, {});
+    for (int64_t d = 0; d < trial.ndofs;) {
+      const int c = std::max(last[d], 0);  // a DOF on no cell: an all-zero column
+      int64_t e = d + 1;
+      while (e < trial.ndofs && std::max(last[e], 0) == c) ++e;
+      slot[c].push_back({d, e - d});
+      d = e;
+    }
+  }
+  return slot;
+}
+
 void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d_out,
-                     cudaStream_t stream) {
+                     cudaStream_t stream, int nchunks, const std::function<void(int)>& chunk_done) {
   check_spaces(a, trial, test);
   const int device = current_device();
   const auto qit = a.options.regular.find(kTriangle);
@@ -213,20 +253,24 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
   const int order = static_cast<int>(sit->second);
   const bool same_grid = trial.grid == test.grid;
   const int64_t nt = test.ndofs, ns = trial.ndofs;
+  const bool single = a.dtype == 0 || a.dtype == 2;
+  const bool cplx = a.kernel == kHelmholtz;
+  const bool dp0 = test.nbasis == 1 && trial.nbasis == 1 && a.op != kHS;
+  nchunks = effective_chunks(trial, nchunks);
+  if (single && !dp0) nchunks = 1;
   a.launches = 0;
 
   ensure_space_device(test, device);
   ensure_space_device(trial, device);
-  Timer timer(a, stream);
+  Timer timer(a, stream, nchunks == 1);
   const GridGeometry& tgeo = grid_geometry(*test.grid, device, rule, stream, a.launches);
   const GridGeometry& sgeo = grid_geometry(*trial.grid, device, rule, stream, a.launches);
   timer.mark();
 
-  const bool single = a.dtype == 0 || a.dtype == 2;
-  const bool cplx = a.kernel == kHelmholtz;
   void* out = d_out;
+  const size_t esize = cplx ? 16 : 8;
   if (single) {
-    a.convert.alloc(static_cast<size_t>(nt) * ns * (cplx ? 16 : 8));
+    a.convert.alloc(static_cast<size_t>(nt) * ns * esize);
     out = a.convert.ptr;
   }
   RegularArgs ra;
@@ -239,29 +283,19 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
   ra.ld = nt;
   ra.out = out;
   const CellSet tcs = cell_set(*test.grid, tgeo), scs = cell_set(*trial.grid, sgeo);
-  const bool dp0 = test.nbasis == 1 && trial.nbasis == 1 && a.op != kHS;
-  if (nt > 0 && ns > 0) {
-    if (dp0) {
-      timer.mark();  // no memset phase: the DP0 kernel writes every entry
-      BEMPP_CUDA(launch_regular_dp0(tcs, scs, rule, ra, stream));
-      ++a.launches;
-    } else {
-      BEMPP_CUDA(cudaMemsetAsync(out, 0, static_cast<size_t>(nt) * ns * (cplx ? 16 : 8), stream));
-      timer.mark();
-      BEMPP_CUDA(launch_regular_scatter(tcs, space_tiles(test), scs, space_tiles(trial), rule,
-                                        ra, stream));
-      ++a.launches;
-    }
-  }
-  timer.mark();
-  if (same_grid && nt > 0 && ns > 0) {
+
+  const bool empty = nt == 0 || ns == 0;
+  const bool singular = same_grid && !empty;
+  SingularArgs sa;
+  SingularRules rules{};
+  SingularPairs pairs{};
+  if (singular) {
     SingularPairList& pl = grid_pairs(*test.grid, device);
     const DeviceRules& dr = device_rules(device, order);
-    SingularRules rules{dr.offset.as<int>(), dr.test_xi.as<double>(), dr.trial_xi.as<double>(),
-                        dr.w.as<double>()};
-    SingularPairs pairs{static_cast<int>(pl.test_cell.size()), pl.d_test.as<int>(),
-                        pl.d_trial.as<int>(), pl.d_config.as<int>()};
-    SingularArgs sa;
+    rules = SingularRules{dr.offset.as<int>(), dr.test_xi.as<double>(), dr.trial_xi.as<double>(),
+                          dr.w.as<double>()};
+    pairs = SingularPairs{static_cast<int>(pl.test_cell.size()), pl.d_test.as<int>(),
+                          pl.d_trial.as<int>(), pl.d_config.as<int>()};
     sa.kernel = a.kernel;
     sa.op = a.op;
     sa.k = a.k;
@@ -270,14 +304,76 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
     sa.out = out;
     sa.unique_entries = dp0 ? 1 : 0;
     sa.pair_values = nullptr;
+  }
+  auto run_singular = [&](int lo, int hi) {
+    sa.trial_lo = lo;
+    sa.trial_hi = hi;
     BEMPP_CUDA(launch_singular(tcs, test.d_dofs.as<int>(), test.nbasis, scs,
                                trial.d_dofs.as<int>(), trial.nbasis, rules, pairs, sa, stream));
     ++a.launches;
-  }
-  if (single) {
-    BEMPP_CUDA(launch_convert_to_single(static_cast<const double*>(out), d_out,
-                                        static_cast<size_t>(nt) * ns * (cplx ? 2 : 1), stream));
-    ++a.launches;
+  };
+  const int tiles = static_cast<int>((trial.grid->ncells + 31) / 32);
+  auto tile_range = [&](int c, int& t0, int& t1) {
+    t0 = static_cast<int>(static_cast<int64_t>(c) * tiles / nchunks);
+    t1 = static_cast<int>(static_cast<int64_t>(c + 1) * tiles / nchunks);
+  };
+
+  if (dp0) {
+    // the direct kernel writes every entry (zero for vertex-sharing pairs), so each chunk
+    // is its regular launch followed by the singular pairs of its trial cells
+    timer.mark();  // no memset phase
+    for (int c = 0; c < nchunks; ++c) {
+      int t0, t1;
+      tile_range(c, t0, t1);
+      if (!empty) {
+        ra.trial_tile0 = t0;
+        ra.trial_tiles = t1 - t0;
+        BEMPP_CUDA(launch_regular_dp0(tcs, scs, rule, ra, stream));
+        ++a.launches;
+        if (nchunks == 1) timer.mark();
+        if (singular) run_singular(nchunks == 1 ? 0 : 32 * t0, nchunks == 1 ? 0x7fffffff : 32 * t1);
+        if (single) {
+          const std::vector<std::pair<int64_t, int64_t>> all{{0, ns}};
+          for (const auto& run : nchunks == 1 ? all : chunk_columns(trial, nchunks)[c]) {
+            const size_t off = static_cast<size_t>(run.first) * nt * (cplx ? 2 : 1);
+            BEMPP_CUDA(launch_convert_to_single(static_cast<const double*>(out) + off,
+                                                static_cast<char*>(d_out) + off * 4,
+                                                static_cast<size_t>(run.second) * nt * (cplx ? 2 : 1),
+                                                stream));
+            ++a.launches;
+          }
+        }
+      } else if (nchunks == 1) {
+        timer.mark();
+      }
+      if (chunk_done) chunk_done(c);
+    }
+  } else {
+    if (!empty) BEMPP_CUDA(cudaMemsetAsync(out, 0, static_cast<size_t>(nt) * ns * esize, stream));
+    timer.mark();
+    // chunked: the singular pairs first (all adds commute), then the regular chunks
+    if (singular && nchunks > 1) run_singular(0, 0x7fffffff);
+    for (int c = 0; c < nchunks; ++c) {
+      int t0, t1;
+      tile_range(c, t0, t1);
+      if (!empty) {
+        ra.trial_tile0 = t0;
+        ra.trial_tiles = t1 - t0;
+        BEMPP_CUDA(launch_regular_scatter(tcs, space_tiles(test), scs, space_tiles(trial), rule,
+                                          ra, stream));
+        ++a.launches;
+      }
+      if (nchunks == 1) {
+        timer.mark();
+        if (singular) run_singular(0, 0x7fffffff);
+        if (single && !empty) {
+          BEMPP_CUDA(launch_convert_to_single(static_cast<const double*>(out), d_out,
+                                              static_cast<size_t>(nt) * ns * (cplx ? 2 : 1), stream));
+          ++a.launches;
+        }
+      }
+      if (chunk_done) chunk_done(c);
+    }
   }
   timer.mark();
   timer.finish();
@@ -302,8 +398,6 @@ void helmholtz_sl_gradient_device(GridT& g, const Options& opts, double k, const
   const auto sit = opts.singular.find({kTriangle, kTriangle});
   if (qit == opts.regular.end() || sit == opts.singular.end())
     throw Error(kInvalidArgument, "options lack triangle quadrature degrees");
-  if (opts.precision != 0)
-    throw Error(kUnsupported, "the adjoint gradient is computed in FP64 only");
   const RegularRule rule = simplex_rule(static_cast<int>(qit->second));
   size_t launches = 0;
   const GridGeometry& geo = grid_geometry(g, device, rule, stream, launches);
@@ -319,7 +413,8 @@ void helmholtz_sl_gradient_device(GridT& g, const Options& opts, double k, const
   }
   BEMPP_CUDA(launch_adjoint_sl(cell_set(g, geo), rule, rules, pairs, k, d_lam, d_mu,
                                g.adjoint_scratch.as<double>(), d_grad_points,
-                               static_cast<int>(g.npoints), d_totals, stream));
+                               static_cast<int>(g.npoints), d_totals, opts.precision == 1,
+                               stream));
 }
 
 MatrixT* assemble_singular_csr(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test) {
@@ -434,4 +529,5 @@ MatrixT* assemble_singular_csr(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& tes
 BoundaryAssemblerT::~BoundaryAssemblerT() {
   for (auto& e : events)
     if (e) cudaEventDestroy(e);
+  if (stream) cudaStreamDestroy(stream);
 }

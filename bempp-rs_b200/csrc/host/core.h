@@ -5,6 +5,7 @@
 
 #include <array>
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -109,6 +110,9 @@ struct GridGeometry {  // device geometry for one regular rule
   DeviceBuffer geom, qpts, qrel, vids;
 };
 
+// Per chunk of a chunked assembly: runs (first column, number of columns).
+using ColumnRuns = std::vector<std::vector<std::pair<int64_t, int64_t>>>;
+
 struct SingularPairList {
   std::vector<int> test_cell, trial_cell, config;
   DeviceBuffer d_test, d_trial, d_config;
@@ -158,6 +162,7 @@ struct SpaceT {
   DeviceBuffer d_dofs;                                   // int32 ncells x nbasis
   DeviceBuffer d_tile_off, d_tile_dofs, d_cell_ldof;     // tile-scatter layout
   int ntiles = 0, max_tile_dofs = 0, tile_cells = 0;
+  std::map<int, bempp_b200::ColumnRuns> chunk_runs;  // by number of chunks
   std::mutex mu;
 };
 
@@ -183,6 +188,10 @@ struct BoundaryAssemblerT {
   cudaEvent_t events[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   int events_recorded = 0;
   DeviceBuffer work;     // device output for host-memory assembly
+  cudaStream_t stream = nullptr;  // host-memory assembly stream (created on first use)
+  // last host-memory assembly: ms waiting for DMA, ms of host copy, copy groups, chunks,
+  // host copy threads
+  std::array<double, 5> host_copy_stats{};
   DeviceBuffer convert;  // FP64 staging for F32 / C32 outputs
   DeviceBuffer pair_values;
   std::mutex mu;
@@ -199,8 +208,22 @@ std::vector<std::vector<int64_t>> cell_colouring(const SpaceT& s);
 size_t dtype_size(uint8_t dtype);
 
 // Dense assembly into device memory (column-major, assembler dtype) on `stream`.
+//
+// With nchunks > 1 the regular part is launched over nchunks consecutive ranges of trial
+// tiles and chunk_done(c) is called (host side, after chunk c's launches are enqueued);
+// the trial DOFs whose columns are final after chunk c are chunk_columns(trial, nchunks)[c].
+// F32 / C32 outputs of non-DP0 spaces are assembled in one chunk.
 void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d_out,
-                     cudaStream_t stream);
+                     cudaStream_t stream, int nchunks = 1,
+                     const std::function<void(int)>& chunk_done = {});
+// Maximal runs [first, first + count) of trial DOFs completed by each chunk of a chunked
+// assembly: a column is complete after the last chunk holding one of its cells.
+const ColumnRuns& chunk_columns(SpaceT& trial, int nchunks);
+// Number of chunks assemble_device uses for a request of `want` (at most one per tile).
+int effective_chunks(const SpaceT& trial, int want);
+// Dense assembly into host memory: chunked device assembly with the device-to-host copy
+// of finished columns (pinned staging ring, parallel host copy) overlapped (host_copy.cpp).
+void assemble_host(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* data);
 // Adjoint gradient of Re(lambda^H A mu), Helmholtz single layer, DP0 x DP0 on one grid;
 // device inputs (complex128 lambda, mu per cell) and outputs ({J, dJ/dk}, npoints x 3).
 void helmholtz_sl_gradient_device(GridT& g, const Options& opts, double k, const double* d_lam,

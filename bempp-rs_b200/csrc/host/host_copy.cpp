@@ -1,0 +1,258 @@
+// Dense assembly into host memory with the device-to-host transfer overlapped.
+//
+// bempp-rs BoundaryAssembler::assemble_into_memory (src/boundary_assemblers.rs:176-214)
+// fills a caller-owned column-major host array.  Copying a finished device matrix into
+// pageable host memory with one cudaMemcpy runs at the driver's pageable rate and starts
+// only after the last kernel.  Here the regular part is assembled in chunks of trial
+// tiles (assemble_device); as soon as a chunk's kernels finish, the columns it completed
+// are copied by DMA into a pinned staging slot on a copy stream, and host threads move
+// the previous slot into the caller's array.  Compute, DMA and host copy overlap; only
+// the last group's copy is exposed.
+//
+// Staging: a process-wide ring of two pinned slots per device (kSlotBytes each) and one
+// copy stream, used by one assembly at a time (mutex).  Host copies run on a small
+// persistent pool of worker threads, each taking an equal byte share of a group.
+#include <sys/mman.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <thread>
+
+#include "core.h"
+
+namespace bempp_b200 {
+
+namespace {
+
+constexpr size_t kSlotBytes = size_t(64) << 20;
+constexpr size_t kChunkTargetBytes = size_t(96) << 20;  // device bytes per chunk (about)
+constexpr int kMaxChunks = 16;
+
+// Persistent pool running one parallel job at a time.
+class CopyPool {
+ public:
+  static CopyPool& get() {
+    static CopyPool pool;
+    return pool;
+  }
+  int size() const { return static_cast<int>(workers_.size()) + 1; }
+  // Runs fn(i) for i in [0, size()) on the workers and the calling thread.
+  void run(const std::function<void(int)>& fn) {
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      job_ = &fn;
+      pending_ = static_cast<int>(workers_.size());
+      ++generation_;
+    }
+    cv_.notify_all();
+    fn(0);
+    std::unique_lock<std::mutex> lock(mu_);
+    done_cv_.wait(lock, [&] { return pending_ == 0; });
+    job_ = nullptr;
+  }
+
+ private:
+  CopyPool() {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int n = static_cast<int>(std::min(16u, std::max(1u, hw / 2)));
+    for (int i = 1; i < n; ++i) workers_.emplace_back([this, i] { loop(i); });
+  }
+  ~CopyPool() {
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : workers_) t.join();
+  }
+  void loop(int id) {
+    uint64_t seen = 0;
+    for (;;) {
+      const std::function<void(int)>* job;
+      {
+        std::unique_lock<std::mutex> lock(mu_);
+        cv_.wait(lock, [&] { return stop_ || generation_ != seen; });
+        if (stop_) return;
+        seen = generation_;
+        job = job_;
+      }
+      (*job)(id);
+      {
+        std::lock_guard<std::mutex> lock(mu_);
+        if (--pending_ == 0) done_cv_.notify_one();
+      }
+    }
+  }
+  std::vector<std::thread> workers_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_cv_;
+  const std::function<void(int)>* job_ = nullptr;
+  int pending_ = 0;
+  uint64_t generation_ = 0;
+  bool stop_ = false;
+};
+
+struct Staging {
+  void* slot[2] = {nullptr, nullptr};
+  cudaStream_t copy = nullptr;
+  cudaEvent_t copied[2] = {nullptr, nullptr};
+  std::vector<cudaEvent_t> chunk_ready;
+  std::mutex mu;
+};
+
+std::mutex g_staging_mu;
+std::map<int, std::unique_ptr<Staging>> g_staging;
+
+Staging& staging(int device) {
+  std::lock_guard<std::mutex> lock(g_staging_mu);
+  auto& s = g_staging[device];
+  if (!s) {
+    auto st = std::make_unique<Staging>();
+    for (int i = 0; i < 2; ++i) {
+      BEMPP_CUDA(cudaHostAlloc(&st->slot[i], kSlotBytes, cudaHostAllocDefault));
+      BEMPP_CUDA(cudaEventCreateWithFlags(&st->copied[i], cudaEventDisableTiming));
+    }
+    BEMPP_CUDA(cudaStreamCreateWithFlags(&st->copy, cudaStreamNonBlocking));
+    s = std::move(st);
+  }
+  return *s;
+}
+
+// One DMA into a staging slot: bytes [src_off, src_off + bytes) of the device matrix,
+// which land at the same offsets of the host matrix.
+struct Piece {
+  size_t src_off, bytes, slot_off;
+};
+struct Group {
+  int chunk = 0;
+  std::vector<Piece> pieces;
+  size_t bytes = 0;
+};
+
+std::vector<Group> plan_groups(const ColumnRuns& runs, size_t col_bytes) {
+  std::vector<Group> groups;
+  for (int c = 0; c < static_cast<int>(runs.size()); ++c) {
+    Group g;
+    g.chunk = c;
+    for (const auto& run : runs[c]) {
+      size_t off = static_cast<size_t>(run.first) * col_bytes;
+      size_t left = static_cast<size_t>(run.second) * col_bytes;
+      while (left > 0) {
+        if (g.bytes == kSlotBytes) {
+          groups.push_back(std::move(g));
+          g = Group();
+          g.chunk = c;
+        }
+        const size_t n = std::min(left, kSlotBytes - g.bytes);
+        g.pieces.push_back({off, n, g.bytes});
+        g.bytes += n;
+        off += n;
+        left -= n;
+      }
+    }
+    if (g.bytes > 0) groups.push_back(std::move(g));
+  }
+  return groups;
+}
+
+// Parallel copy of one staged group into the host matrix.
+void host_copy(const Group& g, const void* slot, void* dst) {
+  CopyPool& pool = CopyPool::get();
+  const int nt = pool.size();
+  const size_t share = (g.bytes + nt - 1) / nt;
+  pool.run([&](int t) {
+    const size_t lo = std::min(g.bytes, share * t), hi = std::min(g.bytes, lo + share);
+    for (const Piece& p : g.pieces) {
+      const size_t a = std::max(lo, p.slot_off), b = std::min(hi, p.slot_off + p.bytes);
+      if (a >= b) continue;
+      std::memcpy(static_cast<char*>(dst) + p.src_off + (a - p.slot_off),
+                  static_cast<const char*>(slot) + a, b - a);
+    }
+  });
+}
+
+}  // namespace
+
+void assemble_host(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* data) {
+  const size_t nt = static_cast<size_t>(test.ndofs), ns = static_cast<size_t>(trial.ndofs);
+  const size_t col_bytes = nt * dtype_size(a.dtype);
+  const size_t bytes = col_bytes * ns;
+  int device = 0;
+  BEMPP_CUDA(cudaGetDevice(&device));
+  a.work.alloc(bytes);
+  if (!a.stream) BEMPP_CUDA(cudaStreamCreateWithFlags(&a.stream, cudaStreamNonBlocking));
+
+  // compute chunking: ~kChunkTargetBytes of output per chunk
+  const bool single = a.dtype == 0 || a.dtype == 2;
+  const bool dp0 = test.nbasis == 1 && trial.nbasis == 1 && a.op != kHS;
+  int want = static_cast<int>(std::min<size_t>(kMaxChunks, (bytes + kChunkTargetBytes - 1) /
+                                                               kChunkTargetBytes));
+  if (single && !dp0) want = 1;
+  const int nchunks = effective_chunks(trial, want);
+  const ColumnRuns& runs = chunk_columns(trial, nchunks);
+  const std::vector<Group> groups = plan_groups(runs, col_bytes);
+
+  // Large destinations are usually fresh, untouched allocations (numpy zeros): ask for
+  // transparent huge pages so that the first-touch faults of the host copy are 512x
+  // fewer.  A hint only; it changes no contents.
+  if (bytes >= (size_t(64) << 20)) {
+    const uintptr_t page = static_cast<uintptr_t>(sysconf(_SC_PAGESIZE));
+    const uintptr_t lo = (reinterpret_cast<uintptr_t>(data) + page - 1) & ~(page - 1);
+    const uintptr_t hi = (reinterpret_cast<uintptr_t>(data) + bytes) & ~(page - 1);
+    if (hi > lo) madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_HUGEPAGE);
+  }
+
+  Staging& st = staging(device);
+  std::lock_guard<std::mutex> lock(st.mu);
+  while (st.chunk_ready.size() < static_cast<size_t>(nchunks)) {
+    cudaEvent_t e;
+    BEMPP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    st.chunk_ready.push_back(e);
+  }
+  // Whatever happens below, no DMA into the staging ring outlives this call.
+  struct Drain {
+    Staging& st;
+    cudaStream_t s;
+    ~Drain() {
+      cudaStreamSynchronize(s);
+      cudaStreamSynchronize(st.copy);
+    }
+  } drain{st, a.stream};
+
+  assemble_device(a, trial, test, a.work.ptr, a.stream, nchunks, [&](int c) {
+    BEMPP_CUDA(cudaEventRecord(st.chunk_ready[c], a.stream));
+  });
+
+  const char* src = static_cast<const char*>(a.work.ptr);
+  auto enqueue = [&](size_t gi) {
+    const Group& g = groups[gi];
+    const int s = static_cast<int>(gi & 1);
+    BEMPP_CUDA(cudaStreamWaitEvent(st.copy, st.chunk_ready[g.chunk], 0));
+    for (const Piece& p : g.pieces)
+      BEMPP_CUDA(cudaMemcpyAsync(static_cast<char*>(st.slot[s]) + p.slot_off, src + p.src_off,
+                                 p.bytes, cudaMemcpyDeviceToHost, st.copy));
+    BEMPP_CUDA(cudaEventRecord(st.copied[s], st.copy));
+  };
+  for (size_t gi = 0; gi < std::min<size_t>(2, groups.size()); ++gi) enqueue(gi);
+  using clock = std::chrono::steady_clock;
+  double wait_ms = 0.0, copy_ms = 0.0;
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    const int s = static_cast<int>(gi & 1);
+    const auto t0 = clock::now();
+    BEMPP_CUDA(cudaEventSynchronize(st.copied[s]));
+    const auto t1 = clock::now();
+    host_copy(groups[gi], st.slot[s], data);
+    copy_ms += std::chrono::duration<double, std::milli>(clock::now() - t1).count();
+    wait_ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
+    if (gi + 2 < groups.size()) enqueue(gi + 2);
+  }
+  a.host_copy_stats = {wait_ms, copy_ms, static_cast<double>(groups.size()),
+                       static_cast<double>(nchunks), static_cast<double>(CopyPool::get().size())};
+  BEMPP_CUDA(cudaStreamSynchronize(a.stream));
+  BEMPP_CUDA(cudaGetLastError());
+}
+
+}  // namespace bempp_b200

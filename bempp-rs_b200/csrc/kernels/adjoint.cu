@@ -18,7 +18,9 @@
 // last kernel scatters the per-cell-vertex gradients to the vertices.
 //
 // Regular pairs use the tiled mapping of regular.cu (32 x 32 cell tiles, lane = test
-// cell); adjacent pairs use one warp per pair over their Duffy rule.  FP64 throughout.
+// cell); adjacent pairs use one warp per pair over their Duffy rule.  FP64, or mixed:
+// far pairs (centroid distance >= 2 diameters) in FP32 with centroid-relative points and
+// the reference phase e^{ik r0} folded into the pair weight, as in regular.cu.
 #include "launch.h"
 #include "tiles.cuh"
 
@@ -41,7 +43,7 @@ __device__ __forceinline__ void jdet_gradient(const double t0[3], const double t
   }
 }
 
-template <int QT>
+template <int QT, bool MIXED>
 __global__ void __launch_bounds__(kThreads, 3)
     adjoint_sl_regular(CellSet cs, RegularRule rule, double k, const double2* __restrict__ lam,
                        const double2* __restrict__ mu, double* __restrict__ grad_cell,
@@ -51,14 +53,14 @@ __global__ void __launch_bounds__(kThreads, 3)
   const int nti = min(kTile, cs.ncells - ti0), nsj = min(kTile, cs.ncells - sj0);
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned char* cursor = smem;
-  const Tile T = carve_tile(cursor, Q, false, 1);
-  const Tile S = carve_tile(cursor, Q, false, 1);
+  const Tile T = carve_tile(cursor, Q, MIXED, 1);
+  const Tile S = carve_tile(cursor, Q, MIXED, 1);
   double* s_test = reinterpret_cast<double*>(cursor);  // [kTile][9] test-cell gradients
   double* s_trial = s_test + kTile * 9;                // [kTile][9] trial-cell gradients
   double* s_tot = s_trial + kTile * 9;                 // J, dJ/dk
   for (int e = threadIdx.x; e < 2 * kTile * 9 + 2; e += kThreads) s_test[e] = 0.0;
-  load_tile(T, cs, ti0, nti, Q, false, nullptr, 1);
-  load_tile(S, cs, sj0, nsj, Q, false, nullptr, 1);
+  load_tile(T, cs, ti0, nti, Q, MIXED, nullptr, 1);
+  load_tile(S, cs, sj0, nsj, Q, MIXED, nullptr, 1);
   __syncthreads();
 
   const int it = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -81,7 +83,94 @@ __global__ void __launch_bounds__(kThreads, 3)
 #pragma unroll
     for (int q = 0; q < Q; ++q) uq[q][0] = uq[q][1] = uq[q][2] = 0.0;
     double vt[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    if (active) {
+    bool far = false;
+    if (MIXED && active) {
+      const double dcx = T.G(fCx, it) - S.G(fCx, js), dcy = T.G(fCy, it) - S.G(fCy, js),
+                   dcz = T.G(fCz, it) - S.G(fCz, js);
+      const double dist2 = dcx * dcx + dcy * dcy + dcz * dcz;
+      const double lim = 2.0 * fmax(T.G(fDiam, it), S.G(fDiam, js));
+      far = dist2 >= lim * lim;
+      if (far) {
+        // FP32 far pair: centroid-relative points, reference phase folded into the weight
+        // c' = c e^{ik r0}, e^{ik r} = e^{ik r0} e^{ik (r - r0)}, r - r0 = s / (r + r0).
+        const float fdx = static_cast<float>(dcx), fdy = static_cast<float>(dcy),
+                    fdz = static_cast<float>(dcz);
+        const double r0 = sqrt(dist2);
+        const float r0f = static_cast<float>(r0), r0sq = r0f * r0f, kf = static_cast<float>(k);
+        float pc, ps;
+        phase_cos_sin(k * r0, pc, ps);
+        const float cr = static_cast<float>(c_re * pc - c_im * ps);
+        const float ci = static_cast<float>(c_re * ps + c_im * pc);
+        const bool taylor = k * (T.G(fRad, it) + S.G(fRad, js)) <= 0.8;
+        float fS0r = 0.f, fS0i = 0.f, fSkr = 0.f, fSki = 0.f;
+        float fuq[QT > 0 ? QT : kMaxRegularPoints][3];
+        float fvt[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+        for (int q = 0; q < Q; ++q) fuq[q][0] = fuq[q][1] = fuq[q][2] = 0.f;
+#pragma unroll 1
+        for (int p = 0; p < Q; ++p) {
+          const float ax = T.R(p, 0, it), ay = T.R(p, 1, it), az = T.R(p, 2, it);
+          const float alpha = 2.f * fmaf(fdx, ax, fmaf(fdy, ay, fdz * az));
+          const float px = fdx + ax, py = fdy + ay, pz = fdz + az;
+          float vp0 = 0.f, vp1 = 0.f, vp2 = 0.f, gr = 0.f, gi = 0.f, er = 0.f, ei = 0.f;
+          const float wp = rule.wf[p];
+#pragma unroll
+          for (int q = 0; q < Q; ++q) {
+            const float yx = S.R(q, 0, js), yy = S.R(q, 1, js), yz = S.R(q, 2, js);
+            const float Dx = ax - yx, Dy = ay - yy, Dz = az - yz;
+            const float beta = 2.f * fmaf(fdx, yx, fmaf(fdy, yy, fdz * yz));
+            const float sq = (alpha - beta) + fmaf(Dx, Dx, fmaf(Dy, Dy, Dz * Dz));
+            const float r2 = r0sq + sq;
+            const float rinv = rsqrt_approx(r2);
+            const float r = r2 * rinv, kr = kf * r;
+            const float t = kf * sq * rcp_approx(r + r0f);
+            float csn, sn;
+            if (taylor)
+              poly_cos_sin(t, csn, sn);
+            else
+              reduced_cos_sin(t, csn, sn);
+            const float wq = rule.wf[q];
+            gr = fmaf(wq * rinv, csn, gr);
+            gi = fmaf(wq * rinv, sn, gi);
+            er = fmaf(wq, csn, er);
+            ei = fmaf(wq, sn, ei);
+            const float f_re = -csn - kr * sn, f_im = kr * csn - sn;
+            const float gs = wq * (cr * f_re - ci * f_im) * (rinv * rinv * rinv);
+            const float dx = px - yx, dy = py - yy, dz = pz - yz;
+            vp0 = fmaf(gs, dx, vp0);
+            vp1 = fmaf(gs, dy, vp1);
+            vp2 = fmaf(gs, dz, vp2);
+            const float wgs = wp * gs;
+            fuq[q][0] = fmaf(wgs, dx, fuq[q][0]);
+            fuq[q][1] = fmaf(wgs, dy, fuq[q][1]);
+            fuq[q][2] = fmaf(wgs, dz, fuq[q][2]);
+          }
+          fS0r = fmaf(wp, gr, fS0r);
+          fS0i = fmaf(wp, gi, fS0i);
+          fSkr = fmaf(wp, er, fSkr);
+          fSki = fmaf(wp, ei, fSki);
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const float f = wp * rule.phif[a][p];
+            fvt[a][0] = fmaf(f, vp0, fvt[a][0]);
+            fvt[a][1] = fmaf(f, vp1, fvt[a][1]);
+            fvt[a][2] = fmaf(f, vp2, fvt[a][2]);
+          }
+        }
+        // back to FP64; S0 and Sk pick up e^{ik r0} through c' in R0 and dk below, so
+        // express them relative to the original c by rotating: S = e^{ik r0} S'.
+        S0_re = static_cast<double>(fS0r) * pc - static_cast<double>(fS0i) * ps;
+        S0_im = static_cast<double>(fS0r) * ps + static_cast<double>(fS0i) * pc;
+        Sk_re = static_cast<double>(fSkr) * pc - static_cast<double>(fSki) * ps;
+        Sk_im = static_cast<double>(fSkr) * ps + static_cast<double>(fSki) * pc;
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+          for (int d = 0; d < 3; ++d) uq[q][d] = fuq[q][d];
+        for (int a = 0; a < 3; ++a)
+          for (int d = 0; d < 3; ++d) vt[a][d] = fvt[a][d];
+      }
+    }
+    if (active && !far) {
 #pragma unroll 1
       for (int p = 0; p < Q; ++p) {
         const double x0 = T.P(p, 0, it), x1 = T.P(p, 1, it), x2 = T.P(p, 2, it);
@@ -307,7 +396,7 @@ __global__ void cell_to_point_gradient(CellSet cs, const double* __restrict__ gr
 cudaError_t launch_adjoint_sl(const CellSet& cs, const RegularRule& rule,
                               const SingularRules& rules, const SingularPairs& pairs, double k,
                               const double* lam, const double* mu, double* grad_cell,
-                              double* grad_points, int npoints, double* totals,
+                              double* grad_points, int npoints, double* totals, bool mixed,
                               cudaStream_t stream) {
   cudaError_t e;
   if ((e = cudaMemsetAsync(grad_cell, 0, sizeof(double) * 9 * cs.ncells, stream)) != cudaSuccess)
@@ -316,20 +405,16 @@ cudaError_t launch_adjoint_sl(const CellSet& cs, const RegularRule& rule,
     return e;
   if ((e = cudaMemsetAsync(totals, 0, sizeof(double) * 2, stream)) != cudaSuccess) return e;
   if (cs.ncells <= 0) return cudaSuccess;
-  const size_t smem = 2 * (sizeof(double) * tile_doubles(rule.npts) + sizeof(int) * tile_ints(1) + 16) +
+  const size_t smem = 2 * (sizeof(double) * tile_doubles(rule.npts) +
+                           sizeof(float) * tile_floats(rule.npts, mixed) + sizeof(int) * tile_ints(1) + 16) +
                       sizeof(double) * (2 * kTile * 9 + 2) + 16;
   dim3 grid((cs.ncells + kTile - 1) / kTile, (cs.ncells + kTile - 1) / kTile);
   const double2* l2 = reinterpret_cast<const double2*>(lam);
   const double2* m2 = reinterpret_cast<const double2*>(mu);
-  if (rule.npts == 6) {
-    auto fn = adjoint_sl_regular<6>;
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    fn<<<grid, kThreads, smem, stream>>>(cs, rule, k, l2, m2, grad_cell, totals);
-  } else {
-    auto fn = adjoint_sl_regular<0>;
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    fn<<<grid, kThreads, smem, stream>>>(cs, rule, k, l2, m2, grad_cell, totals);
-  }
+  auto fn = rule.npts == 6 ? (mixed ? adjoint_sl_regular<6, true> : adjoint_sl_regular<6, false>)
+                           : (mixed ? adjoint_sl_regular<0, true> : adjoint_sl_regular<0, false>);
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  fn<<<grid, kThreads, smem, stream>>>(cs, rule, k, l2, m2, grad_cell, totals);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (pairs.npairs > 0) {
     adjoint_sl_singular<<<(pairs.npairs + 7) / 8, 256, 0, stream>>>(cs, rules, pairs, k, l2, m2,

@@ -31,6 +31,8 @@ struct RegularArgs {
   int out_type;      // OutType
   int64_t ld;        // leading dimension = number of test DOFs
   void* out;         // column-major output
+  int trial_tile0 = 0;   // first trial tile of this launch
+  int trial_tiles = 0;   // trial tiles of this launch (0: all from trial_tile0 on)
 };
 
 // DP0 test x DP0 trial: every entry is written exactly once (no pre-zeroing needed).
@@ -81,6 +83,8 @@ struct SingularArgs {
   void* out;          // dense column-major output (added into), or null
   int unique_entries; // 1 when every pair owns its entries (DP0 x DP0): plain adds
   double* pair_values;  // if non-null: per-pair local blocks (nbt * nbs [*2 complex])
+  int trial_lo = 0;         // only pairs whose trial cell lies in [trial_lo, trial_hi)
+  int trial_hi = 0x7fffffff;
 };
 
 cudaError_t launch_singular(const CellSet& test, const int* test_dofs, int nbt,
@@ -104,7 +108,7 @@ cudaError_t assemble_regular_dp0_noalloc(const RegularArgs& args, const RegularR
 cudaError_t launch_adjoint_sl(const CellSet& cs, const RegularRule& rule,
                               const SingularRules& rules, const SingularPairs& pairs, double k,
                               const double* lam, const double* mu, double* grad_cell,
-                              double* grad_points, int npoints, double* totals,
+                              double* grad_points, int npoints, double* totals, bool mixed,
                               cudaStream_t stream);
 
 // Batched Helmholtz single-layer DP0 sweep (regular.cu): one persistent launch over

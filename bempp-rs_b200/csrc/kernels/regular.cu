@@ -30,39 +30,27 @@
 //     u_p t0 + v_p t1 with (u_p, v_p) = xi_p - (1/3, 1/3), every dot product formed in
 //     FP64 once per pair: (x_p - y_q).n_y = dc.n_y + u_p t0_x.n_y + v_p t1_x.n_y, so no
 //     FP32 cancellation for nearly coplanar pairs;
+//   * s_pq = |d_pq|^2 - |dc|^2 = 2 dc.D + D.D, D = dx_p - dy_q, free of cancellation,
+//     evaluated as A_p + |dy_q|^2 + w_p.dy_q with A_p = |dx_p|^2 + 2 dc.dx_p and
+//     w_p = -2 (dc + dx_p) formed once per test point (4 operations per point pair);
+//     Laplace: r^2 = |dc|^2 + s_pq;
 //   * Helmholtz: e^{ikr} = e^{ik r0} e^{ik delta}, r0 = |dc| in FP64, delta = r - r0 =
-//     (2 dc.D + D.D) / (r + r0), D = dx_p - dy_q, free of cancellation; e^{ik delta} from
-//     the Taylor series of cos / sin (degree 10 / 9, truncation < 3e-8) when
-//     |k delta| <= k (rad_x + rad_y) <= 0.8, else the same series after a Cody-Waite
-//     reduction by pi/2;
-//     e^{ik r0} from the same series after an FP64 reduction of k r0 by pi/2;
+//     s_pq / (r + r0); e^{ik delta} from minimax polynomials of cos / sin on |t| <= 0.8
+//     (degree 8 / 7) when |k delta| <= k (rad_x + rad_y) <= 0.8 holds for every lane of
+//     the warp, else the same polynomials after a Cody-Waite reduction by pi/2;
+//     e^{ik r0} from the same polynomials after an FP64 reduction of k r0 by pi/2;
 //   * DP0 entries sum their 6 inner sums with Kahan compensation; P1 blocks are formed
 //     in FP32 and accumulated into the matrix in FP64.
 #include "launch.h"
+#include <algorithm>
+
 #include "tiles.cuh"
 
 namespace bempp_b200 {
 namespace {
 
-constexpr float kTaylorMax = 0.8f;
+constexpr float kSmallPhaseMax = 0.8f;
 using namespace tiles;
-
-__device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
-  const float y = v - comp;
-  const float t = sum + y;
-  comp = (t - sum) - y;
-  sum = t;
-}
-
-// cos(t), sin(t) for |t| <= pi/4 from their Taylor series (degree 10 and 9; the first
-// omitted terms are below 3e-8 there).
-__device__ __forceinline__ void taylor_cos_sin(float t, float& c, float& s) {
-  const float z = t * t;
-  c = fmaf(z, fmaf(z, fmaf(z, fmaf(z, fmaf(z, -2.7557319e-7f, 2.4801587e-5f), -1.3888889e-3f),
-                           4.1666668e-2f), -0.5f), 1.0f);
-  s = t * fmaf(z, fmaf(z, fmaf(z, fmaf(z, 2.7557319e-6f, -1.9841270e-4f), 8.3333333e-3f),
-                       -0.16666667f), 1.0f);
-}
 
 // Curls of the basis functions of a flat cell: t1 d0(phi) - t0 d1(phi); zero for DP0.
 template <int NB>
@@ -207,59 +195,22 @@ __device__ __forceinline__ void block_fp64(const Tile& T, int it, const Tile& S,
   finish_block<KER, OP, NBT, NBS>(T, it, S, js, k, blk_re, blk_im, S_re, S_im, ore, oim);
 }
 
-__device__ __forceinline__ float rsqrt_approx(float x) {
-  float y;
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-__device__ __forceinline__ float rcp_approx(float x) {
-  float y;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-
-// cos and sin of an argument of any moderate size: Cody-Waite reduction by multiples of
-// pi/2 (two-part constant) to |r| <= pi/4, Taylor series there (truncation < 3e-8), and
-// the quadrant's exchange of sine and cosine.  FP32 arguments up to a few hundred.
-__device__ __forceinline__ void reduced_cos_sin(float t, float& c, float& s) {
-  const float n = rintf(t * 0.636619772f);
-  float r = fmaf(-n, 1.57079637f, t);
-  r = fmaf(-n, -4.37113883e-8f, r);
-  float cr, sr;
-  taylor_cos_sin(r, cr, sr);
-  const int q = static_cast<int>(n) & 3;
-  c = (q == 0) ? cr : (q == 1) ? -sr : (q == 2) ? -cr : sr;
-  s = (q == 0) ? sr : (q == 1) ? cr : (q == 2) ? -sr : -cr;
-}
-
-// e^{i theta} for an FP64 angle: the reduction by pi/2 in FP64 (two-part constant), the
-// series and the quadrant in FP32; absolute error ~1e-7.
-__device__ __forceinline__ void phase_cos_sin(double theta, float& c, float& s) {
-  const double n = rint(theta * 0.63661977236758134308);
-  double r = fma(-n, 1.5707963267948966192, theta);
-  r = fma(-n, 6.1232339957367660359e-17, r);
-  float cr, sr;
-  taylor_cos_sin(static_cast<float>(r), cr, sr);
-  const int q = static_cast<int>(static_cast<long long>(n) & 3);
-  c = (q == 0) ? cr : (q == 1) ? -sr : (q == 2) ? -cr : sr;
-  s = (q == 0) ? sr : (q == 1) ? cr : (q == 2) ? -sr : -cr;
-}
-
 // Per-pair constants of the FP32 far-pair quadrature.
 template <int QT>
 struct FarPair {
   static constexpr int kCap = QT > 0 ? QT : kMaxRegularPoints;
-  float fdx, fdy, fdz;      // dc = c_x - c_y in FP32
+  float m2dx, m2dy, m2dz;   // -2 dc, dc = c_x - c_y in FP32
   float fa0, fa1, fa2;      // normal-derivative factors in tangent coordinates
-  float r0f, r0sq, kf;      // Helmholtz: reference distance and wavenumber
-  float yx[kCap], yy[kCap], yz[kCap];  // trial points relative to c_y
-  float wq[kCap];           // trial weights (times the ADL factor)
-  float beta[kCap];         // 2 dc . dy_q (Helmholtz)
+  float r0f, r0sq, kf;      // reference distance (Helmholtz), |dc|^2, wavenumber
+  float yx[kCap], yy[kCap], yz[kCap], yn[kCap];  // trial points relative to c_y, |.|^2
+  float wq[kCap];           // trial weights times the ADL factor
 };
 
 // Sums of one far pair in FP32: blk[a][b] and S (see block_fp64 for their meaning),
-// without the reference phase e^{ik r0}.
-template <int QT, int KER, int OP, int NBT, int NBS, bool kTaylorOnly>
+// without the reference phase e^{ik r0}.  kSmallPhase: |k (r - r0)| <= 0.8 for every
+// point pair, and the trial data sit in registers (fully unrolled inner loop); otherwise
+// the inner loop reads the trial data from shared memory and reduces the phase.
+template <int QT, int KER, int OP, int NBT, int NBS, bool kSmallPhase>
 __device__ __forceinline__ void far_sums(const Tile& T, int it, const Tile& S, int js,
                                          const RegularRule& rule, const FarPair<QT>& fp,
                                          float blk_re[NBT][NBS],
@@ -273,38 +224,37 @@ __device__ __forceinline__ void far_sums(const Tile& T, int it, const Tile& S, i
   for (int p = 0; p < Q; ++p) {
     const float ax = T.R(p, 0, it), ay = T.R(p, 1, it), az = T.R(p, 2, it);
     const float apf = OP == kDL ? fmaf(rule.uf[p], fp.fa1, fmaf(rule.vf[p], fp.fa2, fp.fa0)) : 1.f;
-    const float alpha = kC ? 2.f * fmaf(fp.fdx, ax, fmaf(fp.fdy, ay, fp.fdz * az)) : 0.f;
-    const float px = fp.fdx + ax, py = fp.fdy + ay, pz = fp.fdz + az;
+    const float wx = fmaf(-2.f, ax, fp.m2dx), wy = fmaf(-2.f, ay, fp.m2dy),
+                wz = fmaf(-2.f, az, fp.m2dz);
+    // A_p (Laplace: plus |dc|^2, so that the sum below is r^2 itself)
+    const float Ap = fmaf(-ax, fp.m2dx, fmaf(-ay, fp.m2dy, fmaf(-az, fp.m2dz,
+                                                                T.R(p, 3, it) + (kC ? 0.f : fp.r0sq))));
     float u_re[NBS], u_im[NBS], g_re = 0.f, g_im = 0.f;
 #pragma unroll
     for (int b = 0; b < NBS; ++b) u_re[b] = u_im[b] = 0.f;
-#pragma unroll(kTaylorOnly ? 6 : 1)
+#pragma unroll(kSmallPhase ? 6 : 1)
     for (int q = 0; q < Q; ++q) {
       // the general (rare) path reads the trial data from shared memory so that the
       // per-pair register arrays are only indexed by compile-time constants
-      const float yq0 = kTaylorOnly ? fp.yx[q] : S.R(q, 0, js);
-      const float yq1 = kTaylorOnly ? fp.yy[q] : S.R(q, 1, js);
-      const float yq2 = kTaylorOnly ? fp.yz[q] : S.R(q, 2, js);
-      const float wq = kTaylorOnly ? fp.wq[q]
-                       : (OP == kADL ? rule.wf[q] * fmaf(rule.uf[q], fp.fa1, fmaf(rule.vf[q], fp.fa2, fp.fa0))
-                                     : rule.wf[q]);
-      const float beta_q = kTaylorOnly ? fp.beta[q]
-                           : 2.f * fmaf(fp.fdx, yq0, fmaf(fp.fdy, yq1, fp.fdz * yq2));
+      const float yq0 = kSmallPhase ? fp.yx[q] : S.R(q, 0, js);
+      const float yq1 = kSmallPhase ? fp.yy[q] : S.R(q, 1, js);
+      const float yq2 = kSmallPhase ? fp.yz[q] : S.R(q, 2, js);
+      const float yqn = kSmallPhase ? fp.yn[q] : S.R(q, 3, js);
+      const float wq = OP != kADL ? rule.wf[q]
+                       : kSmallPhase ? fp.wq[q]
+                                    : rule.wf[q] * fmaf(rule.uf[q], fp.fa1, fmaf(rule.vf[q], fp.fa2, fp.fa0));
+      const float s = fmaf(wx, yq0, fmaf(wy, yq1, fmaf(wz, yq2, Ap + yqn)));
       float kre, kim = 0.f;
       if (!kC) {
-        const float dx = px - yq0, dy = py - yq1, dz = pz - yq2;
-        const float rinv = rsqrt_approx(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+        const float rinv = rsqrt_approx(s);  // s is r^2 here
         kre = (OP == kSL || OP == kHS) ? wq * rinv : wq * (rinv * rinv * rinv);
       } else {
-        const float Dx = ax - yq0, Dy = ay - yq1, Dz = az - yq2;
-        const float s = (alpha - beta_q) + fmaf(Dx, Dx, fmaf(Dy, Dy, Dz * Dz));
         const float r2 = fp.r0sq + s;
         const float rinv = rsqrt_approx(r2);
-        const float r = r2 * rinv;
-        const float t = fp.kf * s * rcp_approx(r + fp.r0f);  // k (r - r0)
+        const float t = fp.kf * s * rcp_approx(fmaf(r2, rinv, fp.r0f));  // k (r - r0)
         float cs, sn;
-        if (kTaylorOnly)
-          taylor_cos_sin(t, cs, sn);
+        if (kSmallPhase)
+          poly_cos_sin(t, cs, sn);
         else
           reduced_cos_sin(t, cs, sn);
         if (OP == kSL || OP == kHS) {
@@ -313,7 +263,7 @@ __device__ __forceinline__ void far_sums(const Tile& T, int it, const Tile& S, i
           kim = f * sn;
         } else {
           // (1 - ik r) e^{ik r} / r^3 with e^{ik r0} applied per pair
-          const float f = wq * (rinv * rinv * rinv), kr = fp.kf * r;
+          const float f = wq * (rinv * rinv * rinv), kr = fp.kf * (r2 * rinv);
           kre = f * fmaf(kr, sn, cs);
           kim = f * fmaf(-kr, cs, sn);
         }
@@ -369,9 +319,11 @@ __device__ __forceinline__ void block_fp32(const Tile& T, int it, const Tile& S,
   FarPair<QT> fp;
   const double dcx = T.G(fCx, it) - S.G(fCx, js), dcy = T.G(fCy, it) - S.G(fCy, js),
                dcz = T.G(fCz, it) - S.G(fCz, js);
-  fp.fdx = static_cast<float>(dcx);
-  fp.fdy = static_cast<float>(dcy);
-  fp.fdz = static_cast<float>(dcz);
+  const float fdx = static_cast<float>(dcx), fdy = static_cast<float>(dcy),
+              fdz = static_cast<float>(dcz);
+  fp.m2dx = -2.f * fdx;
+  fp.m2dy = -2.f * fdy;
+  fp.m2dz = -2.f * fdz;
   fp.fa0 = fp.fa1 = fp.fa2 = 0.f;
   if (OP == kDL) {
     const double nx = S.G(fNx, js), ny = S.G(fNy, js), nz = S.G(fNz, js);
@@ -385,31 +337,35 @@ __device__ __forceinline__ void block_fp32(const Tile& T, int it, const Tile& S,
     fp.fa2 = static_cast<float>(S.G(fT1x, js) * nx + S.G(fT1y, js) * ny + S.G(fT1z, js) * nz);
   }
   float ph_c = 1.f, ph_s = 0.f;
-  bool taylor = true;
-  fp.r0f = fp.r0sq = fp.kf = 0.f;
+  bool small_phase = true;
+  fp.r0f = fp.kf = 0.f;
+  fp.r0sq = fmaf(fdx, fdx, fmaf(fdy, fdy, fdz * fdz));
   if (kC) {
-    const double r0 = sqrt(dcx * dcx + dcy * dcy + dcz * dcz);
+    const double r0sq = dcx * dcx + dcy * dcy + dcz * dcz;
+    const double r0 = r0sq * rsqrt_refined(r0sq);
     fp.r0f = static_cast<float>(r0);
-    fp.r0sq = fp.r0f * fp.r0f;
+    fp.r0sq = static_cast<float>(r0sq);
     fp.kf = static_cast<float>(k);
     phase_cos_sin(k * r0, ph_c, ph_s);
-    taylor = k * (T.G(fRad, it) + S.G(fRad, js)) <= static_cast<double>(kTaylorMax);
+    // warp-uniform choice, so that a warp never runs both variants
+    small_phase = __all_sync(__activemask(), k * (T.G(fRad, it) + S.G(fRad, js)) <=
+                                                 static_cast<double>(kSmallPhaseMax));
   }
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     fp.yx[q] = S.R(q, 0, js);
     fp.yy[q] = S.R(q, 1, js);
     fp.yz[q] = S.R(q, 2, js);
+    fp.yn[q] = S.R(q, 3, js);
     fp.wq[q] = OP == kADL ? rule.wf[q] * fmaf(rule.uf[q], fp.fa1, fmaf(rule.vf[q], fp.fa2, fp.fa0))
                           : rule.wf[q];
-    if (kC) fp.beta[q] = 2.f * fmaf(fp.fdx, fp.yx[q], fmaf(fp.fdy, fp.yy[q], fp.fdz * fp.yz[q]));
   }
   float blk_re[NBT][NBS], blk_im[NBT][NBS], S_re = 0.f, S_im = 0.f;
 #pragma unroll
   for (int a = 0; a < NBT; ++a)
 #pragma unroll
     for (int b = 0; b < NBS; ++b) blk_re[a][b] = blk_im[a][b] = 0.f;
-  if (!kC || taylor)
+  if (small_phase)
     far_sums<QT, KER, OP, NBT, NBS, true>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
   else
     far_sums<QT, KER, OP, NBT, NBS, false>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
@@ -464,10 +420,11 @@ __device__ __forceinline__ void deposit(double* acc_re, double* acc_im, int ndt,
 template <int QT, int KER, int OP, int NBT, int NBS, bool MIXED, bool DIRECT>
 __global__ void __launch_bounds__(kThreads, 4)
     regular_tiles(CellSet test, SpaceTiles tt, CellSet trial, SpaceTiles st, RegularRule rule,
-                  double k, int same_grid, double* __restrict__ out, int64_t ld) {
+                  double k, int same_grid, double* __restrict__ out, int64_t ld, int tile_y0) {
   constexpr bool kC = KER == kHelmholtz;
   const int Q = QT > 0 ? QT : rule.npts;
-  const int ti0 = blockIdx.x * kTile, sj0 = blockIdx.y * kTile;
+  const int sy = blockIdx.y + tile_y0;  // trial tile
+  const int ti0 = blockIdx.x * kTile, sj0 = sy * kTile;
   const int nti = min(kTile, test.ncells - ti0), nsj = min(kTile, trial.ncells - sj0);
 
   extern __shared__ __align__(16) unsigned char smem[];
@@ -478,8 +435,8 @@ __global__ void __launch_bounds__(kThreads, 4)
   if (!DIRECT) {
     tdof0 = tt.tile_dof_off[blockIdx.x];
     ndt = tt.tile_dof_off[blockIdx.x + 1] - tdof0;
-    sdof0 = st.tile_dof_off[blockIdx.y];
-    nds = st.tile_dof_off[blockIdx.y + 1] - sdof0;
+    sdof0 = st.tile_dof_off[sy];
+    nds = st.tile_dof_off[sy + 1] - sdof0;
     const int cap = tt.max_tile_dofs * st.max_tile_dofs;
     acc_re = reinterpret_cast<double*>(cursor);
     acc_im = acc_re + cap;
@@ -757,9 +714,15 @@ cudaError_t launch_one(const CellSet& test, const SpaceTiles& tt, const CellSet&
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  dim3 grid((test.ncells + kTile - 1) / kTile, (trial.ncells + kTile - 1) / kTile);
+  const int trial_tiles = (trial.ncells + kTile - 1) / kTile;
+  if (a.trial_tile0 < 0 || a.trial_tile0 > trial_tiles || a.trial_tiles < 0)
+    return cudaErrorInvalidValue;
+  const int ny = a.trial_tiles > 0 ? std::min(a.trial_tiles, trial_tiles - a.trial_tile0)
+                                   : trial_tiles - a.trial_tile0;
+  if (ny <= 0) return cudaSuccess;
+  dim3 grid((test.ncells + kTile - 1) / kTile, ny);
   fn<<<grid, kThreads, smem, stream>>>(test, tt, trial, st, rule, a.k, a.same_grid,
-                                       static_cast<double*>(a.out), a.ld);
+                                       static_cast<double*>(a.out), a.ld, a.trial_tile0);
   return cudaGetLastError();
 }
 

@@ -36,12 +36,13 @@ __global__ void __launch_bounds__(kThreads)
     singular_fp64(CellSet test, const int* __restrict__ tdofs, CellSet trial,
                   const int* __restrict__ sdofs, SingularRules rules, SingularPairs pairs,
                   double k, double* __restrict__ out, int64_t ld, int unique_entries,
-                  double* __restrict__ pair_values) {
+                  double* __restrict__ pair_values, int trial_lo, int trial_hi) {
   constexpr bool kCplx = KER == kHelmholtz;
   const int lane = threadIdx.x & 31;
   const int pair = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
   if (pair >= pairs.npairs) return;
   const int tc = __ldg(pairs.test_cell + pair), sc = __ldg(pairs.trial_cell + pair);
+  if (sc < trial_lo || sc >= trial_hi) return;  // warp-uniform: one pair per warp
   const int cfg = __ldg(pairs.config + pair);
   CellData x, y;
   load_cell(test, tc, x);
@@ -222,7 +223,7 @@ cudaError_t launch_one(const CellSet& test, const int* tdofs, const CellSet& tri
   const int blocks = (pairs.npairs + warps - 1) / warps;
   singular_fp64<KER, OP, NBT, NBS><<<blocks, kThreads, 0, stream>>>(
       test, tdofs, trial, sdofs, rules, pairs, a.k, static_cast<double*>(a.out), a.ld,
-      a.unique_entries, a.pair_values);
+      a.unique_entries, a.pair_values, a.trial_lo, a.trial_hi);
   return cudaGetLastError();
 }
 

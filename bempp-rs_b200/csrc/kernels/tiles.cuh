@@ -20,17 +20,18 @@ enum TileField : int {
 // Shared-memory image of a tile of kTile cells.
 struct Tile {
   double* pts;  // [(q*3+d) * kTile + c] absolute FP64 points
-  float* rel;   // [(q*3+d) * kTile + c] FP32 offsets from the centroid (mixed only)
+  float* rel;   // [(q*4+d) * kTile + c] FP32 offsets from the centroid, d = 3: their
+                //   squared length (mixed only)
   double* geo;  // [f * kTile + c]
   int* vid;     // [v * kTile + c]
   int* ldof;    // [b * kTile + c]
   __device__ __forceinline__ double P(int q, int d, int c) const { return pts[(q * 3 + d) * kTile + c]; }
-  __device__ __forceinline__ float R(int q, int d, int c) const { return rel[(q * 3 + d) * kTile + c]; }
+  __device__ __forceinline__ float R(int q, int d, int c) const { return rel[(q * 4 + d) * kTile + c]; }
   __device__ __forceinline__ double G(int f, int c) const { return geo[f * kTile + c]; }
 };
 
 __host__ __device__ inline size_t tile_doubles(int q) { return (3 * q + kTileFields) * kTile; }
-__host__ __device__ inline size_t tile_floats(int q, bool mixed) { return mixed ? 3 * q * kTile : 0; }
+__host__ __device__ inline size_t tile_floats(int q, bool mixed) { return mixed ? 4 * q * kTile : 0; }
 __host__ __device__ inline size_t tile_ints(int nb) { return (3 + nb) * kTile; }
 
 // Carves a tile out of shared memory starting at *cursor (8-byte aligned).
@@ -53,10 +54,19 @@ __device__ inline void load_tile(const Tile& t, const CellSet& cs, int c0, int n
   const int N = cs.ncells;
   for (int idx = threadIdx.x; idx < 3 * q * kTile; idx += kThreads) {
     const int c = idx % kTile, pd = idx / kTile;
-    const int64_t src = static_cast<int64_t>(pd) * N + c0 + min(c, n - 1);
-    t.pts[idx] = __ldg(cs.qpts + src);
-    if (mixed) t.rel[idx] = __ldg(cs.qrel + src);
+    t.pts[idx] = __ldg(cs.qpts + static_cast<int64_t>(pd) * N + c0 + min(c, n - 1));
   }
+  if (mixed)
+    for (int idx = threadIdx.x; idx < q * kTile; idx += kThreads) {
+      const int c = idx % kTile, p = idx / kTile;
+      const float* src = cs.qrel + static_cast<int64_t>(3 * p) * N + c0 + min(c, n - 1);
+      const float x = __ldg(src), y = __ldg(src + N), z = __ldg(src + 2 * N);
+      float* dst = t.rel + 4 * p * kTile + c;
+      dst[0] = x;
+      dst[kTile] = y;
+      dst[2 * kTile] = z;
+      dst[3 * kTile] = fmaf(x, x, fmaf(y, y, z * z));
+    }
   for (int c = threadIdx.x; c < kTile; c += kThreads) {
     const int cell = c0 + min(c, n - 1);
     const double nx = g(cs.geom, kNx, N, cell), ny = g(cs.geom, kNy, N, cell),
@@ -76,6 +86,64 @@ __device__ inline void load_tile(const Tile& t, const CellSet& cs, int c0, int n
   }
 }
 
+
+// ---- FP32 helpers of the mixed-precision paths ----
+
+__device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
+  const float y = v - comp;
+  const float t = sum + y;
+  comp = (t - sum) - y;
+  sum = t;
+}
+
+// cos(t), sin(t) for |t| <= 0.8: polynomials in z = t^2 of degree 8 (cos) and 7 (sin)
+// with the leading coefficient fixed to 1, fitted by minimising the maximum error on
+// [-0.8, 0.8] (discrete minimax over 6001 points, a linear program); approximation
+// errors 6.5e-11 (cos) and 3.3e-9 (sin), below FP32 rounding.
+__device__ __forceinline__ void poly_cos_sin(float t, float& c, float& s) {
+  const float z = t * t;
+  c = fmaf(z, fmaf(z, fmaf(z, fmaf(z, 2.43751438e-5f, -1.38866017e-3f), 4.16666195e-2f), -0.5f),
+           1.0f);
+  s = t * fmaf(z, fmaf(z, fmaf(z, -1.95052402e-4f, 8.33209045e-3f), -0.166666538f), 1.0f);
+}
+
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// cos and sin of an argument of any moderate size: Cody-Waite reduction by multiples of
+// pi/2 (two-part constant) to |r| <= pi/4, the polynomials above there, and the
+// quadrant's exchange of sine and cosine.  FP32 arguments up to a few hundred.
+__device__ __forceinline__ void reduced_cos_sin(float t, float& c, float& s) {
+  const float n = rintf(t * 0.636619772f);
+  float r = fmaf(-n, 1.57079637f, t);
+  r = fmaf(-n, -4.37113883e-8f, r);
+  float cr, sr;
+  poly_cos_sin(r, cr, sr);
+  const int q = static_cast<int>(n) & 3;
+  c = (q == 0) ? cr : (q == 1) ? -sr : (q == 2) ? -cr : sr;
+  s = (q == 0) ? sr : (q == 1) ? cr : (q == 2) ? -sr : -cr;
+}
+
+// e^{i theta} for an FP64 angle: the reduction by pi/2 in FP64 (two-part constant), the
+// series and the quadrant in FP32; absolute error ~1e-7.
+__device__ __forceinline__ void phase_cos_sin(double theta, float& c, float& s) {
+  const double n = rint(theta * 0.63661977236758134308);
+  double r = fma(-n, 1.5707963267948966192, theta);
+  r = fma(-n, 6.1232339957367660359e-17, r);
+  float cr, sr;
+  poly_cos_sin(static_cast<float>(r), cr, sr);
+  const int q = static_cast<int>(static_cast<long long>(n) & 3);
+  c = (q == 0) ? cr : (q == 1) ? -sr : (q == 2) ? -cr : sr;
+  s = (q == 0) ? sr : (q == 1) ? cr : (q == 2) ? -sr : -cr;
+}
 
 }  // namespace tiles
 }  // namespace bempp_b200

@@ -364,13 +364,31 @@ def adjoint_timing(args):
         torch.cuda.synchronize()
         return t0.elapsed_time(t1) / reps
 
+    gopts_m = BoundaryAssemblerOptions()
+    gopts_m.set_regular_quadrature_degree(ReferenceCellType.Triangle, Q_REGULAR)
+    from bempp.assembly.boundary import Precision
+
+    gopts_m.set_precision(Precision.Mixed)
+    grad_m = torch.zeros_like(grad)
+    tot_m = torch.zeros_like(tot)
+
+    def gradient_mixed():
+        check(lib.bempp_helmholtz_single_layer_dp0_gradient_device(
+            g, gopts_m._rs_options, k, ffi.cast("void*", lam.data_ptr()),
+            ffi.cast("void*", mu.data_ptr()), ffi.cast("double*", tot_m.data_ptr()),
+            ffi.cast("double*", grad_m.data_ptr()), ffi.cast("void*", stream)), "gradient")
+
     f_ms = timed(forward, 5)
     g_ms = timed(gradient, 5)
+    gm_ms = timed(gradient_mixed, 5)
+    mixed_err = ((grad_m - grad).abs().max() / grad.abs().max()).item()
     jf = forward().item()
     gradient()
     torch.cuda.synchronize()
     return {"workload": "helmholtz_sl_dp0_ico4_k5_gradient", "forward_ms": f_ms,
             "gradient_ms": g_ms, "gradient_over_forward": g_ms / f_ms,
+            "gradient_mixed_ms": gm_ms, "gradient_mixed_over_forward": gm_ms / f_ms,
+            "gradient_mixed_max_rel_err_vs_fp64": mixed_err,
             "J_forward": jf, "J_adjoint": tot[0].item(),
             "note": "forward = dense FP64 assembly into HBM + Re(lambda^H A mu); gradient = "
                     "one adjoint pass (all 7686 coordinates and k)"}
@@ -439,7 +457,9 @@ def run_ours(args):
 
             dist.barrier()
 
-    w = WORKLOADS[args.workload]
+    w = dict(WORKLOADS[args.workload])
+    if args.k is not None:
+        w["k"] = args.k
     wl = Workload(w, args.precision, args.level)
     if args.once:
         wl.step(flush=False)
@@ -461,6 +481,20 @@ def run_ours(args):
     ms_per_step = max_over_ranks(ms_per_step, world)
     value = world * wl.entries_per_step / (ms_per_step * 1e-3)
 
+    mixed_same = None
+    if rank == 0 and not args.skip_north_star and args.precision == "fp64":
+        # the same workload with FP32 far pairs: speed and error against the FP64 result
+        ref = [o.clone() for o in wl.outs]
+        wm = Workload(w, "mixed", args.level)
+        ms_mixed, _ = wm.timed(max(2, args.steps // 2), 2)
+        errs = [(torch.linalg.norm(a - b) / torch.linalg.norm(b)).item()
+                for a, b in zip(wm.outs, ref)]
+        mixed_same = {"ms_per_step": ms_mixed, "entries_per_s": wm.entries_per_step / (ms_mixed * 1e-3),
+                      "speedup_vs_fp64": ms_per_step / ms_mixed,
+                      "rel_frobenius_error_vs_fp64": dict(zip(w["ops"], errs))}
+        del wm, ref
+        torch.cuda.empty_cache()
+
     e2e = None
     if not args.skip_e2e:
         pts_h = np.ascontiguousarray(wl.points)
@@ -469,10 +503,18 @@ def run_ours(args):
         torch.cuda.synchronize()
         barrier()
         t = time.perf_counter()
+        t_build = 0.0
+        t_ops = [0.0] * len(wl.assemblers)
+        copy_stats = [None] * len(wl.assemblers)
         for _ in range(e2e_steps):
+            t1 = time.perf_counter()
             _, s2 = build_space(pts_h, cells_h, w["space"])
-            for _, a in wl.assemblers:
+            t_build += time.perf_counter() - t1
+            for i, (_, a) in enumerate(wl.assemblers):
+                t1 = time.perf_counter()
                 a.assemble(s2, s2)
+                t_ops[i] += time.perf_counter() - t1
+                copy_stats[i] = a.host_copy_stats()
             del s2
         e2e_s = (time.perf_counter() - t) / e2e_steps
         e2e_s = max_over_ranks(e2e_s, world)
@@ -481,6 +523,11 @@ def run_ours(args):
                "h2d_bytes_per_step": int(pts_h.nbytes + cells_h.astype(np.uintp).nbytes),
                "d2h_bytes_per_step": int(wl.entries_per_step * esize),
                "ms_per_step": e2e_s * 1e3,
+               "breakdown_ms": {"grid_and_space": 1e3 * t_build / e2e_steps,
+                                "assemble": {n: 1e3 * t / e2e_steps
+                                             for (n, _), t in zip(wl.assemblers, t_ops)},
+                                "host_copy_last": {n: c for (n, _), c in zip(wl.assemblers,
+                                                                             copy_stats)}},
                "path": "function_space(grid) + BoundaryAssembler.assemble per operator (C-ABI "
                        "boundary_assembler_assemble_into_memory_ex, host numpy output)"}
 
@@ -528,6 +575,8 @@ def run_ours(args):
                        "l2": "flushed between steps (256 MiB write); outputs exceed L2"},
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "clocks": clocks,
         }
+        if mixed_same is not None:
+            line["mixed_same_workload"] = mixed_same
         if ns is not None:
             line["north_star"] = ns
         if adj is not None:
@@ -615,6 +664,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="p1")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--level", type=int, default=None, help="icosphere refinement override")
+    ap.add_argument("--k", type=float, default=None, help="wavenumber override (Helmholtz)")
     ap.add_argument("--once", action="store_true")
     ap.add_argument("--cpu-sample-cells", type=int, default=160)
     ap.add_argument("--skip-cpu", action="store_true")

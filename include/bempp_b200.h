@@ -166,6 +166,11 @@ void boundary_assembler_set_timing(BoundaryAssemblerT *assembler, bool enabled);
 size_t boundary_assembler_phase_times(BoundaryAssemblerT *assembler, double *ms, size_t n);
 /* Addition: number of kernel launches the last assembly enqueued. */
 size_t boundary_assembler_last_launch_count(BoundaryAssemblerT *assembler);
+/* Addition (no counterpart in the reference): statistics of the last host-memory
+ * assembly (boundary_assembler_assemble_into_memory[_ex] / boundary_assembler_assemble):
+ * [ms the host waited for device-to-host DMA, ms of host copies into the caller's array,
+ * copy groups, assembly chunks, host copy threads]; returns the number written (<= n). */
+size_t boundary_assembler_host_copy_stats(BoundaryAssemblerT *assembler, double *out, size_t n);
 /* Addition: measured CUDA-core fused multiply-add throughput of the current device in
  * TFLOP/s (fp64 != 0: FP64, else FP32), the roofline denominator of the regular
  * quadrature kernels. */

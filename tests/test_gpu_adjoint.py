@@ -100,3 +100,18 @@ def test_autograd_function():
     g = grad.cpu().numpy()
     assert np.abs(x.grad.numpy() - 2.0 * g).max() <= 1e-12 * np.abs(g).max()
     assert abs(k.grad.item() - 2.0 * dk.item()) <= 1e-12 * abs(dk.item())
+
+
+def test_mixed_gradient_matches_fp64_gradient():
+    """Mixed precision (FP32 far pairs): J and the gradient agree with the FP64 adjoint."""
+    from bempp.autograd import energy_and_gradient
+
+    pts, cells, lam, mu = problem(4)
+    j64, dk64, g64 = energy_and_gradient(pts, cells, K, lam, mu)
+    jm, dkm, gm = energy_and_gradient(pts, cells, K, lam, mu, mixed=True)
+    g64 = g64.cpu().numpy()
+    gm = gm.cpu().numpy()
+    assert abs(jm.item() - j64.item()) <= 1e-6 * abs(j64.item())
+    err = np.abs(gm - g64).max() / np.abs(g64).max()
+    assert 1e-13 < err <= 1e-5, err
+    assert abs(dkm.item() - dk64.item()) <= 1e-5 * abs(dk64.item())

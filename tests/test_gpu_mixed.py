@@ -44,3 +44,21 @@ def test_mixed_far_from_origin():
     a = gpu_assemble(grid, "laplace", "single_layer", precision=Precision.Mixed)
     o = oracle_assemble(grid, "laplace", "single_layer")
     assert rel_err(a, o) <= MIXED_TOL
+
+
+@pytest.mark.parametrize("kernel,op,k", [
+    ("laplace", "double_layer", 0.0),
+    ("laplace", "adjoint_double_layer", 0.0),
+    ("laplace", "hypersingular", 0.0),
+    ("helmholtz", "double_layer", 8.0),
+    ("helmholtz", "hypersingular", 8.0),
+])
+def test_mixed_p1_matches_oracle(kernel, op, k):
+    pts, cells = shapes.icosphere(3)
+    pts = shapes.radial_perturbation(pts, seed=4)
+    grid = Grid(pts, cells)
+    sp = (1, True)
+    a = gpu_assemble(grid, kernel, op, k, test=sp, trial=sp, precision=Precision.Mixed)
+    o = oracle_assemble(grid, kernel, op, k, test=sp, trial=sp)
+    err = rel_err(a, o)
+    assert 1e-13 < err <= MIXED_TOL
