@@ -282,7 +282,20 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
   ra.out_type = cplx ? kOutC128 : kOutF64;
   ra.ld = nt;
   ra.out = out;
+  // a margin of 1e-6 relative covers the device's own rounding of the radii
+  ra.small_phase = std::fabs(a.k) * (test.grid->max_circumradius() + trial.grid->max_circumradius()) *
+                               (1.0 + 1e-6) <= 0.8 ? 1 : 0;
+  if (ra.precision == kRegularMixed && nt > 0 && ns > 0) {
+    const NearField& nf = near_field(*test.grid, *trial.grid);
+    ra.near.tile_mask = nf.tile_mask.as<int>();
+    ra.near.masks = nf.masks.as<unsigned>();
+    ra.near.list = nf.list.as<int2>();
+    ra.near.nlist = nf.nlist;
+    ra.near.trial_tiles = nf.trial_tiles;
+  }
   const CellSet tcs = cell_set(*test.grid, tgeo), scs = cell_set(*trial.grid, sgeo);
+  // mixed: the FP32 far-pair launch and the FP64 near-pair launch
+  const size_t regular_launches = ra.near.nlist > 0 ? 2 : 1;
 
   const bool empty = nt == 0 || ns == 0;
   const bool singular = same_grid && !empty;
@@ -304,12 +317,13 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
     sa.out = out;
     sa.unique_entries = dp0 ? 1 : 0;
     sa.pair_values = nullptr;
+    sa.fast = ra.precision == kRegularMixed ? 1 : 0;
   }
-  auto run_singular = [&](int lo, int hi) {
+  auto run_singular = [&](int lo, int hi, cudaStream_t s) {
     sa.trial_lo = lo;
     sa.trial_hi = hi;
     BEMPP_CUDA(launch_singular(tcs, test.d_dofs.as<int>(), test.nbasis, scs,
-                               trial.d_dofs.as<int>(), trial.nbasis, rules, pairs, sa, stream));
+                               trial.d_dofs.as<int>(), trial.nbasis, rules, pairs, sa, s));
     ++a.launches;
   };
   const int tiles = static_cast<int>((trial.grid->ncells + 31) / 32);
@@ -319,9 +333,30 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
   };
 
   if (dp0) {
-    // the direct kernel writes every entry (zero for vertex-sharing pairs), so each chunk
-    // is its regular launch followed by the singular pairs of its trial cells
+    // the direct kernels write every entry once, so each chunk is its regular launches
+    // followed by the singular pairs of its trial cells.  Mixed precision: the regular
+    // kernels leave the vertex-sharing entries alone, and the singular kernel of a
+    // one-chunk assembly runs on a side stream beside them (fork / join events).
     timer.mark();  // no memset phase
+    const bool fork = singular && nchunks == 1 && ra.precision == kRegularMixed;
+    if (fork) {
+      if (!a.side || a.side_device != device) {
+        if (a.side) {
+          cudaStreamDestroy(a.side);
+          cudaEventDestroy(a.fork_ev);
+          cudaEventDestroy(a.join_ev);
+          a.side = nullptr;
+        }
+        BEMPP_CUDA(cudaStreamCreateWithFlags(&a.side, cudaStreamNonBlocking));
+        BEMPP_CUDA(cudaEventCreateWithFlags(&a.fork_ev, cudaEventDisableTiming));
+        BEMPP_CUDA(cudaEventCreateWithFlags(&a.join_ev, cudaEventDisableTiming));
+        a.side_device = device;
+      }
+      BEMPP_CUDA(cudaEventRecord(a.fork_ev, stream));
+      BEMPP_CUDA(cudaStreamWaitEvent(a.side, a.fork_ev, 0));
+      run_singular(0, 0x7fffffff, a.side);
+      BEMPP_CUDA(cudaEventRecord(a.join_ev, a.side));
+    }
     for (int c = 0; c < nchunks; ++c) {
       int t0, t1;
       tile_range(c, t0, t1);
@@ -329,9 +364,12 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
         ra.trial_tile0 = t0;
         ra.trial_tiles = t1 - t0;
         BEMPP_CUDA(launch_regular_dp0(tcs, scs, rule, ra, stream));
-        ++a.launches;
+        a.launches += regular_launches;
         if (nchunks == 1) timer.mark();
-        if (singular) run_singular(nchunks == 1 ? 0 : 32 * t0, nchunks == 1 ? 0x7fffffff : 32 * t1);
+        if (fork)
+          BEMPP_CUDA(cudaStreamWaitEvent(stream, a.join_ev, 0));
+        else if (singular)
+          run_singular(nchunks == 1 ? 0 : 32 * t0, nchunks == 1 ? 0x7fffffff : 32 * t1, stream);
         if (single) {
           const std::vector<std::pair<int64_t, int64_t>> all{{0, ns}};
           for (const auto& run : nchunks == 1 ? all : chunk_columns(trial, nchunks)[c]) {
@@ -352,7 +390,7 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
     if (!empty) BEMPP_CUDA(cudaMemsetAsync(out, 0, static_cast<size_t>(nt) * ns * esize, stream));
     timer.mark();
     // chunked: the singular pairs first (all adds commute), then the regular chunks
-    if (singular && nchunks > 1) run_singular(0, 0x7fffffff);
+    if (singular && nchunks > 1) run_singular(0, 0x7fffffff, stream);
     for (int c = 0; c < nchunks; ++c) {
       int t0, t1;
       tile_range(c, t0, t1);
@@ -361,11 +399,11 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
         ra.trial_tiles = t1 - t0;
         BEMPP_CUDA(launch_regular_scatter(tcs, space_tiles(test), scs, space_tiles(trial), rule,
                                           ra, stream));
-        ++a.launches;
+        a.launches += regular_launches;
       }
       if (nchunks == 1) {
         timer.mark();
-        if (singular) run_singular(0, 0x7fffffff);
+        if (singular) run_singular(0, 0x7fffffff, stream);
         if (single && !empty) {
           BEMPP_CUDA(launch_convert_to_single(static_cast<const double*>(out), d_out,
                                               static_cast<size_t>(nt) * ns * (cplx ? 2 : 1), stream));
@@ -530,4 +568,9 @@ BoundaryAssemblerT::~BoundaryAssemblerT() {
   for (auto& e : events)
     if (e) cudaEventDestroy(e);
   if (stream) cudaStreamDestroy(stream);
+  if (side) {
+    cudaStreamDestroy(side);
+    cudaEventDestroy(fork_ev);
+    cudaEventDestroy(join_ev);
+  }
 }

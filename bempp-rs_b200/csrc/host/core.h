@@ -110,6 +110,14 @@ struct GridGeometry {  // device geometry for one regular rule
   DeviceBuffer geom, qpts, qrel, vids;
 };
 
+// Near field of a (test grid, trial grid) pair for the mixed-precision kernels (near.cpp):
+// the device arrays behind NearArgs.
+struct NearField {
+  int test_tiles = 0, trial_tiles = 0, nlist = 0;
+  DeviceBuffer tile_mask, masks, list;
+  size_t near_pairs = 0;  // marked pairs (near or vertex-sharing)
+};
+
 // Per chunk of a chunked assembly: runs (first column, number of columns).
 using ColumnRuns = std::vector<std::vector<std::pair<int64_t, int64_t>>>;
 
@@ -138,8 +146,12 @@ struct GridT {
   std::map<int, std::unique_ptr<bempp_b200::GridGeometry>> geometry;  // keyed by regular npts
   std::unique_ptr<bempp_b200::SingularPairList> pairs;
   DeviceBuffer adjoint_scratch;  // per-cell vertex gradients of the adjoint kernel
+  double max_rad = -1.0;         // largest centroid-to-vertex distance (computed on demand)
+  // near fields with other grids (and itself), keyed by the trial grid's uid
+  std::map<uint64_t, std::unique_ptr<bempp_b200::NearField>> near_fields;
   std::mutex mu;
   void build_topology();
+  double max_circumradius();
 };
 
 struct ElementFamilyT {
@@ -189,6 +201,11 @@ struct BoundaryAssemblerT {
   int events_recorded = 0;
   DeviceBuffer work;     // device output for host-memory assembly
   cudaStream_t stream = nullptr;  // host-memory assembly stream (created on first use)
+  // side stream and fork / join events: the singular kernel of a mixed-precision DP0
+  // assembly runs beside the regular kernels (created on first use, on side_device)
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  int side_device = -1;
   // last host-memory assembly: ms waiting for DMA, ms of host copy, copy groups, chunks,
   // host copy threads
   std::array<double, 5> host_copy_stats{};
@@ -221,6 +238,9 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
 const ColumnRuns& chunk_columns(SpaceT& trial, int nchunks);
 // Number of chunks assemble_device uses for a request of `want` (at most one per tile).
 int effective_chunks(const SpaceT& trial, int want);
+// Near field of (test, trial) on the current device, built on first use and cached in
+// the test grid.
+const NearField& near_field(GridT& test, GridT& trial);
 // Dense assembly into host memory: chunked device assembly with the device-to-host copy
 // of finished columns (pinned staging ring, parallel host copy) overlapped (host_copy.cpp).
 void assemble_host(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* data);

@@ -57,7 +57,7 @@ class CopyPool {
  private:
   CopyPool() {
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const int n = static_cast<int>(std::min(16u, std::max(1u, hw / 2)));
+    const int n = static_cast<int>(std::min(32u, std::max(1u, hw)));
     for (int i = 1; i < n; ++i) workers_.emplace_back([this, i] { loop(i); });
   }
   ~CopyPool() {

@@ -12,6 +12,7 @@
 //   tiles:           the DOFs touched by each run of 32 consecutive cells, for the
 //                    tile-scatter kernel.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "core.h"
@@ -182,3 +183,24 @@ void build_tiles(const SpaceT& s, int tile, std::vector<int>& off, std::vector<i
 }
 
 }  // namespace bempp_b200
+
+// Largest distance from a cell's centroid to its vertices: bounds |x - c_x| for every
+// point of the cell (the mixed-precision kernels' phase bound k (rad_x + rad_y)).
+double GridT::max_circumradius() {
+  std::lock_guard<std::mutex> lock(mu);
+  if (max_rad >= 0.0) return max_rad;
+  double m = 0.0;
+  for (int64_t c = 0; c < ncells; ++c) {
+    const double* v[3] = {&points[3 * cells[3 * c]], &points[3 * cells[3 * c + 1]],
+                          &points[3 * cells[3 * c + 2]]};
+    double cen[3];
+    for (int d = 0; d < 3; ++d) cen[d] = (v[0][d] + v[1][d] + v[2][d]) / 3.0;
+    for (int i = 0; i < 3; ++i) {
+      const double x = v[i][0] - cen[0], y = v[i][1] - cen[1], z = v[i][2] - cen[2];
+      m = std::max(m, std::sqrt(x * x + y * y + z * z));
+    }
+  }
+  max_rad = m;
+  return m;
+}
+

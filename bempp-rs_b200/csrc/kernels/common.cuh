@@ -82,6 +82,39 @@ __device__ __forceinline__ double rsqrt_refined(double a) {
   return fma(y * e, fma(e, 0.375, 0.5), y);
 }
 
+// sin(t) and cos(t) in FP64 for moderate |t| (the phases k r of boundary-element
+// kernels): Cody-Waite reduction r = t - n pi/2 with pi/2 split into two doubles (each
+// step one fused multiply-add), Taylor series of cos and sin on |r| <= pi/4 up to r^16
+// and r^17 (truncation below 1e-19), and the quadrant's exchange of sine and cosine.
+// Absolute error about 1e-16 for |t| up to 1e5 (checked against libm on [-40, 40]).
+__device__ __forceinline__ void sincos_cw(double t, double& s, double& c) {
+  const double n = rint(t * 0.63661977236758134308);
+  double r = fma(-n, 1.5707963267948966192, t);
+  r = fma(-n, 6.1232339957367660359e-17, r);
+  const double z = r * r;
+  double cr = 1.0 / 20922789888000.0;  // 1/16!
+  cr = fma(cr, z, -1.0 / 87178291200.0);
+  cr = fma(cr, z, 1.0 / 479001600.0);
+  cr = fma(cr, z, -1.0 / 3628800.0);
+  cr = fma(cr, z, 1.0 / 40320.0);
+  cr = fma(cr, z, -1.0 / 720.0);
+  cr = fma(cr, z, 1.0 / 24.0);
+  cr = fma(cr, z, -0.5);
+  cr = fma(cr, z, 1.0);
+  double sr = 1.0 / 355687428096000.0;  // 1/17!
+  sr = fma(sr, z, -1.0 / 1307674368000.0);
+  sr = fma(sr, z, 1.0 / 6227020800.0);
+  sr = fma(sr, z, -1.0 / 39916800.0);
+  sr = fma(sr, z, 1.0 / 362880.0);
+  sr = fma(sr, z, -1.0 / 5040.0);
+  sr = fma(sr, z, 1.0 / 120.0);
+  sr = fma(sr, z, -1.0 / 6.0);
+  sr = r * fma(sr, z, 1.0);
+  const int q = static_cast<int>(static_cast<long long>(n) & 3);
+  c = (q == 0) ? cr : (q == 1) ? -sr : (q == 2) ? -cr : sr;
+  s = (q == 0) ? sr : (q == 1) ? cr : (q == 2) ? -sr : -cr;
+}
+
 // P1 basis on the reference triangle: phi0 = 1 - x - y, phi1 = x, phi2 = y.
 __device__ __forceinline__ void p1_basis(double x, double y, double* phi) {
   phi[0] = 1.0 - x - y;

@@ -22,6 +22,19 @@ enum RegularPrecision : int { kRegularFP64 = 0, kRegularMixed = 1 };
 // Output element type of a dense matrix.
 enum OutType : int { kOutF64 = 0, kOutC128 = 1, kOutF32 = 2, kOutC64 = 3 };
 
+// Near field of a (test grid, trial grid) pair for the mixed-precision kernels, built on
+// the host: per tile pair (test tile * trial tiles + trial tile) the index of its 32-word
+// mask or -1; mask word [m * 32 + test lane] has bit j set when the pair (test lane, trial
+// cell j) is near (centroid distance < 2 max diameter) or shares a vertex.  `list` holds
+// (tile pair, m) for every tile pair with a mask.
+struct NearArgs {
+  const int* tile_mask = nullptr;
+  const unsigned* masks = nullptr;
+  const int2* list = nullptr;
+  int nlist = 0;
+  int trial_tiles = 0;
+};
+
 struct RegularArgs {
   int kernel;        // KernelKind
   int op;            // OpKind
@@ -31,6 +44,9 @@ struct RegularArgs {
   int out_type;      // OutType
   int64_t ld;        // leading dimension = number of test DOFs
   void* out;         // column-major output
+  int small_phase = 0;   // Helmholtz, mixed: k (max rad_test + max rad_trial) <= 0.8, so
+                         // |k (r - r0)| <= 0.8 for every far pair (no phase reduction)
+  NearArgs near{};       // mixed: near field (null: near pairs found per pair in the kernel)
   int trial_tile0 = 0;   // first trial tile of this launch
   int trial_tiles = 0;   // trial tiles of this launch (0: all from trial_tile0 on)
 };
@@ -81,8 +97,9 @@ struct SingularArgs {
   int out_type;
   int64_t ld;
   void* out;          // dense column-major output (added into), or null
-  int unique_entries; // 1 when every pair owns its entries (DP0 x DP0): plain adds
+  int unique_entries; // 1 when every pair owns its entry (DP0 x DP0): plain stores
   double* pair_values;  // if non-null: per-pair local blocks (nbt * nbs [*2 complex])
+  int fast = 0;             // mixed-precision assembly: own FP64 rsqrt / sincos (Helmholtz)
   int trial_lo = 0;         // only pairs whose trial cell lies in [trial_lo, trial_hi)
   int trial_hi = 0x7fffffff;
 };

@@ -111,7 +111,8 @@ __device__ __forceinline__ void finish_block(const Tile& T, int it, const Tile& 
 }
 
 // FP64 local block of test cell `it` (tile T) and trial cell `js` (tile S).
-template <int QT, int KER, int OP, int NBT, int NBS, bool kUnroll = true>
+// kFast (the FP64 near pairs of mixed-precision assemblies): sincos_cw for the phase.
+template <int QT, int KER, int OP, int NBT, int NBS, bool kUnroll = true, bool kFast = false>
 __device__ __forceinline__ void block_fp64(const Tile& T, int it, const Tile& S, int js,
                                         const RegularRule& rule, double k,
                                         double ore[NBT][NBS], double oim[NBT][NBS]) {
@@ -147,7 +148,10 @@ __device__ __forceinline__ void block_fp64(const Tile& T, int it, const Tile& S,
       } else {
         const double r = r2 * rinv;
         double sn, cs;
-        sincos(k * r, &sn, &cs);
+        if (kFast)
+          sincos_cw(k * r, sn, cs);
+        else
+          sincos(k * r, &sn, &cs);
         if (OP == kSL || OP == kHS) {
           const double f = wq * rinv;
           kre = f * cs;
@@ -202,14 +206,14 @@ struct FarPair {
   float m2dx, m2dy, m2dz;   // -2 dc, dc = c_x - c_y in FP32
   float fa0, fa1, fa2;      // normal-derivative factors in tangent coordinates
   float r0f, r0sq, kf;      // reference distance (Helmholtz), |dc|^2, wavenumber
-  float yx[kCap], yy[kCap], yz[kCap], yn[kCap];  // trial points relative to c_y, |.|^2
-  float wq[kCap];           // trial weights times the ADL factor
+  float wq[kCap];           // ADL: trial weights times the normal-derivative factor
 };
 
 // Sums of one far pair in FP32: blk[a][b] and S (see block_fp64 for their meaning),
 // without the reference phase e^{ik r0}.  kSmallPhase: |k (r - r0)| <= 0.8 for every
-// point pair, and the trial data sit in registers (fully unrolled inner loop); otherwise
-// the inner loop reads the trial data from shared memory and reduces the phase.
+// point pair (polynomial cos / sin, fully unrolled inner loop); otherwise the phase is
+// reduced by multiples of pi/2 first.  Test and trial points are read from shared memory
+// as float4 (offset from the centroid, squared length): one load per point.
 template <int QT, int KER, int OP, int NBT, int NBS, bool kSmallPhase>
 __device__ __forceinline__ void far_sums(const Tile& T, int it, const Tile& S, int js,
                                          const RegularRule& rule, const FarPair<QT>& fp,
@@ -222,28 +226,23 @@ __device__ __forceinline__ void far_sums(const Tile& T, int it, const Tile& S, i
   float cmp_re = 0.f, cmp_im = 0.f;
 #pragma unroll 1
   for (int p = 0; p < Q; ++p) {
-    const float ax = T.R(p, 0, it), ay = T.R(p, 1, it), az = T.R(p, 2, it);
+    const float4 a = T.R4(p, it);
     const float apf = OP == kDL ? fmaf(rule.uf[p], fp.fa1, fmaf(rule.vf[p], fp.fa2, fp.fa0)) : 1.f;
-    const float wx = fmaf(-2.f, ax, fp.m2dx), wy = fmaf(-2.f, ay, fp.m2dy),
-                wz = fmaf(-2.f, az, fp.m2dz);
-    // A_p (Laplace: plus |dc|^2, so that the sum below is r^2 itself)
-    const float Ap = fmaf(-ax, fp.m2dx, fmaf(-ay, fp.m2dy, fmaf(-az, fp.m2dz,
-                                                                T.R(p, 3, it) + (kC ? 0.f : fp.r0sq))));
+    // s_pq = A_p + |y_q|^2 + w_p . y_q; Laplace adds |dc|^2 so that it is r^2 itself
+    const float wx = fmaf(-2.f, a.x, fp.m2dx), wy = fmaf(-2.f, a.y, fp.m2dy),
+                wz = fmaf(-2.f, a.z, fp.m2dz);
+    const float Ap = fmaf(-a.x, fp.m2dx, fmaf(-a.y, fp.m2dy, fmaf(-a.z, fp.m2dz,
+                                                                  a.w + (kC ? 0.f : fp.r0sq))));
     float u_re[NBS], u_im[NBS], g_re = 0.f, g_im = 0.f;
 #pragma unroll
     for (int b = 0; b < NBS; ++b) u_re[b] = u_im[b] = 0.f;
 #pragma unroll(kSmallPhase ? 6 : 1)
     for (int q = 0; q < Q; ++q) {
-      // the general (rare) path reads the trial data from shared memory so that the
-      // per-pair register arrays are only indexed by compile-time constants
-      const float yq0 = kSmallPhase ? fp.yx[q] : S.R(q, 0, js);
-      const float yq1 = kSmallPhase ? fp.yy[q] : S.R(q, 1, js);
-      const float yq2 = kSmallPhase ? fp.yz[q] : S.R(q, 2, js);
-      const float yqn = kSmallPhase ? fp.yn[q] : S.R(q, 3, js);
+      const float4 y = S.R4(q, js);  // the same address in every lane: a broadcast
       const float wq = OP != kADL ? rule.wf[q]
                        : kSmallPhase ? fp.wq[q]
                                     : rule.wf[q] * fmaf(rule.uf[q], fp.fa1, fmaf(rule.vf[q], fp.fa2, fp.fa0));
-      const float s = fmaf(wx, yq0, fmaf(wy, yq1, fmaf(wz, yq2, Ap + yqn)));
+      const float s = fmaf(wx, y.x, fmaf(wy, y.y, fmaf(wz, y.z, Ap + y.w)));
       float kre, kim = 0.f;
       if (!kC) {
         const float rinv = rsqrt_approx(s);  // s is r^2 here
@@ -309,8 +308,13 @@ __device__ __forceinline__ void far_sums(const Tile& T, int it, const Tile& S, i
   }
 }
 
+// Phase handling of a launch (Helmholtz far pairs): kPhaseRuntime chooses per warp,
+// kPhaseSmall assumes |k (r - r0)| <= 0.8 for every pair of the launch (the host checks
+// k (max rad_x + max rad_y) <= 0.8), kPhaseGeneral reduces every phase.
+enum PhaseMode : int { kPhaseRuntime = 0, kPhaseSmall = 1, kPhaseGeneral = 2 };
+
 // FP32 local block of a far pair (see the file comment for the formulation).
-template <int QT, int KER, int OP, int NBT, int NBS>
+template <int QT, int KER, int OP, int NBT, int NBS, int PH>
 __device__ __forceinline__ void block_fp32(const Tile& T, int it, const Tile& S, int js,
                                            const RegularRule& rule, double k,
                                            double ore[NBT][NBS], double oim[NBT][NBS]) {
@@ -337,7 +341,7 @@ __device__ __forceinline__ void block_fp32(const Tile& T, int it, const Tile& S,
     fp.fa2 = static_cast<float>(S.G(fT1x, js) * nx + S.G(fT1y, js) * ny + S.G(fT1z, js) * nz);
   }
   float ph_c = 1.f, ph_s = 0.f;
-  bool small_phase = true;
+  bool small_phase = PH != kPhaseGeneral;
   fp.r0f = fp.kf = 0.f;
   fp.r0sq = fmaf(fdx, fdx, fmaf(fdy, fdy, fdz * fdz));
   if (kC) {
@@ -348,27 +352,30 @@ __device__ __forceinline__ void block_fp32(const Tile& T, int it, const Tile& S,
     fp.kf = static_cast<float>(k);
     phase_cos_sin(k * r0, ph_c, ph_s);
     // warp-uniform choice, so that a warp never runs both variants
-    small_phase = __all_sync(__activemask(), k * (T.G(fRad, it) + S.G(fRad, js)) <=
-                                                 static_cast<double>(kSmallPhaseMax));
+    if (PH == kPhaseRuntime)
+      small_phase = __all_sync(__activemask(), k * (T.G(fRad, it) + S.G(fRad, js)) <=
+                                                   static_cast<double>(kSmallPhaseMax));
   }
+  if (OP == kADL) {
 #pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    fp.yx[q] = S.R(q, 0, js);
-    fp.yy[q] = S.R(q, 1, js);
-    fp.yz[q] = S.R(q, 2, js);
-    fp.yn[q] = S.R(q, 3, js);
-    fp.wq[q] = OP == kADL ? rule.wf[q] * fmaf(rule.uf[q], fp.fa1, fmaf(rule.vf[q], fp.fa2, fp.fa0))
-                          : rule.wf[q];
+    for (int q = 0; q < Q; ++q)
+      fp.wq[q] = rule.wf[q] * fmaf(rule.uf[q], fp.fa1, fmaf(rule.vf[q], fp.fa2, fp.fa0));
   }
   float blk_re[NBT][NBS], blk_im[NBT][NBS], S_re = 0.f, S_im = 0.f;
 #pragma unroll
   for (int a = 0; a < NBT; ++a)
 #pragma unroll
     for (int b = 0; b < NBS; ++b) blk_re[a][b] = blk_im[a][b] = 0.f;
-  if (small_phase)
+  if (!kC || PH == kPhaseSmall) {
     far_sums<QT, KER, OP, NBT, NBS, true>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
-  else
+  } else if (PH == kPhaseGeneral) {
     far_sums<QT, KER, OP, NBT, NBS, false>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
+  } else {
+    if (small_phase)
+      far_sums<QT, KER, OP, NBT, NBS, true>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
+    else
+      far_sums<QT, KER, OP, NBT, NBS, false>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
+  }
   // back to FP64, applying the reference phase e^{ik r0}
   double bre[NBT][NBS], bim[NBT][NBS];
   double Sre = S_re, Sim = S_im;
@@ -417,14 +424,35 @@ __device__ __forceinline__ void deposit(double* acc_re, double* acc_im, int ndt,
   }
 }
 
-template <int QT, int KER, int OP, int NBT, int NBS, bool MIXED, bool DIRECT>
+// Near-pair handling of a launch.  kNearInKernel: every pair is tested in the kernel and
+// near pairs are queued in shared memory and integrated in FP64 after the main loop (the
+// FP64 kernels skip the test); kNearMasked: the pairs marked in the near-field masks are
+// skipped (FP32 far pairs only); kNearList: one CTA per masked tile pair integrates its
+// marked, non-vertex-sharing pairs in FP64.
+enum NearMode : int { kNearInKernel = 0, kNearMasked = 1, kNearList = 2 };
+
+template <int QT, int KER, int OP, int NBT, int NBS, bool MIXED, bool DIRECT, int PH, int NM>
 __global__ void __launch_bounds__(kThreads, 4)
     regular_tiles(CellSet test, SpaceTiles tt, CellSet trial, SpaceTiles st, RegularRule rule,
-                  double k, int same_grid, double* __restrict__ out, int64_t ld, int tile_y0) {
+                  double k, int same_grid, double* __restrict__ out, int64_t ld, int tile_y0,
+                  int tile_y1, NearArgs near) {
   constexpr bool kC = KER == kHelmholtz;
+  constexpr bool kQueue = MIXED && NM == kNearInKernel;
+  constexpr bool kRel = MIXED && NM != kNearList;  // FP32 offsets staged
   const int Q = QT > 0 ? QT : rule.npts;
-  const int sy = blockIdx.y + tile_y0;  // trial tile
-  const int ti0 = blockIdx.x * kTile, sj0 = sy * kTile;
+  int tx, sy, moff = -1;
+  if (NM == kNearList) {
+    const int2 e = near.list[blockIdx.x];
+    tx = e.x / near.trial_tiles;
+    sy = e.x - tx * near.trial_tiles;
+    moff = e.y;
+    if (sy < tile_y0 || sy >= tile_y1) return;  // a tile pair of another chunk (whole CTA)
+  } else {
+    tx = blockIdx.x;
+    sy = blockIdx.y + tile_y0;
+    if (NM == kNearMasked) moff = __ldg(near.tile_mask + static_cast<int64_t>(tx) * near.trial_tiles + sy);
+  }
+  const int ti0 = tx * kTile, sj0 = sy * kTile;
   const int nti = min(kTile, test.ncells - ti0), nsj = min(kTile, trial.ncells - sj0);
 
   extern __shared__ __align__(16) unsigned char smem[];
@@ -433,8 +461,8 @@ __global__ void __launch_bounds__(kThreads, 4)
   double* acc_im = nullptr;
   int ndt = 0, nds = 0, tdof0 = 0, sdof0 = 0;
   if (!DIRECT) {
-    tdof0 = tt.tile_dof_off[blockIdx.x];
-    ndt = tt.tile_dof_off[blockIdx.x + 1] - tdof0;
+    tdof0 = tt.tile_dof_off[tx];
+    ndt = tt.tile_dof_off[tx + 1] - tdof0;
     sdof0 = st.tile_dof_off[sy];
     nds = st.tile_dof_off[sy + 1] - sdof0;
     const int cap = tt.max_tile_dofs * st.max_tile_dofs;
@@ -442,9 +470,9 @@ __global__ void __launch_bounds__(kThreads, 4)
     acc_im = acc_re + cap;
     cursor += sizeof(double) * cap * (kC ? 2 : 1);
   }
-  const Tile T = carve_tile(cursor, Q, MIXED, NBT);
-  const Tile S = carve_tile(cursor, Q, MIXED, NBS);
-  unsigned short* queue = reinterpret_cast<unsigned short*>(cursor);  // MIXED: near pairs
+  const Tile T = carve_tile(cursor, Q, kRel, NBT);
+  const Tile S = carve_tile(cursor, Q, kRel, NBS);
+  unsigned short* queue = reinterpret_cast<unsigned short*>(cursor);  // kQueue: near pairs
   int* qcount = reinterpret_cast<int*>(cursor + sizeof(unsigned short) * kTile * kTile);
 
   if (!DIRECT)
@@ -452,37 +480,53 @@ __global__ void __launch_bounds__(kThreads, 4)
       acc_re[idx] = 0.0;
       if (kC) acc_im[idx] = 0.0;
     }
-  if (MIXED && threadIdx.x == 0) *qcount = 0;
-  load_tile(T, test, ti0, nti, Q, MIXED, DIRECT ? nullptr : tt.cell_ldof, NBT);
-  load_tile(S, trial, sj0, nsj, Q, MIXED, DIRECT ? nullptr : st.cell_ldof, NBS);
+  if (kQueue && threadIdx.x == 0) *qcount = 0;
+  load_tile(T, test, ti0, nti, Q, kRel, DIRECT ? nullptr : tt.cell_ldof, NBT);
+  load_tile(S, trial, sj0, nsj, Q, kRel, DIRECT ? nullptr : st.cell_ldof, NBS);
   __syncthreads();
 
   const int it = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (it < nti) {
     const int a0 = T.vid[it], a1 = T.vid[kTile + it], a2 = T.vid[2 * kTile + it];
+    const unsigned mword = (NM != kNearInKernel && moff >= 0)
+                               ? __ldg(near.masks + static_cast<int64_t>(moff) * kTile + it)
+                               : 0u;
     for (int js = warp; js < nsj; js += kWarps) {
-      const bool adjacent = same_grid && share_vertex(a0, a1, a2, S.vid[js], S.vid[kTile + js],
-                                                      S.vid[2 * kTile + js]);
       const int64_t o = static_cast<int64_t>(sj0 + js) * ld + ti0 + it;
-      if (adjacent) {
-        if (DIRECT) {
-          if (kC)
-            reinterpret_cast<double2*>(out)[o] = make_double2(0.0, 0.0);
-          else
-            out[o] = 0.0;
-        }
-        continue;
-      }
+      const bool marked = (mword >> js) & 1u;
       double ore[NBT][NBS], oim[NBT][NBS];
-      if (MIXED) {
-        if (near_pair(T, it, S, js)) {
-          const int slot = atomicAdd(qcount, 1);
-          queue[slot] = static_cast<unsigned short>(it | (js << 8));
+      if (NM == kNearList) {
+        if (!marked) continue;
+        if (same_grid && share_vertex(a0, a1, a2, S.vid[js], S.vid[kTile + js], S.vid[2 * kTile + js]))
+          continue;  // vertex-sharing: the singular kernel's
+        block_fp64<QT, KER, OP, NBT, NBS, false, true>(T, it, S, js, rule, k, ore, oim);
+      } else {
+        const bool skip = NM == kNearMasked
+                              ? marked
+                              : same_grid && share_vertex(a0, a1, a2, S.vid[js], S.vid[kTile + js],
+                                                          S.vid[2 * kTile + js]);
+        if (skip) {
+          // DP0: a vertex-sharing entry is written here (zero) and then by the singular
+          // kernel; the masked entries of the mixed path are written by the near-list and
+          // singular kernels alone (which may run concurrently with this one)
+          if (DIRECT && NM == kNearInKernel) {
+            if (kC)
+              reinterpret_cast<double2*>(out)[o] = make_double2(0.0, 0.0);
+            else
+              out[o] = 0.0;
+          }
           continue;
         }
-        block_fp32<QT, KER, OP, NBT, NBS>(T, it, S, js, rule, k, ore, oim);
-      } else {
-        block_fp64<QT, KER, OP, NBT, NBS>(T, it, S, js, rule, k, ore, oim);
+        if (MIXED) {
+          if (kQueue && near_pair(T, it, S, js)) {
+            const int slot = atomicAdd(qcount, 1);
+            queue[slot] = static_cast<unsigned short>(it | (js << 8));
+            continue;
+          }
+          block_fp32<QT, KER, OP, NBT, NBS, PH>(T, it, S, js, rule, k, ore, oim);
+        } else {
+          block_fp64<QT, KER, OP, NBT, NBS>(T, it, S, js, rule, k, ore, oim);
+        }
       }
       if (DIRECT) {
         if (kC)
@@ -494,7 +538,7 @@ __global__ void __launch_bounds__(kThreads, 4)
       }
     }
   }
-  if (MIXED) {
+  if (kQueue) {
     __syncthreads();
     const int nq = *qcount;
     for (int e = threadIdx.x; e < nq; e += kThreads) {
@@ -666,7 +710,7 @@ __global__ void __launch_bounds__(kThreads)
               near_pair(T, it, S, js))
             continue;
           double ore[1][1], oim[1][1];
-          block_fp32<6, kHelmholtz, kSL, 1, 1>(T, it, S, js, rule, k, ore, oim);
+          block_fp32<6, kHelmholtz, kSL, 1, 1, kPhaseRuntime>(T, it, S, js, rule, k, ore, oim);
           out[static_cast<long long>(sj0 + js) * nc + ti0 + it] =
               make_float2(static_cast<float>(ore[0][0]), static_cast<float>(oim[0][0]));
         }
@@ -691,39 +735,82 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-size_t smem_bytes(int q, bool mixed, bool direct, bool cplx, int max_t, int max_s, int nbt,
-                  int nbs) {
+size_t smem_bytes(int q, bool rel, bool queue, bool direct, bool cplx, int max_t, int max_s,
+                  int nbt, int nbs) {
   size_t b = 0;
   if (!direct) b += sizeof(double) * static_cast<size_t>(max_t) * max_s * (cplx ? 2 : 1);
   for (int nb : {nbt, nbs}) {
-    b += sizeof(double) * tile_doubles(q) + sizeof(float) * tile_floats(q, mixed) +
+    b = (b + 15) & ~size_t(15);
+    b += sizeof(double) * tile_doubles(q) + sizeof(float) * tile_floats(q, rel) +
          sizeof(int) * tile_ints(nb);
     b = (b + 15) & ~size_t(15);
   }
-  if (mixed) b += sizeof(unsigned short) * kTile * kTile + sizeof(int);
+  if (queue) b += sizeof(unsigned short) * kTile * kTile + sizeof(int);
   return b + 16;
+}
+
+template <int QT, int KER, int OP, int NBT, int NBS, bool MIXED, bool DIRECT, int PH, int NM>
+cudaError_t launch_mode(const CellSet& test, const SpaceTiles& tt, const CellSet& trial,
+                        const SpaceTiles& st, const RegularRule& rule, const RegularArgs& a,
+                        int ty0, int ty1, cudaStream_t stream) {
+  const size_t smem = smem_bytes(rule.npts, MIXED && NM != kNearList, MIXED && NM == kNearInKernel,
+                                 DIRECT, KER == kHelmholtz, tt.max_tile_dofs, st.max_tile_dofs,
+                                 NBT, NBS);
+  auto fn = regular_tiles<QT, KER, OP, NBT, NBS, MIXED, DIRECT, PH, NM>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  dim3 grid;
+  if (NM == kNearList) {
+    if (a.near.nlist <= 0) return cudaSuccess;
+    grid = dim3(a.near.nlist);
+  } else {
+    grid = dim3((test.ncells + kTile - 1) / kTile, ty1 - ty0);
+  }
+  fn<<<grid, kThreads, smem, stream>>>(test, tt, trial, st, rule, a.k, a.same_grid,
+                                       static_cast<double*>(a.out), a.ld, ty0, ty1, a.near);
+  return cudaGetLastError();
 }
 
 template <int QT, int KER, int OP, int NBT, int NBS, bool MIXED, bool DIRECT>
 cudaError_t launch_one(const CellSet& test, const SpaceTiles& tt, const CellSet& trial,
                        const SpaceTiles& st, const RegularRule& rule, const RegularArgs& a,
                        cudaStream_t stream) {
-  const size_t smem = smem_bytes(rule.npts, MIXED, DIRECT, KER == kHelmholtz, tt.max_tile_dofs,
-                                 st.max_tile_dofs, NBT, NBS);
-  auto fn = regular_tiles<QT, KER, OP, NBT, NBS, MIXED, DIRECT>;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
-  if (e != cudaSuccess) return e;
   const int trial_tiles = (trial.ncells + kTile - 1) / kTile;
   if (a.trial_tile0 < 0 || a.trial_tile0 > trial_tiles || a.trial_tiles < 0)
     return cudaErrorInvalidValue;
   const int ny = a.trial_tiles > 0 ? std::min(a.trial_tiles, trial_tiles - a.trial_tile0)
                                    : trial_tiles - a.trial_tile0;
   if (ny <= 0) return cudaSuccess;
-  dim3 grid((test.ncells + kTile - 1) / kTile, ny);
-  fn<<<grid, kThreads, smem, stream>>>(test, tt, trial, st, rule, a.k, a.same_grid,
-                                       static_cast<double*>(a.out), a.ld, a.trial_tile0);
-  return cudaGetLastError();
+  const int ty0 = a.trial_tile0, ty1 = a.trial_tile0 + ny;
+  if constexpr (!MIXED) {
+    return launch_mode<QT, KER, OP, NBT, NBS, false, DIRECT, kPhaseSmall, kNearInKernel>(
+        test, tt, trial, st, rule, a, ty0, ty1, stream);
+  } else {
+    if (!a.near.tile_mask) {
+      // no near field: pairs tested in the kernel (DP0 only; the assembler always builds one)
+      if constexpr (DIRECT) {
+        if (KER == kHelmholtz && !a.small_phase)
+          return launch_mode<QT, KER, OP, NBT, NBS, true, DIRECT, kPhaseGeneral, kNearInKernel>(
+              test, tt, trial, st, rule, a, ty0, ty1, stream);
+        return launch_mode<QT, KER, OP, NBT, NBS, true, DIRECT, kPhaseSmall, kNearInKernel>(
+            test, tt, trial, st, rule, a, ty0, ty1, stream);
+      } else {
+        return cudaErrorInvalidValue;
+      }
+    }
+    if (a.near.trial_tiles != trial_tiles) return cudaErrorInvalidValue;
+    cudaError_t e;
+    if (KER == kHelmholtz && !a.small_phase)
+      e = launch_mode<QT, KER, OP, NBT, NBS, true, DIRECT, kPhaseGeneral, kNearMasked>(
+          test, tt, trial, st, rule, a, ty0, ty1, stream);
+    else
+      e = launch_mode<QT, KER, OP, NBT, NBS, true, DIRECT, kPhaseSmall, kNearMasked>(
+          test, tt, trial, st, rule, a, ty0, ty1, stream);
+    if (e != cudaSuccess) return e;
+    return launch_mode<QT, KER, OP, NBT, NBS, true, DIRECT, kPhaseSmall, kNearList>(
+        test, tt, trial, st, rule, a, ty0, ty1, stream);
+  }
 }
 
 template <int QT, int KER, int OP, bool MIXED>

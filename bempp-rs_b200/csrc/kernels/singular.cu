@@ -31,7 +31,7 @@ __device__ __forceinline__ void load_cell(const CellSet& cs, int c, CellData& d)
   d.jdet = g(cs.geom, kJdet, n, c);
 }
 
-template <int KER, int OP, int NBT, int NBS>
+template <int KER, int OP, int NBT, int NBS, bool FAST>
 __global__ void __launch_bounds__(kThreads)
     singular_fp64(CellSet test, const int* __restrict__ tdofs, CellSet trial,
                   const int* __restrict__ sdofs, SingularRules rules, SingularPairs pairs,
@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(kThreads)
     for (int c = 0; c < 3; ++c)
       d[c] = (x.v0[c] + xi0 * x.t0[c] + xi1 * x.t1[c]) - (y.v0[c] + et0 * y.t0[c] + et1 * y.t1[c]);
     const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-    const double rinv = rsqrt(r2);
+    const double rinv = FAST ? rsqrt_refined(r2) : rsqrt(r2);
     double kre, kim = 0.0;  // w * (kernel factor), see the regular kernels
     if (KER == kLaplace) {
       if (OP == kSL || OP == kHS) {
@@ -79,7 +79,10 @@ __global__ void __launch_bounds__(kThreads)
     } else {
       const double r = r2 * rinv;
       double sn, cs;
-      sincos(k * r, &sn, &cs);
+      if (FAST)
+        sincos_cw(k * r, sn, cs);
+      else
+        sincos(k * r, &sn, &cs);
       if (OP == kSL || OP == kHS) {
         kre = w * rinv * cs;
         kim = w * rinv * sn;
@@ -195,12 +198,11 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
       for (int a = 0; a < NBT; ++a) {
         const int64_t o = col + __ldg(tdofs + tc * NBT + a);
-        if (unique_entries) {
+        if (unique_entries) {  // DP0 x DP0: this pair owns the entry
           if (kCplx) {
-            out[2 * o] += o_re[a][b];
-            out[2 * o + 1] += o_im[a][b];
+            reinterpret_cast<double2*>(out)[o] = make_double2(o_re[a][b], o_im[a][b]);
           } else {
-            out[o] += o_re[a][b];
+            out[o] = o_re[a][b];
           }
         } else {
           if (kCplx) {
@@ -221,7 +223,10 @@ cudaError_t launch_one(const CellSet& test, const int* tdofs, const CellSet& tri
                        const SingularArgs& a, cudaStream_t stream) {
   const int warps = kThreads / 32;
   const int blocks = (pairs.npairs + warps - 1) / warps;
-  singular_fp64<KER, OP, NBT, NBS><<<blocks, kThreads, 0, stream>>>(
+  // FAST: the refined hardware rsqrt and sincos_cw (mixed-precision assemblies; Helmholtz)
+  auto fn = (a.fast && KER == kHelmholtz) ? singular_fp64<KER, OP, NBT, NBS, true>
+                                          : singular_fp64<KER, OP, NBT, NBS, false>;
+  fn<<<blocks, kThreads, 0, stream>>>(
       test, tdofs, trial, sdofs, rules, pairs, a.k, static_cast<double*>(a.out), a.ld,
       a.unique_entries, a.pair_values, a.trial_lo, a.trial_hi);
   return cudaGetLastError();

@@ -20,13 +20,16 @@ enum TileField : int {
 // Shared-memory image of a tile of kTile cells.
 struct Tile {
   double* pts;  // [(q*3+d) * kTile + c] absolute FP64 points
-  float* rel;   // [(q*4+d) * kTile + c] FP32 offsets from the centroid, d = 3: their
-                //   squared length (mixed only)
+  float4* rel;  // [q * kTile + c] FP32 offset from the centroid (x, y, z) and its
+                //   squared length (w) (mixed only)
   double* geo;  // [f * kTile + c]
   int* vid;     // [v * kTile + c]
   int* ldof;    // [b * kTile + c]
   __device__ __forceinline__ double P(int q, int d, int c) const { return pts[(q * 3 + d) * kTile + c]; }
-  __device__ __forceinline__ float R(int q, int d, int c) const { return rel[(q * 4 + d) * kTile + c]; }
+  __device__ __forceinline__ float4 R4(int q, int c) const { return rel[q * kTile + c]; }
+  __device__ __forceinline__ float R(int q, int d, int c) const {
+    return reinterpret_cast<const float*>(rel + q * kTile + c)[d];
+  }
   __device__ __forceinline__ double G(int f, int c) const { return geo[f * kTile + c]; }
 };
 
@@ -34,13 +37,14 @@ __host__ __device__ inline size_t tile_doubles(int q) { return (3 * q + kTileFie
 __host__ __device__ inline size_t tile_floats(int q, bool mixed) { return mixed ? 4 * q * kTile : 0; }
 __host__ __device__ inline size_t tile_ints(int nb) { return (3 + nb) * kTile; }
 
-// Carves a tile out of shared memory starting at *cursor (8-byte aligned).
+// Carves a tile out of shared memory at *cursor rounded up to 16 bytes.
 __device__ inline Tile carve_tile(unsigned char*& cursor, int q, bool mixed, int nb) {
   Tile t;
+  cursor = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(cursor) + 15) & ~uintptr_t(15));
   t.pts = reinterpret_cast<double*>(cursor);
   t.geo = t.pts + 3 * q * kTile;
-  cursor = reinterpret_cast<unsigned char*>(t.geo + kTileFields * kTile);
-  t.rel = reinterpret_cast<float*>(cursor);
+  cursor = reinterpret_cast<unsigned char*>(t.geo + kTileFields * kTile);  // 16-B multiple
+  t.rel = reinterpret_cast<float4*>(cursor);
   cursor += sizeof(float) * tile_floats(q, mixed);
   t.vid = reinterpret_cast<int*>(cursor);
   t.ldof = t.vid + 3 * kTile;
@@ -61,11 +65,7 @@ __device__ inline void load_tile(const Tile& t, const CellSet& cs, int c0, int n
       const int c = idx % kTile, p = idx / kTile;
       const float* src = cs.qrel + static_cast<int64_t>(3 * p) * N + c0 + min(c, n - 1);
       const float x = __ldg(src), y = __ldg(src + N), z = __ldg(src + 2 * N);
-      float* dst = t.rel + 4 * p * kTile + c;
-      dst[0] = x;
-      dst[kTile] = y;
-      dst[2 * kTile] = z;
-      dst[3 * kTile] = fmaf(x, x, fmaf(y, y, z * z));
+      t.rel[p * kTile + c] = make_float4(x, y, z, fmaf(x, x, fmaf(y, y, z * z)));
     }
   for (int c = threadIdx.x; c < kTile; c += kThreads) {
     const int cell = c0 + min(c, n - 1);

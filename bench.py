@@ -305,9 +305,42 @@ def north_star(args):
     res["speedup_mixed_vs_fp64"] = res["fp64"]["ms_per_assembly"] / res["mixed"]["ms_per_assembly"]
     res["mixed_rel_frobenius_error_vs_fp64"] = err
     res["workload"] = w["name"]
+    # the output is written once: 16 B per entry
+    res["mixed_hbm_write_gbs"] = (16 * w_entries(w) / (res["mixed"]["regular_ms"] * 1e-3) / 1e9
+                                  if res["mixed"]["regular_ms"] else None)
     del outs
     torch.cuda.empty_cache()
+    res["helmholtz_p1_operators"] = helmholtz_p1_ops(args)
     return res
+
+
+def w_entries(w):
+    pts, cells = workload_mesh(w)
+    return len(cells) ** 2
+
+
+def helmholtz_p1_ops(args):
+    """Helmholtz DL, ADL and HS (k = 8, P1 x P1, c128) on the 20,480-triangle perturbed
+    sphere: FP64 vs mixed assembly time and the mixed result's error against FP64."""
+    import torch
+
+    w = dict(WORKLOADS["helmholtz_sl"])
+    w.update(space="p1", ops=["double_layer", "adjoint_double_layer", "hypersingular"])
+    out = {}
+    wls = {prec: Workload(w, prec) for prec in ("fp64", "mixed")}
+    for prec, wl in wls.items():
+        wl.timed(1, 2)
+        out[prec] = {name: ph[2] for name, ph in wl.phase_ms().items()}  # regular ms
+        step_ms, _ = wl.timed(max(2, args.steps // 2), 1)
+        out[prec]["ms_per_step"] = step_ms
+    out["rel_frobenius_error_vs_fp64"] = {
+        name: (torch.linalg.norm(a - b) / torch.linalg.norm(b)).item()
+        for name, a, b in zip(w["ops"], wls["mixed"].outs, wls["fp64"].outs)}
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    out["workload"] = "helmholtz_dl_adl_hs_p1_ico5_k8_c128"
+    del wls
+    torch.cuda.empty_cache()
+    return out
 
 
 def adjoint_timing(args):
