@@ -289,13 +289,15 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
     const NearField& nf = near_field(*test.grid, *trial.grid);
     ra.near.tile_mask = nf.tile_mask.as<int>();
     ra.near.masks = nf.masks.as<unsigned>();
-    ra.near.list = nf.list.as<int2>();
-    ra.near.nlist = nf.nlist;
+    ra.near.pairs = nf.pairs.as<int2>();
+    ra.near.npairs = nf.npairs;
     ra.near.trial_tiles = nf.trial_tiles;
+    ra.near.test_dofs = test.d_dofs.as<int>();
+    ra.near.trial_dofs = trial.d_dofs.as<int>();
   }
   const CellSet tcs = cell_set(*test.grid, tgeo), scs = cell_set(*trial.grid, sgeo);
   // mixed: the FP32 far-pair launch and the FP64 near-pair launch
-  const size_t regular_launches = ra.near.nlist > 0 ? 2 : 1;
+  const size_t regular_launches = ra.near.npairs > 0 ? 2 : 1;
 
   const bool empty = nt == 0 || ns == 0;
   const bool singular = same_grid && !empty;

@@ -113,9 +113,9 @@ struct GridGeometry {  // device geometry for one regular rule
 // Near field of a (test grid, trial grid) pair for the mixed-precision kernels (near.cpp):
 // the device arrays behind NearArgs.
 struct NearField {
-  int test_tiles = 0, trial_tiles = 0, nlist = 0;
-  DeviceBuffer tile_mask, masks, list;
-  size_t near_pairs = 0;  // marked pairs (near or vertex-sharing)
+  int test_tiles = 0, trial_tiles = 0, npairs = 0;
+  DeviceBuffer tile_mask, masks, pairs;
+  size_t marked = 0;  // marked pairs (near or vertex-sharing)
 };
 
 // Per chunk of a chunked assembly: runs (first column, number of columns).

@@ -6,9 +6,9 @@
 // get a bounding sphere, only tile pairs whose spheres come within twice the largest cell
 // diameter are examined cell by cell, and each such tile pair gets a 32 x 32 bit mask
 // (one word per test cell) of its near and vertex-sharing pairs.  The FP32 kernel skips
-// the marked pairs; a second launch over the list of masked tile pairs integrates the
-// marked pairs that do not share a vertex in FP64 (vertex-sharing pairs belong to the
-// singular kernel).
+// the marked pairs; a second launch integrates the list of near pairs that share no
+// vertex in FP64, one thread per pair (vertex-sharing pairs belong to the singular
+// kernel).
 #include <algorithm>
 #include <cmath>
 
@@ -90,8 +90,9 @@ const NearField& near_field(GridT& test, GridT& trial) {
 
   std::vector<int> tile_mask(static_cast<size_t>(ntt) * nst, -1);
   std::vector<unsigned> masks;
-  std::vector<int2> list;
+  std::vector<int2> pairs;
   size_t marked = 0;
+  int nmasks = 0;
   for (int a = 0; a < ntt; ++a)
     for (int b = 0; b < nst; ++b) {
       const TileBall &A = tt[a], &B = st[b];
@@ -108,31 +109,29 @@ const NearField& near_field(GridT& test, GridT& trial) {
           const CellBall &x = tc[i0 + i], &y = sc[j0 + j];
           const double ex = x.c[0] - y.c[0], ey = x.c[1] - y.c[1], ez = x.c[2] - y.c[2];
           const double lim = 2.0 * std::max(x.diam, y.diam);
-          const bool near = ex * ex + ey * ey + ez * ez < lim * lim ||
-                            (same && share_vertex(test, i0 + i, trial, j0 + j));
-          if (near) {
+          const bool adjacent = same && share_vertex(test, i0 + i, trial, j0 + j);
+          const bool near = ex * ex + ey * ey + ez * ez < lim * lim;
+          if (near || adjacent) {
             words[i] |= 1u << j;
             any = true;
             ++marked;
+            if (!adjacent)
+              pairs.push_back(make_int2(static_cast<int>(i0 + i), static_cast<int>(j0 + j)));
           }
         }
       if (!any) continue;
-      const int m = static_cast<int>(list.size());
-      tile_mask[static_cast<size_t>(a) * nst + b] = m;
-      list.push_back(make_int2(a * nst + b, m));
+      tile_mask[static_cast<size_t>(a) * nst + b] = nmasks++;
       masks.insert(masks.end(), words, words + kTileCells);
     }
 
   auto nf = std::make_unique<NearField>();
   nf->test_tiles = ntt;
   nf->trial_tiles = nst;
-  nf->nlist = static_cast<int>(list.size());
-  nf->near_pairs = marked;
+  nf->npairs = static_cast<int>(pairs.size());
+  nf->marked = marked;
   nf->tile_mask.upload(tile_mask);
-  if (!masks.empty()) {
-    nf->masks.upload(masks);
-    nf->list.upload(list);
-  }
+  if (!masks.empty()) nf->masks.upload(masks);
+  if (!pairs.empty()) nf->pairs.upload(pairs);
   slot = std::move(nf);
   return *slot;
 }

@@ -25,14 +25,16 @@ enum OutType : int { kOutF64 = 0, kOutC128 = 1, kOutF32 = 2, kOutC64 = 3 };
 // Near field of a (test grid, trial grid) pair for the mixed-precision kernels, built on
 // the host: per tile pair (test tile * trial tiles + trial tile) the index of its 32-word
 // mask or -1; mask word [m * 32 + test lane] has bit j set when the pair (test lane, trial
-// cell j) is near (centroid distance < 2 max diameter) or shares a vertex.  `list` holds
-// (tile pair, m) for every tile pair with a mask.
+// cell j) is near (centroid distance < 2 max diameter) or shares a vertex.  `pairs` lists
+// the near pairs that share no vertex as (test cell, trial cell).
 struct NearArgs {
   const int* tile_mask = nullptr;
   const unsigned* masks = nullptr;
-  const int2* list = nullptr;
-  int nlist = 0;
+  const int2* pairs = nullptr;
+  int npairs = 0;
   int trial_tiles = 0;
+  const int* test_dofs = nullptr;   // cell DOFs (scatter outputs)
+  const int* trial_dofs = nullptr;
 };
 
 struct RegularArgs {

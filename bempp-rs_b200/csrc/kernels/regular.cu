@@ -427,31 +427,27 @@ __device__ __forceinline__ void deposit(double* acc_re, double* acc_im, int ndt,
 // Near-pair handling of a launch.  kNearInKernel: every pair is tested in the kernel and
 // near pairs are queued in shared memory and integrated in FP64 after the main loop (the
 // FP64 kernels skip the test); kNearMasked: the pairs marked in the near-field masks are
-// skipped (FP32 far pairs only); kNearList: one CTA per masked tile pair integrates its
-// marked, non-vertex-sharing pairs in FP64.
-enum NearMode : int { kNearInKernel = 0, kNearMasked = 1, kNearList = 2 };
+// skipped (FP32 far pairs only; near_pairs_fp64 integrates the near ones).
+enum NearMode : int { kNearInKernel = 0, kNearMasked = 1 };
+
+// Resident CTAs per SM the register allocation must allow: 5 for the FP64 Laplace
+// hypersingular kernel (it fits in 96 registers without spills), 4 elsewhere.
+template <int KER, int OP, bool MIXED>
+constexpr int min_ctas() { return (KER == kLaplace && OP == kHS && !MIXED) ? 5 : 4; }
 
 template <int QT, int KER, int OP, int NBT, int NBS, bool MIXED, bool DIRECT, int PH, int NM>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
     regular_tiles(CellSet test, SpaceTiles tt, CellSet trial, SpaceTiles st, RegularRule rule,
                   double k, int same_grid, double* __restrict__ out, int64_t ld, int tile_y0,
                   int tile_y1, NearArgs near) {
   constexpr bool kC = KER == kHelmholtz;
   constexpr bool kQueue = MIXED && NM == kNearInKernel;
-  constexpr bool kRel = MIXED && NM != kNearList;  // FP32 offsets staged
+  constexpr bool kRel = MIXED;  // FP32 offsets staged
   const int Q = QT > 0 ? QT : rule.npts;
-  int tx, sy, moff = -1;
-  if (NM == kNearList) {
-    const int2 e = near.list[blockIdx.x];
-    tx = e.x / near.trial_tiles;
-    sy = e.x - tx * near.trial_tiles;
-    moff = e.y;
-    if (sy < tile_y0 || sy >= tile_y1) return;  // a tile pair of another chunk (whole CTA)
-  } else {
-    tx = blockIdx.x;
-    sy = blockIdx.y + tile_y0;
-    if (NM == kNearMasked) moff = __ldg(near.tile_mask + static_cast<int64_t>(tx) * near.trial_tiles + sy);
-  }
+  const int tx = blockIdx.x, sy = blockIdx.y + tile_y0;
+  const int moff = NM == kNearMasked
+                       ? __ldg(near.tile_mask + static_cast<int64_t>(tx) * near.trial_tiles + sy)
+                       : -1;
   const int ti0 = tx * kTile, sj0 = sy * kTile;
   const int nti = min(kTile, test.ncells - ti0), nsj = min(kTile, trial.ncells - sj0);
 
@@ -495,38 +491,31 @@ __global__ void __launch_bounds__(kThreads, 4)
       const int64_t o = static_cast<int64_t>(sj0 + js) * ld + ti0 + it;
       const bool marked = (mword >> js) & 1u;
       double ore[NBT][NBS], oim[NBT][NBS];
-      if (NM == kNearList) {
-        if (!marked) continue;
-        if (same_grid && share_vertex(a0, a1, a2, S.vid[js], S.vid[kTile + js], S.vid[2 * kTile + js]))
-          continue;  // vertex-sharing: the singular kernel's
-        block_fp64<QT, KER, OP, NBT, NBS, false, true>(T, it, S, js, rule, k, ore, oim);
-      } else {
-        const bool skip = NM == kNearMasked
-                              ? marked
-                              : same_grid && share_vertex(a0, a1, a2, S.vid[js], S.vid[kTile + js],
-                                                          S.vid[2 * kTile + js]);
-        if (skip) {
-          // DP0: a vertex-sharing entry is written here (zero) and then by the singular
-          // kernel; the masked entries of the mixed path are written by the near-list and
-          // singular kernels alone (which may run concurrently with this one)
-          if (DIRECT && NM == kNearInKernel) {
-            if (kC)
-              reinterpret_cast<double2*>(out)[o] = make_double2(0.0, 0.0);
-            else
-              out[o] = 0.0;
-          }
+      const bool skip = NM == kNearMasked
+                            ? marked
+                            : same_grid && share_vertex(a0, a1, a2, S.vid[js], S.vid[kTile + js],
+                                                        S.vid[2 * kTile + js]);
+      if (skip) {
+        // DP0: a vertex-sharing entry is written here (zero) and then by the singular
+        // kernel; the masked entries of the mixed path are written by the near-pair and
+        // singular kernels alone (which may run concurrently with this one)
+        if (DIRECT && NM == kNearInKernel) {
+          if (kC)
+            reinterpret_cast<double2*>(out)[o] = make_double2(0.0, 0.0);
+          else
+            out[o] = 0.0;
+        }
+        continue;
+      }
+      if (MIXED) {
+        if (kQueue && near_pair(T, it, S, js)) {
+          const int slot = atomicAdd(qcount, 1);
+          queue[slot] = static_cast<unsigned short>(it | (js << 8));
           continue;
         }
-        if (MIXED) {
-          if (kQueue && near_pair(T, it, S, js)) {
-            const int slot = atomicAdd(qcount, 1);
-            queue[slot] = static_cast<unsigned short>(it | (js << 8));
-            continue;
-          }
-          block_fp32<QT, KER, OP, NBT, NBS, PH>(T, it, S, js, rule, k, ore, oim);
-        } else {
-          block_fp64<QT, KER, OP, NBT, NBS>(T, it, S, js, rule, k, ore, oim);
-        }
+        block_fp32<QT, KER, OP, NBT, NBS, PH>(T, it, S, js, rule, k, ore, oim);
+      } else {
+        block_fp64<QT, KER, OP, NBT, NBS>(T, it, S, js, rule, k, ore, oim);
       }
       if (DIRECT) {
         if (kC)
@@ -572,6 +561,55 @@ __global__ void __launch_bounds__(kThreads, 4)
         }
       } else if (re != 0.0) {
         atomicAdd(out + o, re);
+      }
+    }
+  }
+}
+
+// FP64 near pairs of a mixed-precision assembly: one thread per pair of the near list
+// (test cell, trial cell), each staging its two cells into its own column of a per-warp
+// pair of shared-memory tiles and integrating them with block_fp64 (own sincos).
+// Only pairs whose trial cell lies in [trial_lo, trial_hi) (a chunk) are done.  DP0 x DP0
+// entries are stored; other spaces add into the output with atomics.
+template <int QT, int KER, int OP, int NBT, int NBS, bool DIRECT>
+__global__ void __launch_bounds__(kThreads)
+    near_pairs_fp64(CellSet test, CellSet trial, RegularRule rule, double k, NearArgs near,
+                    double* __restrict__ out, int64_t ld, int trial_lo, int trial_hi) {
+  constexpr bool kC = KER == kHelmholtz;
+  const int Q = QT > 0 ? QT : rule.npts;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;  // blockDim.x = 32 x warps
+  unsigned char* cursor = smem + static_cast<size_t>(warp) * 2 *
+                                     (sizeof(double) * tile_doubles(Q) + sizeof(int) * tile_ints(1) + 16);
+  const Tile T = carve_tile(cursor, Q, false, 1);
+  const Tile S = carve_tile(cursor, Q, false, 1);
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= near.npairs) return;
+  const int2 pr = __ldg(near.pairs + e);
+  if (pr.y < trial_lo || pr.y >= trial_hi) return;
+  stage_cell(T, lane, test, pr.x, Q);  // this lane's column only: no synchronisation
+  stage_cell(S, lane, trial, pr.y, Q);
+  double ore[NBT][NBS], oim[NBT][NBS];
+  block_fp64<QT, KER, OP, NBT, NBS, false, true>(T, lane, S, lane, rule, k, ore, oim);
+  if (DIRECT) {
+    const int64_t o = static_cast<int64_t>(pr.y) * ld + pr.x;
+    if (kC)
+      reinterpret_cast<double2*>(out)[o] = make_double2(ore[0][0], oim[0][0]);
+    else
+      out[o] = ore[0][0];
+  } else {
+#pragma unroll
+    for (int b = 0; b < NBS; ++b) {
+      const int64_t col = static_cast<int64_t>(__ldg(near.trial_dofs + pr.y * NBS + b)) * ld;
+#pragma unroll
+      for (int a = 0; a < NBT; ++a) {
+        const int64_t o = col + __ldg(near.test_dofs + pr.x * NBT + a);
+        if (kC) {
+          atomicAdd(out + 2 * o, ore[a][b]);
+          atomicAdd(out + 2 * o + 1, oim[a][b]);
+        } else {
+          atomicAdd(out + o, ore[a][b]);
+        }
       }
     }
   }
@@ -753,22 +791,37 @@ template <int QT, int KER, int OP, int NBT, int NBS, bool MIXED, bool DIRECT, in
 cudaError_t launch_mode(const CellSet& test, const SpaceTiles& tt, const CellSet& trial,
                         const SpaceTiles& st, const RegularRule& rule, const RegularArgs& a,
                         int ty0, int ty1, cudaStream_t stream) {
-  const size_t smem = smem_bytes(rule.npts, MIXED && NM != kNearList, MIXED && NM == kNearInKernel,
-                                 DIRECT, KER == kHelmholtz, tt.max_tile_dofs, st.max_tile_dofs,
-                                 NBT, NBS);
+  const size_t smem = smem_bytes(rule.npts, MIXED, MIXED && NM == kNearInKernel, DIRECT,
+                                 KER == kHelmholtz, tt.max_tile_dofs, st.max_tile_dofs, NBT, NBS);
   auto fn = regular_tiles<QT, KER, OP, NBT, NBS, MIXED, DIRECT, PH, NM>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  dim3 grid;
-  if (NM == kNearList) {
-    if (a.near.nlist <= 0) return cudaSuccess;
-    grid = dim3(a.near.nlist);
-  } else {
-    grid = dim3((test.ncells + kTile - 1) / kTile, ty1 - ty0);
-  }
+  const dim3 grid((test.ncells + kTile - 1) / kTile, ty1 - ty0);
   fn<<<grid, kThreads, smem, stream>>>(test, tt, trial, st, rule, a.k, a.same_grid,
                                        static_cast<double*>(a.out), a.ld, ty0, ty1, a.near);
+  return cudaGetLastError();
+}
+
+template <int QT, int KER, int OP, int NBT, int NBS, bool DIRECT>
+cudaError_t launch_near_pairs(const CellSet& test, const CellSet& trial, const RegularRule& rule,
+                              const RegularArgs& a, int ty0, int ty1, cudaStream_t stream) {
+  if (a.near.npairs <= 0) return cudaSuccess;
+  if (!DIRECT && (!a.near.test_dofs || !a.near.trial_dofs)) return cudaErrorInvalidValue;
+  // two tiles per warp (each lane stages its own column); up to 4 warps within 200 KB
+  const size_t per_warp = 2 * (sizeof(double) * tile_doubles(rule.npts) + sizeof(int) * tile_ints(1) + 16);
+  const int warps = static_cast<int>(std::max<size_t>(1, std::min<size_t>(kWarps, (200u << 10) / per_warp)));
+  const size_t smem = warps * per_warp + 16;
+  auto fn = near_pairs_fp64<QT, KER, OP, NBT, NBS, DIRECT>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  const int threads = 32 * warps;
+  const int blocks = (a.near.npairs + threads - 1) / threads;
+  const int lo = ty0 * kTile;
+  const int hi = ty1 * kTile >= trial.ncells ? 0x7fffffff : ty1 * kTile;
+  fn<<<blocks, threads, smem, stream>>>(test, trial, rule, a.k, a.near,
+                                        static_cast<double*>(a.out), a.ld, lo, hi);
   return cudaGetLastError();
 }
 
@@ -808,8 +861,7 @@ cudaError_t launch_one(const CellSet& test, const SpaceTiles& tt, const CellSet&
       e = launch_mode<QT, KER, OP, NBT, NBS, true, DIRECT, kPhaseSmall, kNearMasked>(
           test, tt, trial, st, rule, a, ty0, ty1, stream);
     if (e != cudaSuccess) return e;
-    return launch_mode<QT, KER, OP, NBT, NBS, true, DIRECT, kPhaseSmall, kNearList>(
-        test, tt, trial, st, rule, a, ty0, ty1, stream);
+    return launch_near_pairs<QT, KER, OP, NBT, NBS, DIRECT>(test, trial, rule, a, ty0, ty1, stream);
   }
 }
 

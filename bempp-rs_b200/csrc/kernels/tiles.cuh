@@ -53,6 +53,22 @@ __device__ inline Tile carve_tile(unsigned char*& cursor, int q, bool mixed, int
   return t;
 }
 
+__device__ inline void stage_geo(const Tile& t, int c, const CellSet& cs, int cell) {
+  const int N = cs.ncells;
+  const double nx = g(cs.geom, kNx, N, cell), ny = g(cs.geom, kNy, N, cell),
+               nz = g(cs.geom, kNz, N, cell);
+  t.geo[fJdet * kTile + c] = g(cs.geom, kJdet, N, cell);
+  t.geo[fNx * kTile + c] = nx;
+  t.geo[fNy * kTile + c] = ny;
+  t.geo[fNz * kTile + c] = nz;
+  t.geo[fH * kTile + c] = g(cs.geom, kV0x, N, cell) * nx + g(cs.geom, kV0y, N, cell) * ny +
+                          g(cs.geom, kV0z, N, cell) * nz;
+  for (int f = 0; f < 6; ++f) t.geo[(fT0x + f) * kTile + c] = g(cs.geom, kT0x + f, N, cell);
+  for (int f = 0; f < 3; ++f) t.geo[(fCx + f) * kTile + c] = g(cs.geom, kCx + f, N, cell);
+  t.geo[fDiam * kTile + c] = g(cs.geom, kDiam, N, cell);
+  t.geo[fRad * kTile + c] = g(cs.geom, kRad, N, cell);
+}
+
 __device__ inline void load_tile(const Tile& t, const CellSet& cs, int c0, int n, int q, bool mixed,
                           const uint8_t* cell_ldof, int nb) {
   const int N = cs.ncells;
@@ -69,21 +85,19 @@ __device__ inline void load_tile(const Tile& t, const CellSet& cs, int c0, int n
     }
   for (int c = threadIdx.x; c < kTile; c += kThreads) {
     const int cell = c0 + min(c, n - 1);
-    const double nx = g(cs.geom, kNx, N, cell), ny = g(cs.geom, kNy, N, cell),
-                 nz = g(cs.geom, kNz, N, cell);
-    t.geo[fJdet * kTile + c] = g(cs.geom, kJdet, N, cell);
-    t.geo[fNx * kTile + c] = nx;
-    t.geo[fNy * kTile + c] = ny;
-    t.geo[fNz * kTile + c] = nz;
-    t.geo[fH * kTile + c] = g(cs.geom, kV0x, N, cell) * nx + g(cs.geom, kV0y, N, cell) * ny +
-                            g(cs.geom, kV0z, N, cell) * nz;
-    for (int f = 0; f < 6; ++f) t.geo[(fT0x + f) * kTile + c] = g(cs.geom, kT0x + f, N, cell);
-    for (int f = 0; f < 3; ++f) t.geo[(fCx + f) * kTile + c] = g(cs.geom, kCx + f, N, cell);
-    t.geo[fDiam * kTile + c] = g(cs.geom, kDiam, N, cell);
-    t.geo[fRad * kTile + c] = g(cs.geom, kRad, N, cell);
+    stage_geo(t, c, cs, cell);
     for (int v = 0; v < 3; ++v) t.vid[v * kTile + c] = c < n ? __ldg(cs.vids + v * N + cell) : -1 - v;
     for (int b = 0; b < nb; ++b) t.ldof[b * kTile + c] = cell_ldof ? cell_ldof[cell * nb + b] : 0;
   }
+}
+
+// One cell's FP64 quadrature points and geometry into column c of a tile (the staging of
+// a single lane).
+__device__ inline void stage_cell(const Tile& t, int c, const CellSet& cs, int cell, int q) {
+  const int N = cs.ncells;
+  for (int pd = 0; pd < 3 * q; ++pd)
+    t.pts[pd * kTile + c] = __ldg(cs.qpts + static_cast<int64_t>(pd) * N + cell);
+  stage_geo(t, c, cs, cell);
 }
 
 
