@@ -23,19 +23,25 @@ void GridT::build_topology() {
   for (int64_t c = 0; c < ncells; ++c)
     for (int i = 0; i < 3; ++i) vertex_cells[cells[3 * c + i]].push_back(static_cast<int>(c));
   // edges: numbered in first-visit order over cells and local edges [1,2], [0,2], [0,1]
-  std::map<std::pair<int, int>, int> index;
+  // (an open-addressing hash table of the packed vertex pairs)
   cell_edges.resize(ncells);
   const int local[3][2] = {{1, 2}, {0, 2}, {0, 1}};
+  size_t cap = 16;
+  while (cap < static_cast<size_t>(6 * ncells)) cap <<= 1;
+  std::vector<uint64_t> keys(cap, ~uint64_t(0));
+  std::vector<int> vals(cap, -1);
   for (int64_t c = 0; c < ncells; ++c)
     for (int e = 0; e < 3; ++e) {
-      int a = cells[3 * c + local[e][0]], b = cells[3 * c + local[e][1]];
-      auto key = std::make_pair(std::min(a, b), std::max(a, b));
-      auto it = index.find(key);
-      if (it == index.end()) {
-        it = index.emplace(key, static_cast<int>(edges.size())).first;
-        edges.push_back(key);
+      const int a = cells[3 * c + local[e][0]], b = cells[3 * c + local[e][1]];
+      const uint64_t key = (static_cast<uint64_t>(std::min(a, b)) << 32) | static_cast<uint32_t>(std::max(a, b));
+      size_t h = static_cast<size_t>((key * 0x9E3779B97F4A7C15ull) >> 17) & (cap - 1);
+      while (keys[h] != key && keys[h] != ~uint64_t(0)) h = (h + 1) & (cap - 1);
+      if (keys[h] != key) {
+        keys[h] = key;
+        vals[h] = static_cast<int>(edges.size());
+        edges.push_back({std::min(a, b), std::max(a, b)});
       }
-      cell_edges[c][e] = it->second;
+      cell_edges[c][e] = vals[h];
     }
 }
 
@@ -118,36 +124,59 @@ std::vector<std::vector<int64_t>> cell_colouring(const SpaceT& s) {
 // Singular pair enumeration; pairs grouped by configuration (as cell_pairs[config] in
 // make_cell_blocks), vertices visited in increasing order.
 void build_singular_pairs(GridT& g, SingularPairList& out) {
-  const auto& cfgs = singular_configurations();
-  std::vector<std::vector<std::pair<int, int>>> by_cfg(cfgs.size());
-  std::vector<std::pair<int, int>> pairs;
+  const int ncfg = static_cast<int>(singular_configurations().size());
+  std::vector<std::vector<std::pair<int, int>>> by_cfg(ncfg);
+  for (auto& b : by_cfg) b.reserve(static_cast<size_t>(g.ncells) / 2 + 16);
+  const int* cells = g.cells.data();
   for (int64_t v = 0; v < g.npoints; ++v)
     for (int tc : g.vertex_cells[v])
       for (int sc : g.vertex_cells[v]) {
-        pairs.clear();
+        // shared vertices as (test local, trial local), trial local ascending; the pair
+        // belongs to its smallest shared vertex
+        int ts[3], ss[3], n = 0;
         bool smallest = true;
         for (int si = 0; si < 3 && smallest; ++si)
           for (int ti = 0; ti < 3; ++ti)
-            if (g.cells[3 * tc + ti] == g.cells[3 * sc + si]) {
-              if (g.cells[3 * tc + ti] < v) {
+            if (cells[3 * tc + ti] == cells[3 * sc + si]) {
+              if (cells[3 * tc + ti] < v) {
                 smallest = false;
                 break;
               }
-              pairs.push_back({ti, si});
+              ts[n] = ti;
+              ss[n] = si;
+              ++n;
             }
         if (!smallest) continue;
-        auto it = std::find(cfgs.begin(), cfgs.end(), pairs);
-        if (it == cfgs.end()) throw Error(kInternal, "unknown adjacency configuration");
-        by_cfg[it - cfgs.begin()].push_back({tc, sc});
+        // configuration index in the order of singular_configurations(): 9 vertex pairings
+        // (test * 3 + trial), 18 edge pairings (edges opposite et / es, two orientations),
+        // identical cells last
+        int cfg;
+        if (n == 1) {
+          cfg = ts[0] * 3 + ss[0];
+        } else if (n == 2) {
+          const int et = 3 - ts[0] - ts[1], es = 3 - ss[0] - ss[1];
+          cfg = 9 + (et * 3 + es) * 2 + (ts[0] < ts[1] ? 0 : 1);
+        } else if (n == 3 && ts[0] == 0 && ts[1] == 1 && ts[2] == 2) {
+          cfg = 27;
+        } else {
+          throw Error(kInternal, "unknown adjacency configuration");
+        }
+        if (cfg >= ncfg) throw Error(kInternal, "unknown adjacency configuration");
+        by_cfg[cfg].push_back({tc, sc});
       }
+  size_t total = 0;
+  for (const auto& b : by_cfg) total += b.size();
   out.test_cell.clear();
   out.trial_cell.clear();
   out.config.clear();
-  for (size_t c = 0; c < by_cfg.size(); ++c)
+  out.test_cell.reserve(total);
+  out.trial_cell.reserve(total);
+  out.config.reserve(total);
+  for (int c = 0; c < ncfg; ++c)
     for (auto& p : by_cfg[c]) {
       out.test_cell.push_back(p.first);
       out.trial_cell.push_back(p.second);
-      out.config.push_back(static_cast<int>(c));
+      out.config.push_back(c);
     }
 }
 
