@@ -69,6 +69,55 @@ class Precision(Enum):
     Mixed = _lib.Precision_Mixed
 
 
+# Dense outputs of at least this many bytes are allocated page-locked (set to None to
+# always allocate pageable numpy memory).
+PINNED_OUTPUT_MIN_BYTES = 16 << 20
+
+
+class _PageLockedBlock:
+    """Owner of one page-locked block of the library's cache, exposed to numpy through
+    ``__array_interface__`` (column-major); the block returns to the cache when the last
+    array viewing it is gone."""
+
+    def __init__(self, shape, dtype):
+        self._dtype = np.dtype(dtype)
+        self._shape = tuple(int(x) for x in shape)
+        nbytes = int(np.prod(self._shape)) * self._dtype.itemsize
+        self._ptr = _lib.bempp_host_alloc(nbytes)
+        if self._ptr == _ffi.NULL:
+            raise MemoryError(_last_error())
+        item = self._dtype.itemsize
+        self.__array_interface__ = {
+            "shape": self._shape, "typestr": self._dtype.str,
+            "data": (int(_ffi.cast("uintptr_t", self._ptr)), False),
+            "strides": (item, item * self._shape[0]), "version": 3}
+
+    def __del__(self):
+        ptr = getattr(self, "_ptr", None)
+        if ptr is not None and ptr != _ffi.NULL:
+            try:
+                _lib.bempp_host_free(ptr)
+            except Exception:  # interpreter shutdown
+                pass
+
+
+def _host_output(shape, dtype):
+    """Column-major output array for ``assemble``.
+
+    Large matrices live in page-locked blocks of the library's cache: the library then
+    writes the finished columns into them by DMA while later columns are still being
+    computed, with no staging copy, and a block freed by one result is reused by the
+    next.  Every entry is overwritten by the assembly.
+    """
+    nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+    if PINNED_OUTPUT_MIN_BYTES is not None and nbytes >= PINNED_OUTPUT_MIN_BYTES:
+        try:
+            return np.asarray(_PageLockedBlock(shape, dtype))
+        except MemoryError:  # page-locking refused: pageable memory
+            pass
+    return np.zeros(shape, dtype=dtype, order="F")
+
+
 class BoundaryAssemblerOptions(object):
     """Boundary assembler options."""
 
@@ -175,9 +224,7 @@ class BoundaryAssembler(object):
     ) -> npt.NDArray[np.floating]:
         """Assemble operator into a dense matrix."""
         self._check_spaces(trial_space, test_space)
-        output = np.zeros(
-            (test_space.global_size, trial_space.global_size), dtype=self.dtype, order="F"
-        )
+        output = _host_output((test_space.global_size, trial_space.global_size), self.dtype)
         _check(
             _lib.boundary_assembler_assemble_into_memory_ex(
                 self._rs_assembler,
@@ -237,10 +284,10 @@ class BoundaryAssembler(object):
     def host_copy_stats(self) -> typing.Dict[str, float]:
         """Host side of the last host-memory assembly: DMA wait and host copy times (ms),
         copy groups, assembly chunks and copy threads."""
-        buf = np.zeros(5, dtype=np.float64)
+        buf = np.zeros(6, dtype=np.float64)
         n = _lib.boundary_assembler_host_copy_stats(
-            self._rs_assembler, _ffi.cast("double*", buf.ctypes.data), 5)
-        keys = ("dma_wait_ms", "host_copy_ms", "groups", "chunks", "threads")
+            self._rs_assembler, _ffi.cast("double*", buf.ctypes.data), 6)
+        keys = ("dma_wait_ms", "host_copy_ms", "groups", "chunks", "threads", "prefault_ms")
         return {k: float(v) for k, v in zip(keys[:n], buf[:n])}
 
     def launch_count(self) -> int:

@@ -307,6 +307,67 @@ BemppStatus bempp_measure_fma_peak(int fp64, int iters, int reps, double* tflops
   });
 }
 
+// ------------------------------------------------------------ page-locked outputs ---
+// A cache of page-locked blocks: cudaHostAlloc'ing a gigabyte takes hundreds of
+// milliseconds, so freed blocks are kept for the next result of a similar size (a block
+// is reused for requests between half its size and its size).  Free blocks beyond
+// kHostCacheBytes are released.
+namespace {
+constexpr size_t kHostCacheBytes = size_t(16) << 30;
+std::mutex g_host_mu;
+std::map<void*, size_t> g_host_used;
+std::multimap<size_t, void*> g_host_free;  // by size
+size_t g_host_free_bytes = 0;
+}  // namespace
+
+void* bempp_host_alloc(size_t bytes) {
+  void* out = nullptr;
+  guarded([&] {
+    if (bytes == 0) throw Error(kInvalidArgument, "zero-byte block");
+    std::lock_guard<std::mutex> lock(g_host_mu);
+    auto it = g_host_free.lower_bound(bytes);
+    if (it != g_host_free.end() && it->first / 2 <= bytes) {
+      out = it->second;
+      g_host_used[out] = it->first;
+      g_host_free_bytes -= it->first;
+      g_host_free.erase(it);
+      return;
+    }
+    const size_t size = (bytes + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);
+    BEMPP_CUDA(cudaHostAlloc(&out, size, cudaHostAllocDefault));
+    g_host_used[out] = size;
+  });
+  return out;
+}
+
+void bempp_host_free(void* ptr) {
+  if (!ptr) return;
+  std::lock_guard<std::mutex> lock(g_host_mu);
+  auto it = g_host_used.find(ptr);
+  if (it == g_host_used.end()) return;
+  g_host_free.emplace(it->second, ptr);
+  g_host_free_bytes += it->second;
+  g_host_used.erase(it);
+  while (g_host_free_bytes > kHostCacheBytes && !g_host_free.empty()) {
+    auto big = std::prev(g_host_free.end());
+    cudaFreeHost(big->second);
+    g_host_free_bytes -= big->first;
+    g_host_free.erase(big);
+  }
+}
+
+size_t bempp_host_trim(void) {
+  std::lock_guard<std::mutex> lock(g_host_mu);
+  size_t released = 0;
+  for (auto& e : g_host_free) {
+    cudaFreeHost(e.second);
+    released += e.first;
+  }
+  g_host_free.clear();
+  g_host_free_bytes = 0;
+  return released;
+}
+
 // ---------------------------------------------------------------------- matrices ---
 size_t matrix_shape0(MatrixT* m) { return m ? m->rows : 0; }
 size_t matrix_shape1(MatrixT* m) { return m ? m->cols : 0; }

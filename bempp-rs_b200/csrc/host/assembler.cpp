@@ -391,8 +391,8 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
   } else {
     if (!empty) BEMPP_CUDA(cudaMemsetAsync(out, 0, static_cast<size_t>(nt) * ns * esize, stream));
     timer.mark();
-    // chunked: the singular pairs first (all adds commute), then the regular chunks
-    if (singular && nchunks > 1) run_singular(0, 0x7fffffff, stream);
+    // chunked: each chunk adds its regular pairs and the singular pairs of its trial cells
+    // (all adds commute), so its columns are final when it ends
     for (int c = 0; c < nchunks; ++c) {
       int t0, t1;
       tile_range(c, t0, t1);
@@ -402,6 +402,7 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
         BEMPP_CUDA(launch_regular_scatter(tcs, space_tiles(test), scs, space_tiles(trial), rule,
                                           ra, stream));
         a.launches += regular_launches;
+        if (singular && nchunks > 1) run_singular(32 * t0, c + 1 == nchunks ? 0x7fffffff : 32 * t1, stream);
       }
       if (nchunks == 1) {
         timer.mark();
@@ -570,6 +571,8 @@ BoundaryAssemblerT::~BoundaryAssemblerT() {
   for (auto& e : events)
     if (e) cudaEventDestroy(e);
   if (stream) cudaStreamDestroy(stream);
+  if (copy_stream) cudaStreamDestroy(copy_stream);
+  for (auto e : chunk_ev) cudaEventDestroy(e);
   if (side) {
     cudaStreamDestroy(side);
     cudaEventDestroy(fork_ev);

@@ -201,14 +201,16 @@ struct BoundaryAssemblerT {
   int events_recorded = 0;
   DeviceBuffer work;     // device output for host-memory assembly
   cudaStream_t stream = nullptr;  // host-memory assembly stream (created on first use)
+  cudaStream_t copy_stream = nullptr;     // page-locked destinations: direct DMA stream
+  std::vector<cudaEvent_t> chunk_ev;      // and its per-chunk events
   // side stream and fork / join events: the singular kernel of a mixed-precision DP0
   // assembly runs beside the regular kernels (created on first use, on side_device)
   cudaStream_t side = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   int side_device = -1;
   // last host-memory assembly: ms waiting for DMA, ms of host copy, copy groups, chunks,
-  // host copy threads
-  std::array<double, 5> host_copy_stats{};
+  // host copy threads, ms of destination page prefaulting
+  std::array<double, 6> host_copy_stats{};
   DeviceBuffer convert;  // FP64 staging for F32 / C32 outputs
   DeviceBuffer pair_values;
   std::mutex mu;

@@ -12,8 +12,13 @@
 // Staging: a process-wide ring of two pinned slots per device (kSlotBytes each) and one
 // copy stream, used by one assembly at a time (mutex).  Host copies run on a small
 // persistent pool of worker threads, each taking an equal byte share of a group.
+// A destination that is itself page-locked skips the staging: the columns go there by
+// DMA directly.
 #include <sys/mman.h>
 #include <unistd.h>
+#if defined(__x86_64__)
+#include <emmintrin.h>
+#endif
 
 #include <algorithm>
 #include <chrono>
@@ -158,6 +163,66 @@ std::vector<Group> plan_groups(const ColumnRuns& runs, size_t col_bytes) {
   return groups;
 }
 
+// memcpy with non-temporal stores: the destination (a large, usually fresh array that
+// the caller reads much later) is written without first reading its cache lines, one
+// memory pass fewer than a cached copy.  The caller issues the store fence.
+void stream_copy(char* dst, const char* src, size_t n) {
+#if defined(__x86_64__)
+  const size_t head = std::min(n, (16 - reinterpret_cast<uintptr_t>(dst) % 16) % 16);
+  std::memcpy(dst, src, head);
+  dst += head;
+  src += head;
+  n -= head;
+  const size_t blocks = n / 64;
+  for (size_t i = 0; i < blocks; ++i, dst += 64, src += 64) {
+    const __m128i a = _mm_loadu_si128(reinterpret_cast<const __m128i*>(src));
+    const __m128i b = _mm_loadu_si128(reinterpret_cast<const __m128i*>(src + 16));
+    const __m128i c = _mm_loadu_si128(reinterpret_cast<const __m128i*>(src + 32));
+    const __m128i d = _mm_loadu_si128(reinterpret_cast<const __m128i*>(src + 48));
+    _mm_stream_si128(reinterpret_cast<__m128i*>(dst), a);
+    _mm_stream_si128(reinterpret_cast<__m128i*>(dst + 16), b);
+    _mm_stream_si128(reinterpret_cast<__m128i*>(dst + 32), c);
+    _mm_stream_si128(reinterpret_cast<__m128i*>(dst + 48), d);
+  }
+  std::memcpy(dst, src, n - 64 * blocks);
+#else
+  std::memcpy(dst, src, n);
+#endif
+}
+
+#ifndef MADV_POPULATE_WRITE
+#define MADV_POPULATE_WRITE 23  // Linux 5.14+
+#endif
+
+// Page faults of one group's destination ranges, taken ahead of the copy while the host
+// would otherwise wait for the GPU: madvise(MADV_POPULATE_WRITE) on the pages covering
+// each range (pages already present are left as they are; missing ones arrive zeroed),
+// or, where the kernel lacks it, a one-byte write at the first address of each page
+// inside the range.  Only ranges of groups not yet copied are given; the copy overwrites
+// them.
+void prefault(const Group& g, void* dst) {
+  CopyPool& pool = CopyPool::get();
+  const uintptr_t page = static_cast<uintptr_t>(sysconf(_SC_PAGESIZE));
+  const int nt = pool.size();
+  const size_t share = (g.bytes + nt - 1) / nt;
+  pool.run([&](int t) {
+    const size_t lo = std::min(g.bytes, share * t), hi = std::min(g.bytes, lo + share);
+    for (const Piece& p : g.pieces) {
+      const size_t a = std::max(lo, p.slot_off), b = std::min(hi, p.slot_off + p.bytes);
+      if (a >= b) continue;
+      char* first = static_cast<char*>(dst) + p.src_off + (a - p.slot_off);
+      char* last = first + (b - a);
+      const uintptr_t p0 = reinterpret_cast<uintptr_t>(first) & ~(page - 1);
+      const uintptr_t p1 = (reinterpret_cast<uintptr_t>(last) + page - 1) & ~(page - 1);
+      if (madvise(reinterpret_cast<void*>(p0), p1 - p0, MADV_POPULATE_WRITE) == 0) continue;
+      for (char* q = first; q < last;) {
+        *reinterpret_cast<volatile char*>(q) = 0;
+        q = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(q) / page + 1) * page);
+      }
+    }
+  });
+}
+
 // Parallel copy of one staged group into the host matrix.
 void host_copy(const Group& g, const void* slot, void* dst) {
   CopyPool& pool = CopyPool::get();
@@ -168,10 +233,28 @@ void host_copy(const Group& g, const void* slot, void* dst) {
     for (const Piece& p : g.pieces) {
       const size_t a = std::max(lo, p.slot_off), b = std::min(hi, p.slot_off + p.bytes);
       if (a >= b) continue;
-      std::memcpy(static_cast<char*>(dst) + p.src_off + (a - p.slot_off),
+      stream_copy(static_cast<char*>(dst) + p.src_off + (a - p.slot_off),
                   static_cast<const char*>(slot) + a, b - a);
     }
+#if defined(__x86_64__)
+    _mm_sfence();  // this thread's streaming stores are visible before the job ends
+#endif
   });
+}
+
+// True when both ends of [p, p + bytes) are page-locked host memory known to CUDA
+// (cudaHostAlloc / cudaHostRegister), which the copy engines can write directly.
+bool page_locked(const void* p, size_t bytes) {
+  const char* ends[2] = {static_cast<const char*>(p), static_cast<const char*>(p) + bytes - 1};
+  for (const char* q : ends) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, q) != cudaSuccess) {
+      cudaGetLastError();  // pageable memory on older drivers: not an error here
+      return false;
+    }
+    if (at.type != cudaMemoryTypeHost) return false;
+  }
+  return true;
 }
 
 }  // namespace
@@ -193,6 +276,44 @@ void assemble_host(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* dat
   if (single && !dp0) want = 1;
   const int nchunks = effective_chunks(trial, want);
   const ColumnRuns& runs = chunk_columns(trial, nchunks);
+
+  if (page_locked(data, bytes)) {
+    // A page-locked destination takes each chunk's finished columns straight from the
+    // device (one DMA per run of columns on a copy stream): no staging, no host copy.
+    if (!a.copy_stream) BEMPP_CUDA(cudaStreamCreateWithFlags(&a.copy_stream, cudaStreamNonBlocking));
+    while (a.chunk_ev.size() < static_cast<size_t>(nchunks)) {
+      cudaEvent_t e;
+      BEMPP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      a.chunk_ev.push_back(e);
+    }
+    struct Drain {
+      cudaStream_t s0, s1;
+      ~Drain() {
+        cudaStreamSynchronize(s0);
+        cudaStreamSynchronize(s1);
+      }
+    } drain{a.stream, a.copy_stream};
+    assemble_device(a, trial, test, a.work.ptr, a.stream, nchunks, [&](int c) {
+      BEMPP_CUDA(cudaEventRecord(a.chunk_ev[c], a.stream));
+    });
+    const char* src = static_cast<const char*>(a.work.ptr);
+    size_t ncopies = 0;
+    for (int c = 0; c < nchunks; ++c) {
+      BEMPP_CUDA(cudaStreamWaitEvent(a.copy_stream, a.chunk_ev[c], 0));
+      for (const auto& run : runs[c]) {
+        const size_t off = static_cast<size_t>(run.first) * col_bytes;
+        BEMPP_CUDA(cudaMemcpyAsync(static_cast<char*>(data) + off, src + off,
+                                   static_cast<size_t>(run.second) * col_bytes,
+                                   cudaMemcpyDeviceToHost, a.copy_stream));
+        ++ncopies;
+      }
+    }
+    BEMPP_CUDA(cudaStreamSynchronize(a.copy_stream));
+    BEMPP_CUDA(cudaStreamSynchronize(a.stream));
+    a.host_copy_stats = {0.0, 0.0, static_cast<double>(ncopies), static_cast<double>(nchunks),
+                         0.0, 0.0};
+    return;
+  }
   const std::vector<Group> groups = plan_groups(runs, col_bytes);
 
   // Large destinations are usually fresh, untouched allocations (numpy zeros): ask for
@@ -238,10 +359,21 @@ void assemble_host(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* dat
   };
   for (size_t gi = 0; gi < std::min<size_t>(2, groups.size()); ++gi) enqueue(gi);
   using clock = std::chrono::steady_clock;
-  double wait_ms = 0.0, copy_ms = 0.0;
+  double wait_ms = 0.0, copy_ms = 0.0, prefault_ms = 0.0;
+  size_t touched = 0;  // groups [0, touched) have been prefaulted or copied
   for (size_t gi = 0; gi < groups.size(); ++gi) {
     const int s = static_cast<int>(gi & 1);
     const auto t0 = clock::now();
+    // while this group's data is still on its way, take the page faults of the next ones
+    touched = std::max(touched, gi);
+    while (touched < groups.size()) {
+      const cudaError_t q = cudaEventQuery(st.copied[s]);
+      if (q == cudaSuccess) break;
+      if (q != cudaErrorNotReady) BEMPP_CUDA(q);
+      const auto tp = clock::now();
+      prefault(groups[touched++], data);
+      prefault_ms += std::chrono::duration<double, std::milli>(clock::now() - tp).count();
+    }
     BEMPP_CUDA(cudaEventSynchronize(st.copied[s]));
     const auto t1 = clock::now();
     host_copy(groups[gi], st.slot[s], data);
@@ -249,10 +381,10 @@ void assemble_host(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* dat
     wait_ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
     if (gi + 2 < groups.size()) enqueue(gi + 2);
   }
-  a.host_copy_stats = {wait_ms, copy_ms, static_cast<double>(groups.size()),
-                       static_cast<double>(nchunks), static_cast<double>(CopyPool::get().size())};
+  a.host_copy_stats = {wait_ms - prefault_ms, copy_ms, static_cast<double>(groups.size()),
+                       static_cast<double>(nchunks), static_cast<double>(CopyPool::get().size()),
+                       prefault_ms};
   BEMPP_CUDA(cudaStreamSynchronize(a.stream));
-  BEMPP_CUDA(cudaGetLastError());
 }
 
 }  // namespace bempp_b200

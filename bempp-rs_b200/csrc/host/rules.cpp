@@ -84,9 +84,12 @@ RegularRule simplex_rule(int npoints) {
       r.vf[i] = static_cast<float>(e.points[2 * i + 1] - 1.0 / 3.0);
       const double x = e.points[2 * i], y = e.points[2 * i + 1];
       const double phi[3] = {1.0 - x - y, x, y};
+      r.u[i] = x - 1.0 / 3.0;
+      r.v[i] = y - 1.0 / 3.0;
       for (int b = 0; b < 3; ++b) {
         r.phi[b][i] = phi[b];
         r.phif[b][i] = static_cast<float>(phi[b]);
+        r.wphi[b][i] = e.weights[i] * phi[b];
       }
     }
     return r;

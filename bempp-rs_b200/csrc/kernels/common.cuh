@@ -42,6 +42,11 @@ struct RegularRule {
   // P1 basis values phi_b(xi_q) = (1 - x - y, x, y) at each point, FP64 and FP32
   double phi[3][kMaxRegularPoints];
   float phif[3][kMaxRegularPoints];
+  // FP64 offsets from the centroid in reference coordinates, (u, v) = xi - (1/3, 1/3),
+  // and the weights times the P1 basis values, w_q phi_b(xi_q)
+  double u[kMaxRegularPoints];
+  double v[kMaxRegularPoints];
+  double wphi[3][kMaxRegularPoints];
 };
 
 struct CellSet {
@@ -113,6 +118,18 @@ __device__ __forceinline__ void sincos_cw(double t, double& s, double& c) {
   const int q = static_cast<int>(static_cast<long long>(n) & 3);
   c = (q == 0) ? cr : (q == 1) ? -sr : (q == 2) ? -cr : sr;
   s = (q == 0) ? sr : (q == 1) ? cr : (q == 2) ? -sr : -cr;
+}
+
+// a^(-3/2) for normal positive FP64 a: the rsqrt.approx.ftz.f64 seed y refined by the
+// series (1 - e)^(-3/2) = 1 + 3e/2 + 15e^2/8 + O(e^3) with e = 1 - a y^2 (the inverse cube
+// of a distance from its square, for double-layer kernels).
+__device__ __forceinline__ double rinv3_refined(double a) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+  const double y2 = y * y;
+  const double e = fma(-a, y2, 1.0);
+  const double y3 = y2 * y;
+  return fma(y3 * e, fma(e, 1.875, 1.5), y3);
 }
 
 // P1 basis on the reference triangle: phi0 = 1 - x - y, phi1 = x, phi2 = y.

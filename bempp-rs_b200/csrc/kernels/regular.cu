@@ -125,12 +125,26 @@ __device__ __forceinline__ void block_fp64(const Tile& T, int it, const Tile& S,
   for (int a = 0; a < NBT; ++a)
 #pragma unroll
     for (int b = 0; b < NBS; ++b) blk_re[a][b] = blk_im[a][b] = 0.0;
-  const double nxi = T.G(fNx, it), nyi = T.G(fNy, it), nzi = T.G(fNz, it), hi = T.G(fH, it);
-  const double nxj = S.G(fNx, js), nyj = S.G(fNy, js), nzj = S.G(fNz, js), hj = S.G(fH, js);
+  // normal-derivative factors in the cells' tangent coordinates, free of the cancellation
+  // of x.n - h far from the origin: with dc = c_x - c_y and (u, v) = xi - (1/3, 1/3),
+  // DL (x_p - y).n_y = dc.n_y + u_p t0_x.n_y + v_p t1_x.n_y (y on the trial plane),
+  // ADL (y_q - x).n_x = -dc.n_x + u_q t0_y.n_x + v_q t1_y.n_x (x on the test plane)
+  double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+  if (OP == kDL || OP == kADL) {
+    const double dcx = T.G(fCx, it) - S.G(fCx, js), dcy = T.G(fCy, it) - S.G(fCy, js),
+                 dcz = T.G(fCz, it) - S.G(fCz, js);
+    const Tile& N = OP == kDL ? S : T;    // the cell whose normal is used
+    const Tile& D = OP == kDL ? T : S;    // the cell whose tangents are used
+    const int cn = OP == kDL ? js : it, cd = OP == kDL ? it : js;
+    const double nx = N.G(fNx, cn), ny = N.G(fNy, cn), nz = N.G(fNz, cn);
+    f0 = (OP == kDL ? 1.0 : -1.0) * (dcx * nx + dcy * ny + dcz * nz);
+    f1 = D.G(fT0x, cd) * nx + D.G(fT0y, cd) * ny + D.G(fT0z, cd) * nz;
+    f2 = D.G(fT1x, cd) * nx + D.G(fT1y, cd) * ny + D.G(fT1z, cd) * nz;
+  }
 #pragma unroll 1
   for (int p = 0; p < Q; ++p) {
     const double x0 = T.P(p, 0, it), x1 = T.P(p, 1, it), x2 = T.P(p, 2, it);
-    const double ap = OP == kDL ? x0 * nxj + x1 * nyj + x2 * nzj - hj : 1.0;
+    const double ap = OP == kDL ? fma(rule.u[p], f1, fma(rule.v[p], f2, f0)) : 1.0;
     double u_re[NBS], u_im[NBS], g_re = 0.0, g_im = 0.0;
 #pragma unroll
     for (int b = 0; b < NBS; ++b) u_re[b] = u_im[b] = 0.0;
@@ -139,13 +153,26 @@ __device__ __forceinline__ void block_fp64(const Tile& T, int it, const Tile& S,
       const double y0 = S.P(q, 0, js), y1 = S.P(q, 1, js), y2 = S.P(q, 2, js);
       const double dx = x0 - y0, dy = x1 - y1, dz = x2 - y2;
       const double r2 = dx * dx + dy * dy + dz * dz;
+      if (KER == kLaplace) {
+        // 1/r or 1/r^3 straight from the refined hardware seed; the weight (times the
+        // basis value for P1) enters as a rule constant of the accumulating FMA
+        double kern = (OP == kSL || OP == kHS) ? rsqrt_refined(r2) : rinv3_refined(r2);
+        if (OP == kADL) kern *= fma(rule.u[q], f1, fma(rule.v[q], f2, f0));
+        if (OP == kHS) {
+          g_re = fma(kern, rule.w[q], g_re);
+        } else if (NBS == 1) {
+          u_re[0] = fma(kern, rule.w[q], u_re[0]);
+        } else {
+#pragma unroll
+          for (int b = 0; b < NBS; ++b) u_re[b] = fma(kern, rule.wphi[b][q], u_re[b]);
+        }
+        continue;
+      }
       const double rinv = rsqrt_refined(r2);
       double wq = rule.w[q];
-      if (OP == kADL) wq *= y0 * nxi + y1 * nyi + y2 * nzi - hi;
+      if (OP == kADL) wq *= fma(rule.u[q], f1, fma(rule.v[q], f2, f0));
       double kre, kim = 0.0;
-      if (KER == kLaplace) {
-        kre = (OP == kSL || OP == kHS) ? wq * rinv : wq * rinv * rinv * rinv;
-      } else {
+      {
         const double r = r2 * rinv;
         double sn, cs;
         if (kFast)

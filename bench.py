@@ -533,14 +533,21 @@ def run_ours(args):
         pts_h = np.ascontiguousarray(wl.points)
         cells_h = np.ascontiguousarray(wl.cells)
         e2e_steps = max(1, min(args.steps, 3))
+        # one untimed step: first-use costs (page-locked output blocks, copy threads)
+        _, s2 = build_space(pts_h, cells_h, w["space"])
+        for _, a in wl.assemblers:
+            a.assemble(s2, s2)
+        del s2
         torch.cuda.synchronize()
         barrier()
         t = time.perf_counter()
         t_build = 0.0
         t_ops = [0.0] * len(wl.assemblers)
         copy_stats = [None] * len(wl.assemblers)
+        t_free = 0.0
+        steps_ms = []
         for _ in range(e2e_steps):
-            t1 = time.perf_counter()
+            t0 = t1 = time.perf_counter()
             _, s2 = build_space(pts_h, cells_h, w["space"])
             t_build += time.perf_counter() - t1
             for i, (_, a) in enumerate(wl.assemblers):
@@ -548,7 +555,10 @@ def run_ours(args):
                 a.assemble(s2, s2)
                 t_ops[i] += time.perf_counter() - t1
                 copy_stats[i] = a.host_copy_stats()
+            t1 = time.perf_counter()
             del s2
+            t_free += time.perf_counter() - t1
+            steps_ms.append(1e3 * (time.perf_counter() - t0))
         e2e_s = (time.perf_counter() - t) / e2e_steps
         e2e_s = max_over_ranks(e2e_s, world)
         esize = 16 if w["kernel"] == "helmholtz" else 8
@@ -556,7 +566,8 @@ def run_ours(args):
                "h2d_bytes_per_step": int(pts_h.nbytes + cells_h.astype(np.uintp).nbytes),
                "d2h_bytes_per_step": int(wl.entries_per_step * esize),
                "ms_per_step": e2e_s * 1e3,
-               "breakdown_ms": {"grid_and_space": 1e3 * t_build / e2e_steps,
+               "breakdown_ms": {"steps": steps_ms, "grid_and_space": 1e3 * t_build / e2e_steps,
+                                "free_grid_and_space": 1e3 * t_free / e2e_steps,
                                 "assemble": {n: 1e3 * t / e2e_steps
                                              for (n, _), t in zip(wl.assemblers, t_ops)},
                                 "host_copy_last": {n: c for (n, _), c in zip(wl.assemblers,

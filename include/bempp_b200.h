@@ -169,12 +169,22 @@ size_t boundary_assembler_last_launch_count(BoundaryAssemblerT *assembler);
 /* Addition (no counterpart in the reference): statistics of the last host-memory
  * assembly (boundary_assembler_assemble_into_memory[_ex] / boundary_assembler_assemble):
  * [ms the host waited for device-to-host DMA, ms of host copies into the caller's array,
- * copy groups, assembly chunks, host copy threads]; returns the number written (<= n). */
+ * copy groups, assembly chunks, host copy threads, ms spent taking the destination's page
+ * faults ahead of the copies]; returns the number written (<= n). */
 size_t boundary_assembler_host_copy_stats(BoundaryAssemblerT *assembler, double *out, size_t n);
 /* Addition: measured CUDA-core fused multiply-add throughput of the current device in
  * TFLOP/s (fp64 != 0: FP64, else FP32), the roofline denominator of the regular
  * quadrature kernels. */
 BemppStatus bempp_measure_fma_peak(int fp64, int iters, int reps, double *tflops);
+/* Addition (no counterpart in the reference): page-locked host blocks for dense outputs.
+ * A matrix assembled into page-locked memory is written by DMA as its columns finish,
+ * with no staging copy.  bempp_host_alloc returns a block of at least `bytes` (NULL and
+ * bempp_last_error() on failure) from a process-wide cache; bempp_host_free returns it
+ * to the cache (blocks stay page-locked for reuse); bempp_host_trim releases every
+ * cached free block to the system and returns the bytes released. */
+void *bempp_host_alloc(size_t bytes);
+void bempp_host_free(void *ptr);
+size_t bempp_host_trim(void);
 
 /* ------------------------------------------------------------------ matrices ----- */
 /* src/bindings/matrices.rs:6-20 */

@@ -1,7 +1,9 @@
 """Host-memory assembly (BoundaryAssembler.assemble -> boundary_assembler_assemble_into_memory_ex)
 on matrices large enough to be assembled in several chunks of trial tiles, with the
 device-to-host copy of finished columns overlapped: the result must equal the
-single-launch device assembly (assemble_into_device) of the same operator.
+single-launch device assembly (assemble_into_device) of the same operator.  Every case
+runs twice: into a page-locked output (direct DMA of finished columns) and into a
+pageable numpy array (pinned staging ring and host copy threads).
 
 DP0 x DP0 entries are written by one kernel and one singular add each, so the chunked
 result is bit-identical; P1 entries are sums of atomic adds whose order differs between
@@ -24,8 +26,23 @@ from test_gpu_parity import oracle_assemble, rel_err
 
 pytestmark = pytest.mark.gpu
 
+
+@pytest.fixture(params=["page_locked", "pageable"], autouse=True)
+def output_memory(request, monkeypatch):
+    from bempp.assembly import boundary
+
+    if request.param == "pageable":
+        monkeypatch.setattr(boundary, "PINNED_OUTPUT_MIN_BYTES", None)
+    return request.param
+
 OPS = {"single_layer": OperatorType.SingleLayer, "double_layer": OperatorType.DoubleLayer,
        "hypersingular": OperatorType.Hypersingular}
+
+
+def boundary_pinned():
+    from bempp.assembly import boundary
+
+    return boundary.PINNED_OUTPUT_MIN_BYTES is not None
 
 
 def assemble_both(level, kernel, op, k, degree, dtype):
@@ -44,6 +61,8 @@ def assemble_both(level, kernel, op, k, degree, dtype):
     else:
         a = create_helmholtz_assembler(OPS[op], k, opts, dtype)
     host = a.assemble(sp, sp)
+    if boundary_pinned():
+        assert type(host.base).__name__ == "_PageLockedBlock"
     n = sp.global_size
     tdt = {np.float64: torch.float64, np.float32: torch.float32,
            np.complex128: torch.complex128, np.complex64: torch.complex64}[dtype]
@@ -83,3 +102,13 @@ def test_chunked_p1_helmholtz_hypersingular():
     # 2562^2 complex128 = 105 MB: 2 chunks
     _, host, dev = assemble_both(4, "helmholtz", "hypersingular", 5.0, 1, np.complex128)
     assert rel_err(host, dev) <= 1e-13
+
+
+def test_page_locked_result_outlives_the_next_assembly():
+    """A kept result is not reused for the next one (its block stays alive)."""
+    _, first, _ = assemble_both(4, "laplace", "double_layer", 0.0, 0, np.float64)
+    keep = first.copy()
+    _, second, _ = assemble_both(4, "laplace", "single_layer", 0.0, 0, np.float64)
+    assert np.array_equal(first, keep)
+    assert not np.array_equal(first, second)
+
