@@ -103,13 +103,14 @@ const GridGeometry& grid_geometry(GridT& g, int device, const RegularRule& rule,
     auto geo = std::make_unique<GridGeometry>();
     const size_t n = g.ncells;
     geo->npts = rule.npts;
-    geo->geom.alloc(sizeof(double) * kNumGeomFields * n);
-    geo->qpts.alloc(sizeof(double) * 3 * rule.npts * n);
-    geo->qrel.alloc(sizeof(float) * 3 * rule.npts * n);
-    geo->vids.alloc(sizeof(int) * 3 * n);
+    const size_t S = static_cast<size_t>(cell_stride(static_cast<int>(n)));  // padded rows
+    geo->geom.alloc(sizeof(double) * kNumGeomFields * S);
+    geo->qpts.alloc(sizeof(double) * 3 * rule.npts * S);
+    geo->qrel.alloc(sizeof(float4) * rule.npts * S);
+    geo->vids.alloc(sizeof(int) * 3 * S);
     BEMPP_CUDA(launch_geometry(g.d_points.as<double>(), g.d_cells.as<int>(),
                                static_cast<int>(n), rule, geo->geom.as<double>(),
-                               geo->qpts.as<double>(), geo->qrel.as<float>(),
+                               geo->qpts.as<double>(), geo->qrel.as<float4>(),
                                geo->vids.as<int>(), stream));
     ++launches;
     // the cache is shared by every stream that assembles on this grid: finish it now
@@ -160,9 +161,10 @@ void ensure_space_device(SpaceT& s, int device) {
 CellSet cell_set(const GridT& g, const GridGeometry& geo) {
   CellSet c;
   c.ncells = static_cast<int>(g.ncells);
+  c.stride = cell_stride(c.ncells);
   c.geom = geo.geom.as<double>();
   c.qpts = geo.qpts.as<double>();
-  c.qrel = geo.qrel.as<float>();
+  c.qrel = geo.qrel.as<float4>();
   c.vids = geo.vids.as<int>();
   return c;
 }

@@ -242,6 +242,12 @@ void host_copy(const Group& g, const void* slot, void* dst) {
   });
 }
 
+void check_stage_timeouts() {
+  unsigned n = 0;
+  BEMPP_CUDA(take_stage_timeouts(&n));
+  if (n) throw Error(kCudaError, std::to_string(n) + " tile blocks timed out staging their input");
+}
+
 // True when both ends of [p, p + bytes) are page-locked host memory known to CUDA
 // (cudaHostAlloc / cudaHostRegister), which the copy engines can write directly.
 bool page_locked(const void* p, size_t bytes) {
@@ -310,6 +316,7 @@ void assemble_host(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* dat
     }
     BEMPP_CUDA(cudaStreamSynchronize(a.copy_stream));
     BEMPP_CUDA(cudaStreamSynchronize(a.stream));
+    check_stage_timeouts();
     a.host_copy_stats = {0.0, 0.0, static_cast<double>(ncopies), static_cast<double>(nchunks),
                          0.0, 0.0};
     return;
@@ -385,6 +392,7 @@ void assemble_host(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* dat
                        static_cast<double>(nchunks), static_cast<double>(CopyPool::get().size()),
                        prefault_ms};
   BEMPP_CUDA(cudaStreamSynchronize(a.stream));
+  check_stage_timeouts();
 }
 
 }  // namespace bempp_b200

@@ -115,9 +115,10 @@ void helmholtz_sl_sweep_device(GridT* const* grids, size_t ngrids, const double*
       const GridGeometry& geo = sweep_geometry(*grids[i], device, rule);
       SweepMesh& m = a.mesh[r];
       m.cells.ncells = static_cast<int>(grids[i]->ncells);
+      m.cells.stride = cell_stride(m.cells.ncells);
       m.cells.geom = geo.geom.as<double>();
       m.cells.qpts = geo.qpts.as<double>();
-      m.cells.qrel = geo.qrel.as<float>();
+      m.cells.qrel = geo.qrel.as<float4>();
       m.cells.vids = geo.vids.as<int>();
       m.out = static_cast<float2*>(outs[i]);
       m.ntiles = static_cast<int>((grids[i]->ncells + 31) / 32);

@@ -296,7 +296,7 @@ struct CellGeo {
 };
 
 __device__ __forceinline__ void load_geo(const CellSet& cs, int c, CellGeo& g) {
-  const int N = cs.ncells;
+  const int N = cs.stride;
   for (int d = 0; d < 3; ++d) {
     g.v0[d] = bempp_b200::g(cs.geom, kV0x + d, N, c);
     g.t0[d] = bempp_b200::g(cs.geom, kT0x + d, N, c);
@@ -384,7 +384,7 @@ __global__ void cell_to_point_gradient(CellSet cs, const double* __restrict__ gr
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= cs.ncells) return;
   for (int a = 0; a < 3; ++a) {
-    const int v = cs.vids[a * cs.ncells + c];
+    const int v = cs.vids[a * cs.stride + c];
     for (int d = 0; d < 3; ++d)
       atomicAdd(grad_points + 3 * static_cast<int64_t>(v) + d,
                 grad_cell[static_cast<int64_t>(c) * 9 + a * 3 + d]);

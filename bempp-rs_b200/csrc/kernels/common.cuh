@@ -1,11 +1,15 @@
 // Device-side data layout and Green's-function math shared by the assembly kernels.
 //
 // Layout in HBM (one allocation per grid, field-major so that a warp reading 32
-// consecutive cells of one field issues one 256-byte transaction):
-//   geom[f * ncells + c], f in GeomField     per-cell FP64 geometry of a flat triangle
-//   qpts[(p * 3 + d) * ncells + c]           physical regular quadrature point p of cell c
-//   qrel[(p * 3 + d) * ncells + c]           FP32 offset of that point from the centroid
-//   vids[i * ncells + c], i = 0..2           vertex (point) indices, for adjacency tests
+// consecutive cells of one field issues one 256-byte transaction).  Rows have the stride
+// S = ncells rounded up to a multiple of 32 (cell_stride), so that every 32-cell tile of
+// every row starts on a 256-byte boundary and can be staged by bulk (TMA) copies; the
+// padding cells hold zero geometry and vertex ids -1, -2, -3:
+//   geom[f * S + c], f in GeomField          per-cell FP64 geometry of a flat triangle
+//   qpts[(p * 3 + d) * S + c]                physical regular quadrature point p of cell c
+//   qrel[p * S + c]                          float4: FP32 offset of that point from the
+//                                            centroid (x, y, z) and its squared length (w)
+//   vids[i * S + c], i = 0..2                vertex (point) indices, for adjacency tests
 #pragma once
 
 #include <cuda_runtime.h>
@@ -22,8 +26,12 @@ enum GeomField : int {
   kCx, kCy, kCz,             // centroid
   kDiam,                     // element diameter (longest edge)
   kRad,                      // largest distance from the centroid to a vertex
+  kH,                        // v0 . n (the plane's offset)
   kNumGeomFields
 };
+
+// Row stride of the per-cell arrays of a grid with n cells.
+__host__ __device__ inline int cell_stride(int n) { return (n + 31) & ~31; }
 
 constexpr int kMaxRegularPoints = 37;
 constexpr double kInv4Pi = 0.079577471545947667884;
@@ -51,10 +59,11 @@ struct RegularRule {
 
 struct CellSet {
   int ncells;
-  const double* geom;   // kNumGeomFields * ncells
-  const double* qpts;   // npts * 3 * ncells
-  const float* qrel;    // npts * 3 * ncells (mixed precision only)
-  const int* vids;      // 3 * ncells
+  int stride;           // cell_stride(ncells)
+  const double* geom;   // kNumGeomFields * stride
+  const double* qpts;   // npts * 3 * stride
+  const float4* qrel;   // npts * stride (mixed precision only)
+  const int* vids;      // 3 * stride
 };
 
 // Kernel families and operators (OperatorType values of the C-ABI).

@@ -9,10 +9,20 @@ namespace bempp_b200 {
 
 __global__ void geometry_kernel(const double* __restrict__ points, const int* __restrict__ cells,
                                 int n, RegularRule rule, double* __restrict__ geom,
-                                double* __restrict__ qpts, float* __restrict__ qrel,
+                                double* __restrict__ qpts, float4* __restrict__ qrel,
                                 int* __restrict__ vids) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n) return;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int S = cell_stride(n);
+  if (c >= S) return;
+  if (c >= n) {  // padding of the last tile
+    for (int f = 0; f < kNumGeomFields; ++f) geom[static_cast<int64_t>(f) * S + c] = 0.0;
+    for (int p = 0; p < rule.npts; ++p) {
+      for (int k = 0; k < 3; ++k) qpts[static_cast<int64_t>(p * 3 + k) * S + c] = 0.0;
+      if (qrel) qrel[static_cast<int64_t>(p) * S + c] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    for (int i = 0; i < 3; ++i) vids[i * S + c] = -1 - i;
+    return;
+  }
   int i0 = cells[3 * c], i1 = cells[3 * c + 1], i2 = cells[3 * c + 2];
   double a[3], b[3], d[3];
   for (int k = 0; k < 3; ++k) {
@@ -33,30 +43,34 @@ __global__ void geometry_kernel(const double* __restrict__ points, const int* __
   };
   double diam = fmax(dist(a, b), fmax(dist(a, d), dist(b, d)));
   double rad = fmax(dist(a, cen), fmax(dist(b, cen), dist(d, cen)));
+  const double nrm[3] = {cr[0] / jdet, cr[1] / jdet, cr[2] / jdet};
   double vals[kNumGeomFields] = {a[0], a[1], a[2], t0[0], t0[1], t0[2], t1[0], t1[1], t1[2],
-                                 cr[0] / jdet, cr[1] / jdet, cr[2] / jdet, jdet,
-                                 cen[0], cen[1], cen[2], diam, rad};
-  for (int f = 0; f < kNumGeomFields; ++f) geom[static_cast<int64_t>(f) * n + c] = vals[f];
+                                 nrm[0], nrm[1], nrm[2], jdet,
+                                 cen[0], cen[1], cen[2], diam, rad,
+                                 a[0] * nrm[0] + a[1] * nrm[1] + a[2] * nrm[2]};
+  for (int f = 0; f < kNumGeomFields; ++f) geom[static_cast<int64_t>(f) * S + c] = vals[f];
   for (int p = 0; p < rule.npts; ++p) {
-    double x0 = rule.xi[2 * p], x1 = rule.xi[2 * p + 1];
+    const double x0 = rule.xi[2 * p], x1 = rule.xi[2 * p + 1];
+    float r[3];
     for (int k = 0; k < 3; ++k) {
-      double x = a[k] + x0 * t0[k] + x1 * t1[k];
-      int64_t idx = static_cast<int64_t>(p * 3 + k) * n + c;
-      qpts[idx] = x;
-      if (qrel) qrel[idx] = static_cast<float>(x0 * t0[k] + x1 * t1[k] + (a[k] - cen[k]));
+      qpts[static_cast<int64_t>(p * 3 + k) * S + c] = a[k] + x0 * t0[k] + x1 * t1[k];
+      r[k] = static_cast<float>(x0 * t0[k] + x1 * t1[k] + (a[k] - cen[k]));
     }
+    if (qrel)
+      qrel[static_cast<int64_t>(p) * S + c] =
+          make_float4(r[0], r[1], r[2], fmaf(r[0], r[0], fmaf(r[1], r[1], r[2] * r[2])));
   }
   vids[c] = i0;
-  vids[n + c] = i1;
-  vids[2 * n + c] = i2;
+  vids[S + c] = i1;
+  vids[2 * S + c] = i2;
 }
 
 cudaError_t launch_geometry(const double* points, const int* cells, int ncells,
-                            const RegularRule& rule, double* geom, double* qpts, float* qrel,
+                            const RegularRule& rule, double* geom, double* qpts, float4* qrel,
                             int* vids, cudaStream_t stream) {
   if (ncells <= 0) return cudaSuccess;
   int threads = 128;
-  int blocks = (ncells + threads - 1) / threads;
+  int blocks = (cell_stride(ncells) + threads - 1) / threads;
   geometry_kernel<<<blocks, threads, 0, stream>>>(points, cells, ncells, rule, geom, qpts,
                                                   qrel, vids);
   return cudaGetLastError();

@@ -12,8 +12,12 @@ namespace bempp_b200 {
 
 // Per-cell FP64 geometry, regular quadrature points and vertex ids of a flat-triangle
 // grid (points: npoints x 3 FP64; cells: ncells x 3 int32).
+// Number of regular-kernel blocks since the last call whose shared-memory tile copies
+// did not complete within their bounded wait (and that wrote nothing); resets it.
+cudaError_t take_stage_timeouts(unsigned* count);
+
 cudaError_t launch_geometry(const double* points, const int* cells, int ncells,
-                            const RegularRule& rule, double* geom, double* qpts, float* qrel,
+                            const RegularRule& rule, double* geom, double* qpts, float4* qrel,
                             int* vids, cudaStream_t stream);
 
 // Arithmetic of the regular far-pair quadrature.

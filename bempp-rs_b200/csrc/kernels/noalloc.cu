@@ -9,7 +9,7 @@
 // geometry kernel writes).  This file keeps that scratch in one file-scope
 // `static __device__` array of fixed size, so bempp_assemble_regular_dp0_noalloc
 // allocates nothing on the device (and makes no allocating library call): every GPU that
-// loads the library holds the array (9.6 MB) until the process exits.
+// loads the library holds the array (10.6 MB) until the process exits.
 //
 // The entry point assembles the regular-quadrature matrix between two distinct meshes:
 // every (test cell, trial cell) pair with the regular rule and no singular part, which
@@ -31,10 +31,11 @@ constexpr int kNoAllocMaxPoints = 12;
 constexpr int kMaxDevices = 64;
 
 // Scratch of one mesh, in doubles: geometry fields, FP64 quadrature points, FP32 offsets
-// and int32 vertex ids (both packed two per double).
+// (float4 per point: two doubles) and int32 vertex ids (two per double), with rows of
+// kNoAllocMaxCells cells (a multiple of 32, so every sub-array keeps 256-byte alignment).
 constexpr size_t kGeomDoubles = static_cast<size_t>(kNumGeomFields) * kNoAllocMaxCells;
 constexpr size_t kQptsDoubles = static_cast<size_t>(3) * kNoAllocMaxPoints * kNoAllocMaxCells;
-constexpr size_t kQrelDoubles = kQptsDoubles / 2;
+constexpr size_t kQrelDoubles = static_cast<size_t>(2) * kNoAllocMaxPoints * kNoAllocMaxCells;
 constexpr size_t kVidsDoubles = static_cast<size_t>(3) * kNoAllocMaxCells / 2;
 constexpr size_t kMeshDoubles = kGeomDoubles + kQptsDoubles + kQrelDoubles + kVidsDoubles;
 
@@ -59,12 +60,13 @@ cudaError_t scratch_address(int device, double** out) {
 }
 
 CellSet mesh_scratch(double* base, int ncells, int npts) {
-  // field-major layouts with the mesh's own cell count as stride (see common.cuh)
+  // field-major layouts with the padded stride of common.cuh
   CellSet cs;
   cs.ncells = ncells;
+  cs.stride = cell_stride(ncells);
   double* geom = base;
   double* qpts = geom + kGeomDoubles;
-  float* qrel = reinterpret_cast<float*>(qpts + kQptsDoubles);
+  float4* qrel = reinterpret_cast<float4*>(qpts + kQptsDoubles);
   int* vids = reinterpret_cast<int*>(qpts + kQptsDoubles + kQrelDoubles);
   (void)npts;
   cs.geom = geom;
@@ -96,12 +98,12 @@ cudaError_t assemble_regular_dp0_noalloc(const RegularArgs& args, const RegularR
   CellSet test = mesh_scratch(base, test_ncells, rule.npts);
   CellSet trial = mesh_scratch(base + kMeshDoubles, trial_ncells, rule.npts);
   e = launch_geometry(test_points, test_cells, test_ncells, rule, const_cast<double*>(test.geom),
-                      const_cast<double*>(test.qpts), const_cast<float*>(test.qrel),
+                      const_cast<double*>(test.qpts), const_cast<float4*>(test.qrel),
                       const_cast<int*>(test.vids), stream);
   if (e != cudaSuccess) return e;
   e = launch_geometry(trial_points, trial_cells, trial_ncells, rule,
                       const_cast<double*>(trial.geom), const_cast<double*>(trial.qpts),
-                      const_cast<float*>(trial.qrel), const_cast<int*>(trial.vids), stream);
+                      const_cast<float4*>(trial.qrel), const_cast<int*>(trial.vids), stream);
   if (e != cudaSuccess) return e;
   return launch_regular_dp0(test, trial, rule, args, stream);
 }

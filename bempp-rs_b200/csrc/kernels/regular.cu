@@ -50,6 +50,9 @@ namespace bempp_b200 {
 namespace {
 
 constexpr float kSmallPhaseMax = 0.8f;
+
+// Blocks whose tile copies did not complete within the bounded wait (never expected).
+__device__ unsigned g_stage_timeouts = 0;
 using namespace tiles;
 
 // Curls of the basis functions of a flat cell: t1 d0(phi) - t0 d1(phi); zero for DP0.
@@ -479,7 +482,8 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
   const int nti = min(kTile, test.ncells - ti0), nsj = min(kTile, trial.ncells - sj0);
 
   extern __shared__ __align__(16) unsigned char smem[];
-  unsigned char* cursor = smem;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem);  // completion of the tile copies
+  unsigned char* cursor = smem + 16;
   double* acc_re = nullptr;
   double* acc_im = nullptr;
   int ndt = 0, nds = 0, tdof0 = 0, sdof0 = 0;
@@ -498,15 +502,33 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
   unsigned short* queue = reinterpret_cast<unsigned short*>(cursor);  // kQueue: near pairs
   int* qcount = reinterpret_cast<int*>(cursor + sizeof(unsigned short) * kTile * kTile);
 
-  if (!DIRECT)
+  // Both tiles arrive by bulk (TMA) copies issued by one thread and completed on the
+  // mbarrier, while the other threads clear the accumulator and load local DOF indices.
+  if (threadIdx.x == 0) mbar_init(mbar, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(mbar, 2 * bulk_tile_bytes(Q, kRel));
+    stage_tile_bulk(T, test, ti0, Q, kRel, mbar);
+    stage_tile_bulk(S, trial, sj0, Q, kRel, mbar);
+  }
+  if (!DIRECT) {
     for (int idx = threadIdx.x; idx < ndt * nds; idx += kThreads) {
       acc_re[idx] = 0.0;
       if (kC) acc_im[idx] = 0.0;
     }
+    load_ldof(T, ti0, nti, tt.cell_ldof, NBT);
+    load_ldof(S, sj0, nsj, st.cell_ldof, NBS);
+  }
   if (kQueue && threadIdx.x == 0) *qcount = 0;
-  load_tile(T, test, ti0, nti, Q, kRel, DIRECT ? nullptr : tt.cell_ldof, NBT);
-  load_tile(S, trial, sj0, nsj, Q, kRel, DIRECT ? nullptr : st.cell_ldof, NBS);
-  __syncthreads();
+  const bool staged = mbar_wait_bounded(mbar, 0);
+  if (__syncthreads_or(!staged)) {
+    // the copies did not complete in time: record it, give them a last bounded wait and
+    // leave this block's entries unwritten (the host reports the failure)
+    if (threadIdx.x == 0) atomicAdd(&g_stage_timeouts, 1u);
+    mbar_wait_bounded(mbar, 0);
+    return;
+  }
 
   const int it = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (it < nti) {
@@ -802,7 +824,7 @@ __global__ void __launch_bounds__(kThreads)
 
 size_t smem_bytes(int q, bool rel, bool queue, bool direct, bool cplx, int max_t, int max_s,
                   int nbt, int nbs) {
-  size_t b = 0;
+  size_t b = 16;  // the mbarrier
   if (!direct) b += sizeof(double) * static_cast<size_t>(max_t) * max_s * (cplx ? 2 : 1);
   for (int nb : {nbt, nbs}) {
     b = (b + 15) & ~size_t(15);
@@ -948,6 +970,13 @@ cudaError_t dispatch(const CellSet& test, const SpaceTiles& tt, const CellSet& t
 }  // namespace
 
 int scatter_tile_cells() { return kTile; }
+
+cudaError_t take_stage_timeouts(unsigned* count) {
+  cudaError_t e = cudaMemcpyFromSymbol(count, g_stage_timeouts, sizeof(unsigned));
+  if (e != cudaSuccess || *count == 0) return e;
+  const unsigned zero = 0;
+  return cudaMemcpyToSymbol(g_stage_timeouts, &zero, sizeof(unsigned));
+}
 
 size_t sweep_smem_bytes() {
   size_t b = 0;

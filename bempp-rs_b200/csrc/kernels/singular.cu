@@ -21,7 +21,7 @@ struct CellData {
 };
 
 __device__ __forceinline__ void load_cell(const CellSet& cs, int c, CellData& d) {
-  const int n = cs.ncells;
+  const int n = cs.stride;
   for (int k = 0; k < 3; ++k) {
     d.v0[k] = g(cs.geom, kV0x + k, n, c);
     d.t0[k] = g(cs.geom, kT0x + k, n, c);

@@ -12,10 +12,15 @@ constexpr int kTile = 32;
 constexpr int kThreads = 128;
 constexpr int kWarps = kThreads / 32;
 
+// Geometry rows of a tile: the grid's rows kT0x .. kH, in the same order, so that a tile
+// is staged by copying whole rows.
 enum TileField : int {
-  fJdet = 0, fNx, fNy, fNz, fH, fT0x, fT0y, fT0z, fT1x, fT1y, fT1z, fCx, fCy, fCz, fDiam,
-  fRad, kTileFields
+  fT0x = 0, fT0y, fT0z, fT1x, fT1y, fT1z, fNx, fNy, fNz, fJdet, fCx, fCy, fCz, fDiam, fRad,
+  fH, kTileFields
 };
+static_assert(kH - kT0x + 1 == kTileFields && kNx - kT0x == fNx && kJdet - kT0x == fJdet &&
+                  kCx - kT0x == fCx && kDiam - kT0x == fDiam && kRad - kT0x == fRad,
+              "tile rows mirror the grid's geometry rows");
 
 // Shared-memory image of a tile of kTile cells.
 struct Tile {
@@ -36,8 +41,14 @@ struct Tile {
 __host__ __device__ inline size_t tile_doubles(int q) { return (3 * q + kTileFields) * kTile; }
 __host__ __device__ inline size_t tile_floats(int q, bool mixed) { return mixed ? 4 * q * kTile : 0; }
 __host__ __device__ inline size_t tile_ints(int nb) { return (3 + nb) * kTile; }
+// Bytes of one tile staged by bulk copies (points, geometry, FP32 offsets, vertex ids).
+__host__ __device__ inline unsigned bulk_tile_bytes(int q, bool mixed) {
+  return static_cast<unsigned>(sizeof(double) * tile_doubles(q) + sizeof(float) * tile_floats(q, mixed) +
+                               sizeof(int) * 3 * kTile);
+}
 
-// Carves a tile out of shared memory at *cursor rounded up to 16 bytes.
+// Carves a tile out of shared memory at *cursor rounded up to 16 bytes.  Every row of
+// the tile starts on a 16-byte boundary (the bulk copies' requirement).
 __device__ inline Tile carve_tile(unsigned char*& cursor, int q, bool mixed, int nb) {
   Tile t;
   cursor = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(cursor) + 15) & ~uintptr_t(15));
@@ -54,52 +65,110 @@ __device__ inline Tile carve_tile(unsigned char*& cursor, int q, bool mixed, int
 }
 
 __device__ inline void stage_geo(const Tile& t, int c, const CellSet& cs, int cell) {
-  const int N = cs.ncells;
-  const double nx = g(cs.geom, kNx, N, cell), ny = g(cs.geom, kNy, N, cell),
-               nz = g(cs.geom, kNz, N, cell);
-  t.geo[fJdet * kTile + c] = g(cs.geom, kJdet, N, cell);
-  t.geo[fNx * kTile + c] = nx;
-  t.geo[fNy * kTile + c] = ny;
-  t.geo[fNz * kTile + c] = nz;
-  t.geo[fH * kTile + c] = g(cs.geom, kV0x, N, cell) * nx + g(cs.geom, kV0y, N, cell) * ny +
-                          g(cs.geom, kV0z, N, cell) * nz;
-  for (int f = 0; f < 6; ++f) t.geo[(fT0x + f) * kTile + c] = g(cs.geom, kT0x + f, N, cell);
-  for (int f = 0; f < 3; ++f) t.geo[(fCx + f) * kTile + c] = g(cs.geom, kCx + f, N, cell);
-  t.geo[fDiam * kTile + c] = g(cs.geom, kDiam, N, cell);
-  t.geo[fRad * kTile + c] = g(cs.geom, kRad, N, cell);
+  for (int f = 0; f < kTileFields; ++f) t.geo[f * kTile + c] = g(cs.geom, kT0x + f, cs.stride, cell);
 }
 
+// Local DOF indices of the tile's cells (scatter kernels), by plain loads.
+__device__ inline void load_ldof(const Tile& t, int c0, int n, const uint8_t* cell_ldof, int nb) {
+  for (int idx = threadIdx.x; idx < nb * kTile; idx += kThreads) {
+    const int c = idx % kTile, b = idx / kTile;
+    t.ldof[idx] = cell_ldof ? cell_ldof[(c0 + min(c, n - 1)) * nb + b] : 0;
+  }
+}
+
+// Whole tile by plain loads from all threads (rows of the padded grid arrays; the
+// padding cells of the last tile come along and are never used).
 __device__ inline void load_tile(const Tile& t, const CellSet& cs, int c0, int n, int q, bool mixed,
                           const uint8_t* cell_ldof, int nb) {
-  const int N = cs.ncells;
+  const int64_t S = cs.stride;
   for (int idx = threadIdx.x; idx < 3 * q * kTile; idx += kThreads) {
     const int c = idx % kTile, pd = idx / kTile;
-    t.pts[idx] = __ldg(cs.qpts + static_cast<int64_t>(pd) * N + c0 + min(c, n - 1));
+    t.pts[idx] = __ldg(cs.qpts + pd * S + c0 + c);
   }
   if (mixed)
     for (int idx = threadIdx.x; idx < q * kTile; idx += kThreads) {
       const int c = idx % kTile, p = idx / kTile;
-      const float* src = cs.qrel + static_cast<int64_t>(3 * p) * N + c0 + min(c, n - 1);
-      const float x = __ldg(src), y = __ldg(src + N), z = __ldg(src + 2 * N);
-      t.rel[p * kTile + c] = make_float4(x, y, z, fmaf(x, x, fmaf(y, y, z * z)));
+      t.rel[idx] = __ldg(cs.qrel + p * S + c0 + c);
     }
-  for (int c = threadIdx.x; c < kTile; c += kThreads) {
-    const int cell = c0 + min(c, n - 1);
-    stage_geo(t, c, cs, cell);
-    for (int v = 0; v < 3; ++v) t.vid[v * kTile + c] = c < n ? __ldg(cs.vids + v * N + cell) : -1 - v;
-    for (int b = 0; b < nb; ++b) t.ldof[b * kTile + c] = cell_ldof ? cell_ldof[cell * nb + b] : 0;
+  for (int idx = threadIdx.x; idx < kTileFields * kTile; idx += kThreads) {
+    const int c = idx % kTile, f = idx / kTile;
+    t.geo[idx] = __ldg(cs.geom + (kT0x + f) * S + c0 + c);
   }
+  for (int idx = threadIdx.x; idx < 3 * kTile; idx += kThreads) {
+    const int c = idx % kTile, v = idx / kTile;
+    t.vid[idx] = __ldg(cs.vids + v * S + c0 + c);
+  }
+  load_ldof(t, c0, n, cell_ldof, nb);
 }
 
 // One cell's FP64 quadrature points and geometry into column c of a tile (the staging of
 // a single lane).
 __device__ inline void stage_cell(const Tile& t, int c, const CellSet& cs, int cell, int q) {
-  const int N = cs.ncells;
-  for (int pd = 0; pd < 3 * q; ++pd)
-    t.pts[pd * kTile + c] = __ldg(cs.qpts + static_cast<int64_t>(pd) * N + cell);
+  const int64_t S = cs.stride;
+  for (int pd = 0; pd < 3 * q; ++pd) t.pts[pd * kTile + c] = __ldg(cs.qpts + pd * S + cell);
   stage_geo(t, c, cs, cell);
 }
 
+// ---- tile staging by bulk (TMA) copies, completed on a shared-memory mbarrier ----
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* m, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(m)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* m, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(m)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* m, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_addr(m)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Waits for the mbarrier phase with the given parity, giving up after a bounded number
+// of polls (each poll suspends for a hardware-defined interval): true when it completed.
+__device__ inline bool mbar_wait_bounded(uint64_t* m, unsigned parity) {
+  for (int i = 0; i < (1 << 22); ++i)
+    if (mbar_try_wait(m, parity)) return true;
+  return false;
+}
+
+// One 1-D bulk copy global -> shared; both addresses 16-byte aligned, size a multiple of
+// 16 bytes; its bytes complete a transaction on the mbarrier.
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes, uint64_t* m) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(m))
+      : "memory");
+}
+
+// Issues the bulk copies of one tile (one thread): every row is 32 cells starting at a
+// multiple of 32 of a padded grid array, so sources are 256-byte aligned.
+__device__ inline void stage_tile_bulk(const Tile& t, const CellSet& cs, int c0, int q, bool mixed,
+                                       uint64_t* m) {
+  const int64_t S = cs.stride;
+  for (int pd = 0; pd < 3 * q; ++pd)
+    bulk_copy(t.pts + pd * kTile, cs.qpts + pd * S + c0, sizeof(double) * kTile, m);
+  for (int f = 0; f < kTileFields; ++f)
+    bulk_copy(t.geo + f * kTile, cs.geom + (kT0x + f) * S + c0, sizeof(double) * kTile, m);
+  if (mixed)
+    for (int p = 0; p < q; ++p)
+      bulk_copy(t.rel + p * kTile, cs.qrel + p * S + c0, sizeof(float4) * kTile, m);
+  for (int v = 0; v < 3; ++v) bulk_copy(t.vid + v * kTile, cs.vids + v * S + c0, sizeof(int) * kTile, m);
+}
 
 // ---- FP32 helpers of the mixed-precision paths ----
 

@@ -62,6 +62,14 @@ FLOPS_PER_PAIR = {
     ("helmholtz", "single_layer", "dp0"): 720,
 }
 
+# DRAM bytes (read + write) per launch of the dominant regular kernel, from one ncu capture
+# of the full-size workload (profiles/dram_traffic_laplace_p1_ico5_fp64.md).
+DRAM_TRAFFIC_PER_LAUNCH = {
+    ("laplace", "double_layer", "p1", 20480): 906.63e6 + 845.16e6,
+    ("laplace", "adjoint_double_layer", "p1", 20480): 903.91e6 + 841.06e6,
+    ("laplace", "hypersingular", "p1", 20480): 904.41e6 + 841.18e6,
+}
+
 WORKLOADS = {
     "p1": dict(name="laplace_dl_adl_hs_p1_ico5_f64", kernel="laplace", space="p1", level=5,
                perturb=True, k=0.0,
@@ -589,7 +597,9 @@ def run_ours(args):
     roofline = {
         "bound": "fp64", "kernel": f"regular kernel, {w['kernel']} {dom} ({w['space']})",
         "achieved": ach, "peak": peak, "unit": "TFLOP/s",
-        "frac": (ach / peak) if (ach and peak) else None, "traffic": None,
+        "frac": (ach / peak) if (ach and peak) else None,
+        "traffic": DRAM_TRAFFIC_PER_LAUNCH.get((w["kernel"], dom, w["space"], len(wl.cells))),
+        "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
         "peak_source": "measured FP64 FMA-chain probe (bempp_measure_fma_peak) on this GPU; "
                        "MEASURED_PEAKS.json has no FP64 CUDA-core figure",
         "regular_pairs": nreg, "per_operator": per_op,
