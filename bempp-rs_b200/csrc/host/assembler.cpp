@@ -24,7 +24,8 @@ namespace bempp_b200 {
 
 void build_singular_pairs(GridT& g, SingularPairList& out);
 void build_tiles(const SpaceT& s, int tile, std::vector<int>& off, std::vector<int>& dofs,
-                 std::vector<uint8_t>& ldof, int& max_dofs);
+                 std::vector<uint8_t>& ldof, int& max_dofs, std::vector<uint8_t>& inc_off,
+                 std::vector<uint8_t>& inc_ent);
 int scatter_tile_cells();
 cudaError_t launch_convert_to_single(const double* src, void* dst, size_t n_reals,
                                      cudaStream_t stream);
@@ -150,7 +151,10 @@ void ensure_space_device(SpaceT& s, int device) {
   std::vector<int> off, tdofs;
   std::vector<uint8_t> ldof;
   s.tile_cells = scatter_tile_cells();
-  build_tiles(s, s.tile_cells, off, tdofs, ldof, s.max_tile_dofs);
+  std::vector<uint8_t> inc_off, inc_ent;
+  build_tiles(s, s.tile_cells, off, tdofs, ldof, s.max_tile_dofs, inc_off, inc_ent);
+  s.d_tile_inc_off.upload(inc_off);
+  s.d_tile_inc_ent.upload(inc_ent);
   s.ntiles = static_cast<int>(off.size()) - 1;
   s.d_tile_off.upload(off);
   s.d_tile_dofs.upload(tdofs);
@@ -178,6 +182,8 @@ SpaceTiles space_tiles(const SpaceT& s) {
   t.tile_dof_off = s.d_tile_off.as<int>();
   t.tile_dofs = s.d_tile_dofs.as<int>();
   t.cell_ldof = s.d_cell_ldof.as<uint8_t>();
+  t.inc_off = s.d_tile_inc_off.as<uint8_t>();
+  t.inc_ent = s.d_tile_inc_ent.as<uint8_t>();
   return t;
 }
 

@@ -173,6 +173,7 @@ struct SpaceT {
   int device = -1;
   DeviceBuffer d_dofs;                                   // int32 ncells x nbasis
   DeviceBuffer d_tile_off, d_tile_dofs, d_cell_ldof;     // tile-scatter layout
+  DeviceBuffer d_tile_inc_off, d_tile_inc_ent;           // and its DOF incidence
   int ntiles = 0, max_tile_dofs = 0, tile_cells = 0;
   std::map<int, bempp_b200::ColumnRuns> chunk_runs;  // by number of chunks
   std::mutex mu;

@@ -182,8 +182,13 @@ void build_singular_pairs(GridT& g, SingularPairList& out) {
 
 // Tile layout for the scatter kernel: tiles of `tile` consecutive cells, their sorted
 // unique DOFs, and each cell's DOFs as indices into its tile's list.
+// Also the incidence of each tile's local DOFs: for local DOF d of tile t, the entries
+// inc_ent[t * 3 * tile + k], k in [inc_off[t * (3 * tile + 1) + d], ... + d + 1), each
+// b * tile + c for the cell c of the tile whose local basis function b is DOF d (cells
+// ascending, then b).
 void build_tiles(const SpaceT& s, int tile, std::vector<int>& off, std::vector<int>& dofs,
-                 std::vector<uint8_t>& ldof, int& max_dofs) {
+                 std::vector<uint8_t>& ldof, int& max_dofs, std::vector<uint8_t>& inc_off,
+                 std::vector<uint8_t>& inc_ent) {
   const int64_t nc = s.grid->ncells;
   const int nb = s.nbasis;
   const int ntiles = static_cast<int>((nc + tile - 1) / tile);
@@ -191,7 +196,9 @@ void build_tiles(const SpaceT& s, int tile, std::vector<int>& off, std::vector<i
   dofs.clear();
   ldof.assign(nc * nb, 0);
   max_dofs = 0;
-  std::vector<int> local;
+  inc_off.assign(static_cast<size_t>(ntiles) * (3 * tile + 1), 0);
+  inc_ent.assign(static_cast<size_t>(ntiles) * 3 * tile, 0);
+  std::vector<int> local, count;
   for (int t = 0; t < ntiles; ++t) {
     const int64_t c0 = static_cast<int64_t>(t) * tile, c1 = std::min<int64_t>(c0 + tile, nc);
     local.clear();
@@ -208,6 +215,18 @@ void build_tiles(const SpaceT& s, int tile, std::vector<int>& off, std::vector<i
     dofs.insert(dofs.end(), local.begin(), local.end());
     off[t + 1] = static_cast<int>(dofs.size());
     max_dofs = std::max<int>(max_dofs, static_cast<int>(local.size()));
+    // incidence (counting sort of the tile's (cell, basis) entries by local DOF)
+    const int nd = static_cast<int>(local.size());
+    uint8_t* io = &inc_off[static_cast<size_t>(t) * (3 * tile + 1)];
+    uint8_t* ie = &inc_ent[static_cast<size_t>(t) * 3 * tile];
+    count.assign(nd + 1, 0);
+    for (int64_t c = c0; c < c1; ++c)
+      for (int b = 0; b < nb; ++b) ++count[ldof[c * nb + b] + 1];
+    for (int d = 0; d < nd; ++d) count[d + 1] += count[d];
+    for (int d = 0; d <= nd; ++d) io[d] = static_cast<uint8_t>(count[d]);
+    for (int64_t c = c0; c < c1; ++c)
+      for (int b = 0; b < nb; ++b)
+        ie[count[ldof[c * nb + b]]++] = static_cast<uint8_t>(b * tile + (c - c0));
   }
 }
 

@@ -71,6 +71,10 @@ struct SpaceTiles {
   const int* tile_dof_off;  // ntiles + 1
   const int* tile_dofs;     // global DOF numbers of each tile, ascending
   const uint8_t* cell_ldof; // ncells * nbasis local (in-tile) DOF indices
+  // incidence of the local DOFs: per tile (3 * tile_cells + 1) offsets and 3 * tile_cells
+  // entries b * tile_cells + c, grouped by local DOF
+  const uint8_t* inc_off = nullptr;
+  const uint8_t* inc_ent = nullptr;
 };
 
 // Any pair of spaces: per-tile shared-memory accumulation, then atomic adds into a

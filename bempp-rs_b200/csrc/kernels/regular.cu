@@ -473,6 +473,10 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
   constexpr bool kC = KER == kHelmholtz;
   constexpr bool kQueue = MIXED && NM == kNearInKernel;
   constexpr bool kRel = MIXED;  // FP32 offsets staged
+  // P1 (or DP1) test space: the lanes' local blocks go through a per-warp stage and are
+  // summed per test DOF (lane = DOF) before the accumulator, so that no two lanes of a
+  // warp update the same entry (test cells share vertex DOFs)
+  constexpr bool kGather = !DIRECT && NBT == 3;
   const int Q = QT > 0 ? QT : rule.npts;
   const int tx = blockIdx.x, sy = blockIdx.y + tile_y0;
   const int moff = NM == kNearMasked
@@ -497,6 +501,19 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
     acc_im = acc_re + cap;
     cursor += sizeof(double) * cap * (kC ? 2 : 1);
   }
+  double* stage_re = nullptr;  // kGather: [warp][(a * NBS + b) * kTile + lane]
+  double* stage_im = nullptr;
+  uint8_t* inc_off = nullptr;  // kGather: the test tile's DOF incidence
+  uint8_t* inc_ent = nullptr;
+  if (kGather) {
+    constexpr int kStage = kWarps * kTile * NBT * NBS;
+    stage_re = reinterpret_cast<double*>(cursor);
+    stage_im = stage_re + kStage;
+    cursor += sizeof(double) * kStage * (kC ? 2 : 1);
+    inc_off = cursor;
+    inc_ent = cursor + 3 * kTile + 1;
+    cursor += 6 * kTile + 1;
+  }
   const Tile T = carve_tile(cursor, Q, kRel, NBT);
   const Tile S = carve_tile(cursor, Q, kRel, NBS);
   unsigned short* queue = reinterpret_cast<unsigned short*>(cursor);  // kQueue: near pairs
@@ -519,6 +536,10 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
     }
     load_ldof(T, ti0, nti, tt.cell_ldof, NBT);
     load_ldof(S, sj0, nsj, st.cell_ldof, NBS);
+    if (kGather)
+      for (int i = threadIdx.x; i < 6 * kTile + 1; i += kThreads)
+        inc_off[i] = i <= 3 * kTile ? __ldg(tt.inc_off + static_cast<int64_t>(tx) * (3 * kTile + 1) + i)
+                                    : __ldg(tt.inc_ent + static_cast<int64_t>(tx) * 3 * kTile + i - (3 * kTile + 1));
   }
   if (kQueue && threadIdx.x == 0) *qcount = 0;
   const bool staged = mbar_wait_bounded(mbar, 0);
@@ -531,17 +552,23 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
   }
 
   const int it = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (it < nti) {
-    const int a0 = T.vid[it], a1 = T.vid[kTile + it], a2 = T.vid[2 * kTile + it];
-    const unsigned mword = (NM != kNearInKernel && moff >= 0)
-                               ? __ldg(near.masks + static_cast<int64_t>(moff) * kTile + it)
-                               : 0u;
-    for (int js = warp; js < nsj; js += kWarps) {
+  const bool lane_cell = it < nti;
+  int a0 = -1, a1 = -2, a2 = -3;
+  unsigned mword = 0u;
+  if (lane_cell) {
+    a0 = T.vid[it];
+    a1 = T.vid[kTile + it];
+    a2 = T.vid[2 * kTile + it];
+    if (NM != kNearInKernel && moff >= 0)
+      mword = __ldg(near.masks + static_cast<int64_t>(moff) * kTile + it);
+  }
+  for (int js = warp; js < nsj; js += kWarps) {  // warp-uniform trip count
+    double ore[NBT][NBS], oim[NBT][NBS];
+    bool have = false;
+    if (lane_cell) {
       const int64_t o = static_cast<int64_t>(sj0 + js) * ld + ti0 + it;
-      const bool marked = (mword >> js) & 1u;
-      double ore[NBT][NBS], oim[NBT][NBS];
       const bool skip = NM == kNearMasked
-                            ? marked
+                            ? ((mword >> js) & 1u) != 0u
                             : same_grid && share_vertex(a0, a1, a2, S.vid[js], S.vid[kTile + js],
                                                         S.vid[2 * kTile + js]);
       if (skip) {
@@ -554,26 +581,57 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
           else
             out[o] = 0.0;
         }
-        continue;
-      }
-      if (MIXED) {
-        if (kQueue && near_pair(T, it, S, js)) {
-          const int slot = atomicAdd(qcount, 1);
-          queue[slot] = static_cast<unsigned short>(it | (js << 8));
-          continue;
-        }
-        block_fp32<QT, KER, OP, NBT, NBS, PH>(T, it, S, js, rule, k, ore, oim);
+      } else if (kQueue && near_pair(T, it, S, js)) {
+        const int slot = atomicAdd(qcount, 1);
+        queue[slot] = static_cast<unsigned short>(it | (js << 8));
       } else {
-        block_fp64<QT, KER, OP, NBT, NBS>(T, it, S, js, rule, k, ore, oim);
-      }
-      if (DIRECT) {
-        if (kC)
-          reinterpret_cast<double2*>(out)[o] = make_double2(ore[0][0], oim[0][0]);
+        if (MIXED)
+          block_fp32<QT, KER, OP, NBT, NBS, PH>(T, it, S, js, rule, k, ore, oim);
         else
-          out[o] = ore[0][0];
-      } else {
-        deposit<NBT, NBS, kC>(acc_re, acc_im, ndt, T, it, S, js, ore, oim);
+          block_fp64<QT, KER, OP, NBT, NBS>(T, it, S, js, rule, k, ore, oim);
+        have = true;
+        if (DIRECT) {
+          if (kC)
+            reinterpret_cast<double2*>(out)[o] = make_double2(ore[0][0], oim[0][0]);
+          else
+            out[o] = ore[0][0];
+        } else if (!kGather) {
+          deposit<NBT, NBS, kC>(acc_re, acc_im, ndt, T, it, S, js, ore, oim);
+        }
       }
+    }
+    if (kGather) {
+      double* sr = stage_re + warp * (kTile * NBT * NBS);
+      double* si = stage_im + warp * (kTile * NBT * NBS);
+#pragma unroll
+      for (int a = 0; a < NBT; ++a)
+#pragma unroll
+        for (int b = 0; b < NBS; ++b) {
+          sr[(a * NBS + b) * kTile + it] = have ? ore[a][b] : 0.0;
+          if (kC) si[(a * NBS + b) * kTile + it] = have ? oim[a][b] : 0.0;
+        }
+      __syncwarp();
+      for (int d = it; d < ndt; d += kTile) {
+        double g_re[NBS], g_im[NBS];
+#pragma unroll
+        for (int b = 0; b < NBS; ++b) g_re[b] = g_im[b] = 0.0;
+        for (int e = inc_off[d]; e < inc_off[d + 1]; ++e) {
+          const int ab = inc_ent[e];  // a * kTile + cell
+          const int a = ab >> 5, c = ab & (kTile - 1);
+#pragma unroll
+          for (int b = 0; b < NBS; ++b) {
+            g_re[b] += sr[(a * NBS + b) * kTile + c];
+            if (kC) g_im[b] += si[(a * NBS + b) * kTile + c];
+          }
+        }
+#pragma unroll
+        for (int b = 0; b < NBS; ++b) {
+          const int idx = d + ndt * S.ldof[b * kTile + js];
+          atomicAdd(acc_re + idx, g_re[b]);
+          if (kC) atomicAdd(acc_im + idx, g_im[b]);
+        }
+      }
+      __syncwarp();
     }
   }
   if (kQueue) {
@@ -826,6 +884,8 @@ size_t smem_bytes(int q, bool rel, bool queue, bool direct, bool cplx, int max_t
                   int nbt, int nbs) {
   size_t b = 16;  // the mbarrier
   if (!direct) b += sizeof(double) * static_cast<size_t>(max_t) * max_s * (cplx ? 2 : 1);
+  if (!direct && nbt == 3)  // stage and DOF incidence of the gather
+    b += sizeof(double) * kWarps * kTile * nbt * nbs * (cplx ? 2 : 1) + 6 * kTile + 1;
   for (int nb : {nbt, nbs}) {
     b = (b + 15) & ~size_t(15);
     b += sizeof(double) * tile_doubles(q) + sizeof(float) * tile_floats(q, rel) +
