@@ -477,6 +477,10 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
   // summed per test DOF (lane = DOF) before the accumulator, so that no two lanes of a
   // warp update the same entry (test cells share vertex DOFs)
   constexpr bool kGather = !DIRECT && NBT == 3;
+  // real FP64 P1 blocks (not the hypersingular kernel, which keeps 5 CTAs per SM; not the
+  // mixed kernels, whose larger tiles would then limit the CTAs per SM): one accumulator
+  // per warp, updated with plain adds, summed at the flush
+  constexpr int kAcc = (kGather && !kC && !MIXED && OP != kHS) ? kWarps : 1;
   const int Q = QT > 0 ? QT : rule.npts;
   const int tx = blockIdx.x, sy = blockIdx.y + tile_y0;
   const int moff = NM == kNearMasked
@@ -490,16 +494,16 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
   unsigned char* cursor = smem + 16;
   double* acc_re = nullptr;
   double* acc_im = nullptr;
-  int ndt = 0, nds = 0, tdof0 = 0, sdof0 = 0;
+  int ndt = 0, nds = 0, tdof0 = 0, sdof0 = 0, cap = 0;
   if (!DIRECT) {
     tdof0 = tt.tile_dof_off[tx];
     ndt = tt.tile_dof_off[tx + 1] - tdof0;
     sdof0 = st.tile_dof_off[sy];
     nds = st.tile_dof_off[sy + 1] - sdof0;
-    const int cap = tt.max_tile_dofs * st.max_tile_dofs;
+    cap = tt.max_tile_dofs * st.max_tile_dofs;
     acc_re = reinterpret_cast<double*>(cursor);
     acc_im = acc_re + cap;
-    cursor += sizeof(double) * cap * (kC ? 2 : 1);
+    cursor += sizeof(double) * cap * (kC ? 2 : 1) * kAcc;
   }
   double* stage_re = nullptr;  // kGather: [warp][(a * NBS + b) * kTile + lane]
   double* stage_im = nullptr;
@@ -530,10 +534,11 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
     stage_tile_bulk(S, trial, sj0, Q, kRel, mbar);
   }
   if (!DIRECT) {
-    for (int idx = threadIdx.x; idx < ndt * nds; idx += kThreads) {
-      acc_re[idx] = 0.0;
-      if (kC) acc_im[idx] = 0.0;
-    }
+    for (int w = 0; w < kAcc; ++w)
+      for (int idx = threadIdx.x; idx < ndt * nds; idx += kThreads) {
+        acc_re[w * cap + idx] = 0.0;
+        if (kC) acc_im[idx] = 0.0;
+      }
     load_ldof(T, ti0, nti, tt.cell_ldof, NBT);
     load_ldof(S, sj0, nsj, st.cell_ldof, NBS);
     if (kGather)
@@ -627,8 +632,12 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
 #pragma unroll
         for (int b = 0; b < NBS; ++b) {
           const int idx = d + ndt * S.ldof[b * kTile + js];
-          atomicAdd(acc_re + idx, g_re[b]);
-          if (kC) atomicAdd(acc_im + idx, g_im[b]);
+          if (kAcc > 1) {
+            acc_re[warp * cap + idx] += g_re[b];  // this warp's copy; distinct per lane
+          } else {
+            atomicAdd(acc_re + idx, g_re[b]);
+            if (kC) atomicAdd(acc_im + idx, g_im[b]);
+          }
         }
       }
       __syncwarp();
@@ -659,7 +668,9 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
     for (int idx = threadIdx.x; idx < ndt * nds; idx += kThreads) {
       const int a = idx % ndt, b = idx / ndt;
       const int64_t o = static_cast<int64_t>(sdofs[b]) * ld + tdofs[a];
-      const double re = acc_re[idx];
+      double re = acc_re[idx];
+#pragma unroll
+      for (int w = 1; w < kAcc; ++w) re += acc_re[w * cap + idx];
       if (kC) {
         const double im = acc_im[idx];
         if (re != 0.0 || im != 0.0) {
@@ -881,9 +892,9 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 size_t smem_bytes(int q, bool rel, bool queue, bool direct, bool cplx, int max_t, int max_s,
-                  int nbt, int nbs) {
+                  int nbt, int nbs, int acc_copies) {
   size_t b = 16;  // the mbarrier
-  if (!direct) b += sizeof(double) * static_cast<size_t>(max_t) * max_s * (cplx ? 2 : 1);
+  if (!direct) b += sizeof(double) * static_cast<size_t>(max_t) * max_s * (cplx ? 2 : 1) * acc_copies;
   if (!direct && nbt == 3)  // stage and DOF incidence of the gather
     b += sizeof(double) * kWarps * kTile * nbt * nbs * (cplx ? 2 : 1) + 6 * kTile + 1;
   for (int nb : {nbt, nbs}) {
@@ -900,8 +911,10 @@ template <int QT, int KER, int OP, int NBT, int NBS, bool MIXED, bool DIRECT, in
 cudaError_t launch_mode(const CellSet& test, const SpaceTiles& tt, const CellSet& trial,
                         const SpaceTiles& st, const RegularRule& rule, const RegularArgs& a,
                         int ty0, int ty1, cudaStream_t stream) {
+  constexpr int kAcc = (!DIRECT && NBT == 3 && KER != kHelmholtz && !MIXED && OP != kHS) ? kWarps : 1;
   const size_t smem = smem_bytes(rule.npts, MIXED, MIXED && NM == kNearInKernel, DIRECT,
-                                 KER == kHelmholtz, tt.max_tile_dofs, st.max_tile_dofs, NBT, NBS);
+                                 KER == kHelmholtz, tt.max_tile_dofs, st.max_tile_dofs, NBT, NBS,
+                                 kAcc);
   auto fn = regular_tiles<QT, KER, OP, NBT, NBS, MIXED, DIRECT, PH, NM>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
