@@ -286,6 +286,8 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
   ra.op = a.op;
   ra.k = a.k;
   ra.same_grid = same_grid ? 1 : 0;
+  // one space on both sides and a symmetric kernel: lower-triangle tile pairs, mirrored
+  ra.symmetric = (&trial == &test && same_grid && (a.op == kSL || a.op == kHS)) ? 1 : 0;
   ra.precision = a.options.precision == 1 ? kRegularMixed : kRegularFP64;
   ra.out_type = cplx ? kOutC128 : kOutF64;
   ra.ld = nt;

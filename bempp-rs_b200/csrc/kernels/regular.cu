@@ -454,6 +454,31 @@ __device__ __forceinline__ void deposit(double* acc_re, double* acc_im, int ndt,
   }
 }
 
+// Tile pair of block b of a lower-triangle launch: pairs (tx, sy) with sy in [ty0, ...) and
+// tx in [sy, ntt), row by row: row m (sy = ty0 + m) starts at m L - m (m - 1) / 2, with
+// L = ntt - ty0 the first row's length.
+__device__ __forceinline__ void lower_tile_pair(int b, int ntt, int ty0, int& tx, int& sy) {
+  const long long L = ntt - ty0, B = b;
+  const double twoL1 = 2.0 * static_cast<double>(L) + 1.0;
+  long long m = static_cast<long long>((twoL1 - sqrt(twoL1 * twoL1 - 8.0 * static_cast<double>(B))) * 0.5);
+  auto start = [&](long long r) { return r * L - r * (r - 1) / 2; };
+  if (m < 0) m = 0;
+  while (m > 0 && start(m) > B) --m;
+  while (m + 1 < L && start(m + 1) <= B) ++m;
+  sy = ty0 + static_cast<int>(m);
+  tx = sy + static_cast<int>(B - start(m));
+}
+
+template <bool kC>
+__device__ __forceinline__ void mirror_put(double* mir, int it, int js, double re, double im) {
+  if (kC) {
+    mir[2 * (js * (kTile + 1) + it)] = re;
+    mir[2 * (js * (kTile + 1) + it) + 1] = im;
+  } else {
+    mir[js * (kTile + 1) + it] = re;
+  }
+}
+
 // Near-pair handling of a launch.  kNearInKernel: every pair is tested in the kernel and
 // near pairs are queued in shared memory and integrated in FP64 after the main loop (the
 // FP64 kernels skip the test); kNearMasked: the pairs marked in the near-field masks are
@@ -469,7 +494,7 @@ template <int QT, int KER, int OP, int NBT, int NBS, bool MIXED, bool DIRECT, in
 __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
     regular_tiles(CellSet test, SpaceTiles tt, CellSet trial, SpaceTiles st, RegularRule rule,
                   double k, int same_grid, double* __restrict__ out, int64_t ld, int tile_y0,
-                  int tile_y1, NearArgs near) {
+                  int tile_y1, NearArgs near, int symmetric) {
   constexpr bool kC = KER == kHelmholtz;
   constexpr bool kQueue = MIXED && NM == kNearInKernel;
   constexpr bool kRel = MIXED;  // FP32 offsets staged
@@ -482,7 +507,16 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
   // per warp, updated with plain adds, summed at the flush
   constexpr int kAcc = (kGather && !kC && !MIXED && OP != kHS) ? kWarps : 1;
   const int Q = QT > 0 ? QT : rule.npts;
-  const int tx = blockIdx.x, sy = blockIdx.y + tile_y0;
+  // symmetric operator on one space (single layer, hypersingular): only the tile pairs with
+  // tx >= sy are computed, the blocks with tx > sy also written transposed
+  int tx, sy;
+  if (symmetric) {
+    lower_tile_pair(blockIdx.x, (test.ncells + kTile - 1) / kTile, tile_y0, tx, sy);
+  } else {
+    tx = blockIdx.x;
+    sy = blockIdx.y + tile_y0;
+  }
+  const bool mirror = symmetric && tx > sy;
   const int moff = NM == kNearMasked
                        ? __ldg(near.tile_mask + static_cast<int64_t>(tx) * near.trial_tiles + sy)
                        : -1;
@@ -520,6 +554,10 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
   }
   const Tile T = carve_tile(cursor, Q, kRel, NBT);
   const Tile S = carve_tile(cursor, Q, kRel, NBS);
+  // DIRECT, symmetric: the block's entries, [js * (kTile + 1) + it], for the transposed
+  // write; padded rows keep both access patterns free of bank conflicts
+  double* mir = reinterpret_cast<double*>(cursor);
+  if (DIRECT && symmetric) cursor += sizeof(double) * kTile * (kTile + 1) * (kC ? 2 : 1);
   unsigned short* queue = reinterpret_cast<unsigned short*>(cursor);  // kQueue: near pairs
   int* qcount = reinterpret_cast<int*>(cursor + sizeof(unsigned short) * kTile * kTile);
 
@@ -585,6 +623,7 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
             reinterpret_cast<double2*>(out)[o] = make_double2(0.0, 0.0);
           else
             out[o] = 0.0;
+          if (mirror) mirror_put<kC>(mir, it, js, 0.0, 0.0);
         }
       } else if (kQueue && near_pair(T, it, S, js)) {
         const int slot = atomicAdd(qcount, 1);
@@ -600,6 +639,7 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
             reinterpret_cast<double2*>(out)[o] = make_double2(ore[0][0], oim[0][0]);
           else
             out[o] = ore[0][0];
+          if (mirror) mirror_put<kC>(mir, it, js, ore[0][0], oim[0][0]);
         } else if (!kGather) {
           deposit<NBT, NBS, kC>(acc_re, acc_im, ndt, T, it, S, js, ore, oim);
         }
@@ -656,9 +696,27 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
           reinterpret_cast<double2*>(out)[o] = make_double2(ore[0][0], oim[0][0]);
         else
           out[o] = ore[0][0];
+        if (mirror) mirror_put<kC>(mir, pi, pj, ore[0][0], oim[0][0]);
       } else {
         deposit<NBT, NBS, kC>(acc_re, acc_im, ndt, T, pi, S, pj, ore, oim);
       }
+    }
+  }
+  if (DIRECT && mirror) {
+    // the transposed block, entry (row sj0 + j, column ti0 + i), j fastest: coalesced
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kTile * kTile; idx += kThreads) {
+      const int i = idx / kTile, j = idx % kTile;
+      if (i >= nti || j >= nsj) continue;
+      if (NM == kNearMasked && moff >= 0 &&
+          ((__ldg(near.masks + static_cast<int64_t>(moff) * kTile + i) >> j) & 1u))
+        continue;  // a near or vertex-sharing pair: written by the near-pair / singular kernels
+      const int64_t o = static_cast<int64_t>(ti0 + i) * ld + sj0 + j;
+      if (kC)
+        reinterpret_cast<double2*>(out)[o] =
+            make_double2(mir[2 * (j * (kTile + 1) + i)], mir[2 * (j * (kTile + 1) + i) + 1]);
+      else
+        out[o] = mir[j * (kTile + 1) + i];
     }
   }
   if (!DIRECT) {
@@ -671,14 +729,21 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
       double re = acc_re[idx];
 #pragma unroll
       for (int w = 1; w < kAcc; ++w) re += acc_re[w * cap + idx];
+      // symmetric, tx > sy: the same value at the transposed entry
+      const int64_t om = static_cast<int64_t>(tdofs[a]) * ld + sdofs[b];
       if (kC) {
         const double im = acc_im[idx];
         if (re != 0.0 || im != 0.0) {
           atomicAdd(out + 2 * o, re);
           atomicAdd(out + 2 * o + 1, im);
+          if (mirror) {
+            atomicAdd(out + 2 * om, re);
+            atomicAdd(out + 2 * om + 1, im);
+          }
         }
       } else if (re != 0.0) {
         atomicAdd(out + o, re);
+        if (mirror) atomicAdd(out + om, re);
       }
     }
   }
@@ -892,9 +957,10 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 size_t smem_bytes(int q, bool rel, bool queue, bool direct, bool cplx, int max_t, int max_s,
-                  int nbt, int nbs, int acc_copies) {
+                  int nbt, int nbs, int acc_copies, bool mirror) {
   size_t b = 16;  // the mbarrier
   if (!direct) b += sizeof(double) * static_cast<size_t>(max_t) * max_s * (cplx ? 2 : 1) * acc_copies;
+  if (direct && mirror) b += sizeof(double) * kTile * (kTile + 1) * (cplx ? 2 : 1) + 16;
   if (!direct && nbt == 3)  // stage and DOF incidence of the gather
     b += sizeof(double) * kWarps * kTile * nbt * nbs * (cplx ? 2 : 1) + 6 * kTile + 1;
   for (int nb : {nbt, nbs}) {
@@ -914,14 +980,23 @@ cudaError_t launch_mode(const CellSet& test, const SpaceTiles& tt, const CellSet
   constexpr int kAcc = (!DIRECT && NBT == 3 && KER != kHelmholtz && !MIXED && OP != kHS) ? kWarps : 1;
   const size_t smem = smem_bytes(rule.npts, MIXED, MIXED && NM == kNearInKernel, DIRECT,
                                  KER == kHelmholtz, tt.max_tile_dofs, st.max_tile_dofs, NBT, NBS,
-                                 kAcc);
+                                 kAcc, a.symmetric != 0);
   auto fn = regular_tiles<QT, KER, OP, NBT, NBS, MIXED, DIRECT, PH, NM>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  const dim3 grid((test.ncells + kTile - 1) / kTile, ty1 - ty0);
+  const int ntt = (test.ncells + kTile - 1) / kTile;
+  dim3 grid(ntt, ty1 - ty0);
+  if (a.symmetric) {
+    // tile pairs (tx >= sy) of trial tiles [ty0, ty1), one row per trial tile
+    const long long L = ntt - ty0, rows = ty1 - ty0;
+    const long long count = rows * L - rows * (rows - 1) / 2;
+    if (count > 0x7fffffffLL) return cudaErrorInvalidValue;
+    grid = dim3(static_cast<unsigned>(count), 1);
+  }
   fn<<<grid, kThreads, smem, stream>>>(test, tt, trial, st, rule, a.k, a.same_grid,
-                                       static_cast<double*>(a.out), a.ld, ty0, ty1, a.near);
+                                       static_cast<double*>(a.out), a.ld, ty0, ty1, a.near,
+                                       a.symmetric);
   return cudaGetLastError();
 }
 

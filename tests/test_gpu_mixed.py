@@ -62,3 +62,19 @@ def test_mixed_p1_matches_oracle(kernel, op, k):
     o = oracle_assemble(grid, kernel, op, k, test=sp, trial=sp)
     err = rel_err(a, o)
     assert 1e-13 < err <= MIXED_TOL
+
+
+@pytest.mark.parametrize("kernel,op,k,sp", [
+    ("helmholtz", "single_layer", 8.0, (0, False)),
+    ("laplace", "hypersingular", 0.0, (1, True)),
+])
+def test_mixed_one_space_symmetric(kernel, op, k, sp):
+    """The mixed path with the lower-triangle (mirrored) tile pairs of one space object."""
+    pts, cells = shapes.icosphere(3)
+    grid = Grid(shapes.radial_perturbation(pts, seed=12), cells)
+    a = gpu_assemble(grid, kernel, op, k, test=sp, trial=sp, precision=Precision.Mixed,
+                     one_space=True)
+    o = oracle_assemble(grid, kernel, op, k, test=sp, trial=sp)
+    err = rel_err(a, o)
+    assert 1e-13 < err <= MIXED_TOL
+

@@ -31,7 +31,9 @@ def rel_err(a, b):
 
 
 def gpu_assemble(grid, kernel, op, k=0.0, test=(0, False), trial=(0, False), q=6, order=4,
-                 precision=Precision.FP64, dtype=None):
+                 precision=Precision.FP64, dtype=None, one_space=False):
+    """Dense matrix from the GPU assembler.  one_space: test and trial are the same space
+    object, which lets symmetric operators (SL, HS) compute half of the tile pairs."""
     opts = BoundaryAssemblerOptions()
     opts.set_regular_quadrature_degree(ReferenceCellType.Triangle, q)
     opts.set_singular_quadrature_degree(ReferenceCellType.Triangle, ReferenceCellType.Triangle,
@@ -42,7 +44,8 @@ def gpu_assemble(grid, kernel, op, k=0.0, test=(0, False), trial=(0, False), q=6
         return function_space(grid, create_family(
             Family.Lagrange, deg, Continuity.Standard if cont else Continuity.Discontinuous))
 
-    ts, ss = space(*test), space(*trial)
+    ts = space(*test)
+    ss = ts if one_space else space(*trial)
     if kernel == "laplace":
         a = create_laplace_assembler(OPS[op], opts, dtype or np.float64)
     else:
@@ -155,3 +158,22 @@ def test_singular_csr_matches_dense():
                 dense = a.assemble(ss, ts)
                 for i, j, v in zip(csr.row, csr.col, csr.data):
                     assert np.isclose(dense[i, j], v)
+
+
+@pytest.mark.parametrize("kernel,op,k,sp", [
+    ("laplace", "single_layer", 0.0, (0, False)),
+    ("laplace", "single_layer", 0.0, (1, True)),
+    ("laplace", "hypersingular", 0.0, (1, True)),
+    ("helmholtz", "single_layer", 5.0, (0, False)),
+    ("helmholtz", "hypersingular", 5.0, (1, True)),
+])
+def test_one_space_symmetric_operators_match_oracle(kernel, op, k, sp):
+    """Single layer and hypersingular on one space object: only tile pairs (tx >= sy) are
+    computed and the rest is mirrored; the matrix matches the oracle (which computes every
+    pair; its far-pair entries are symmetric to rounding)."""
+    pts, cells = shapes.icosphere(3)
+    grid = Grid(shapes.radial_perturbation(pts, seed=11), cells)
+    a = gpu_assemble(grid, kernel, op, k, test=sp, trial=sp, one_space=True)
+    o = oracle_assemble(grid, kernel, op, k, test=sp, trial=sp)
+    assert rel_err(a, o) <= FP64_TOL
+
