@@ -61,7 +61,9 @@ long long count_items(SweepArgs& a, int kchunk) {
   long long total = 0;
   for (int m = 0; m < a.nmesh; ++m) {
     a.mesh[m].item_begin = total;
-    total += static_cast<long long>(a.mesh[m].ntiles) * a.mesh[m].ntiles * nchunks;
+    // tile pairs (test tile >= trial tile): the kernel mirrors the single layer
+    const long long nt = a.mesh[m].ntiles;
+    total += nt * (nt + 1) / 2 * nchunks;
   }
   a.nitems = total;
   return total;

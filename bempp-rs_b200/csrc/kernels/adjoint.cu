@@ -49,7 +49,12 @@ __global__ void __launch_bounds__(kThreads, 3)
                        const double2* __restrict__ mu, double* __restrict__ grad_cell,
                        double* __restrict__ totals) {
   const int Q = QT > 0 ? QT : rule.npts;
-  const int ti0 = blockIdx.x * kTile, sj0 = blockIdx.y * kTile;
+  // A_ij = A_ji on far pairs (one cell set and one rule on both sides), so only tile pairs
+  // tx >= sy are visited; an off-diagonal tile takes c_ij + c_ji for both orders of its pairs
+  int tx, sy;
+  lower_tile_pair(blockIdx.x, (cs.ncells + kTile - 1) / kTile, 0, tx, sy);
+  const bool both = tx > sy;
+  const int ti0 = tx * kTile, sj0 = sy * kTile;
   const int nti = min(kTile, cs.ncells - ti0), nsj = min(kTile, cs.ncells - sj0);
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned char* cursor = smem;
@@ -66,6 +71,7 @@ __global__ void __launch_bounds__(kThreads, 3)
   const int it = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool valid = it < nti;
   const double2 li = valid ? lam[ti0 + it] : make_double2(0.0, 0.0);
+  const double2 mi = valid && both ? mu[ti0 + it] : make_double2(0.0, 0.0);
   const int a0 = T.vid[it], a1 = T.vid[kTile + it], a2 = T.vid[2 * kTile + it];
   const double jdet_i = T.G(fJdet, it);
 
@@ -75,9 +81,14 @@ __global__ void __launch_bounds__(kThreads, 3)
     const bool adjacent = share_vertex(a0, a1, a2, S.vid[js], S.vid[kTile + js],
                                        S.vid[2 * kTile + js]);
     const bool active = valid && !adjacent;
-    // c = conj(lambda_i) mu_j
+    // c = conj(lambda_i) mu_j (+ conj(lambda_j) mu_i off the diagonal)
     const double2 mj = mu[sj0 + js];
-    const double c_re = li.x * mj.x + li.y * mj.y, c_im = li.x * mj.y - li.y * mj.x;
+    double c_re = li.x * mj.x + li.y * mj.y, c_im = li.x * mj.y - li.y * mj.x;
+    if (both) {
+      const double2 lj = lam[sj0 + js];
+      c_re += lj.x * mi.x + lj.y * mi.y;
+      c_im += lj.x * mi.y - lj.y * mi.x;
+    }
     double S0_re = 0.0, S0_im = 0.0, Sk_re = 0.0, Sk_im = 0.0;
     double uq[QT > 0 ? QT : kMaxRegularPoints][3];
 #pragma unroll
@@ -408,7 +419,9 @@ cudaError_t launch_adjoint_sl(const CellSet& cs, const RegularRule& rule,
   const size_t smem = 2 * (sizeof(double) * tile_doubles(rule.npts) +
                            sizeof(float) * tile_floats(rule.npts, mixed) + sizeof(int) * tile_ints(1) + 16) +
                       sizeof(double) * (2 * kTile * 9 + 2) + 16;
-  dim3 grid((cs.ncells + kTile - 1) / kTile, (cs.ncells + kTile - 1) / kTile);
+  const long long ntt = (cs.ncells + kTile - 1) / kTile;
+  if (ntt * (ntt + 1) / 2 > 0x7fffffffLL) return cudaErrorInvalidValue;
+  const dim3 grid(static_cast<unsigned>(ntt * (ntt + 1) / 2));  // tile pairs tx >= sy
   const double2* l2 = reinterpret_cast<const double2*>(lam);
   const double2* m2 = reinterpret_cast<const double2*>(mu);
   auto fn = rule.npts == 6 ? (mixed ? adjoint_sl_regular<6, true> : adjoint_sl_regular<6, false>)

@@ -454,21 +454,6 @@ __device__ __forceinline__ void deposit(double* acc_re, double* acc_im, int ndt,
   }
 }
 
-// Tile pair of block b of a lower-triangle launch: pairs (tx, sy) with sy in [ty0, ...) and
-// tx in [sy, ntt), row by row: row m (sy = ty0 + m) starts at m L - m (m - 1) / 2, with
-// L = ntt - ty0 the first row's length.
-__device__ __forceinline__ void lower_tile_pair(int b, int ntt, int ty0, int& tx, int& sy) {
-  const long long L = ntt - ty0, B = b;
-  const double twoL1 = 2.0 * static_cast<double>(L) + 1.0;
-  long long m = static_cast<long long>((twoL1 - sqrt(twoL1 * twoL1 - 8.0 * static_cast<double>(B))) * 0.5);
-  auto start = [&](long long r) { return r * L - r * (r - 1) / 2; };
-  if (m < 0) m = 0;
-  while (m > 0 && start(m) > B) --m;
-  while (m + 1 < L && start(m + 1) <= B) ++m;
-  sy = ty0 + static_cast<int>(m);
-  tx = sy + static_cast<int>(B - start(m));
-}
-
 template <bool kC>
 __device__ __forceinline__ void mirror_put(double* mir, int it, int js, double re, double im) {
   if (kC) {
@@ -806,8 +791,12 @@ __global__ void __launch_bounds__(kThreads)
 // first), stages the two tiles once, and for each wavenumber of its chunk writes the
 // complete 32 x 32 block of complex64 entries: far pairs in FP32 (block_fp32), near pairs
 // in FP64 (block_fp64), vertex-sharing pairs by their Duffy rule in FP64 (one warp per
-// pair).  No two items write the same entry, so the launch needs no ordering or atomics
-// on the output; the only shared state is the item counter (reset before every launch).
+// pair).  The single layer is symmetric on one mesh, so only tile pairs (test tile >=
+// trial tile) are items: an off-diagonal item also writes the transposed block (through
+// shared memory, coalesced), whose vertex-sharing entries take their own Duffy rule (the
+// rules of the two orders of a pair differ).  No two items write the same entry, so the
+// launch needs no ordering or atomics on the output; the only shared state is the item
+// counter (reset before every launch).
 
 // Adjacency configuration (0..27, the order of singular_configurations()) of two cells
 // with vertex ids a[3] (test) and b[3] (trial) that share at least one vertex.
@@ -880,6 +869,7 @@ __global__ void __launch_bounds__(kThreads)
   unsigned char* adjc = reinterpret_cast<unsigned char*>(adjq + kTile * kTile);
   int* counts = reinterpret_cast<int*>(adjc + kTile * kTile);  // near, adjacent
   long long* s_item = reinterpret_cast<long long*>(counts + 2);
+  float2* mir = reinterpret_cast<float2*>(s_item + 1);  // [js * (kTile + 1) + it]
   const int it = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (;;) {
     if (threadIdx.x == 0) {
@@ -895,8 +885,9 @@ __global__ void __launch_bounds__(kThreads)
     const long long local = item - M.item_begin;
     const int nchunks = (a.nk + a.kchunk - 1) / a.kchunk;
     const int kc = static_cast<int>(local % nchunks);
-    const long long tp = local / nchunks;
-    const int tt = static_cast<int>(tp / M.ntiles), st = static_cast<int>(tp % M.ntiles);
+    int tt, st;
+    lower_tile_pair(static_cast<int>(local / nchunks), M.ntiles, 0, tt, st);
+    const bool mirror = tt > st;
     const int nc = M.cells.ncells;
     const int ti0 = tt * kTile, sj0 = st * kTile;
     const int nti = min(kTile, nc - ti0), nsj = min(kTile, nc - sj0);
@@ -932,16 +923,18 @@ __global__ void __launch_bounds__(kThreads)
             continue;
           double ore[1][1], oim[1][1];
           block_fp32<6, kHelmholtz, kSL, 1, 1, kPhaseRuntime>(T, it, S, js, rule, k, ore, oim);
-          out[static_cast<long long>(sj0 + js) * nc + ti0 + it] =
-              make_float2(static_cast<float>(ore[0][0]), static_cast<float>(oim[0][0]));
+          const float2 v = make_float2(static_cast<float>(ore[0][0]), static_cast<float>(oim[0][0]));
+          out[static_cast<long long>(sj0 + js) * nc + ti0 + it] = v;
+          if (mirror) mir[js * (kTile + 1) + it] = v;
         }
       }
       for (int e = threadIdx.x; e < nnear; e += kThreads) {
         const int pi = nearq[e] & 0xff, pj = nearq[e] >> 8;
         double ore[1][1], oim[1][1];
         block_fp64<6, kHelmholtz, kSL, 1, 1, false>(T, pi, S, pj, rule, k, ore, oim);
-        out[static_cast<long long>(sj0 + pj) * nc + ti0 + pi] =
-            make_float2(static_cast<float>(ore[0][0]), static_cast<float>(oim[0][0]));
+        const float2 v = make_float2(static_cast<float>(ore[0][0]), static_cast<float>(oim[0][0]));
+        out[static_cast<long long>(sj0 + pj) * nc + ti0 + pi] = v;
+        if (mirror) mir[pj * (kTile + 1) + pi] = v;
       }
       for (int e = warp; e < nadj; e += kWarps) {
         const int pi = adjq[e] & 0xff, pj = adjq[e] >> 8;
@@ -950,6 +943,24 @@ __global__ void __launch_bounds__(kThreads)
         if (it == 0)
           out[static_cast<long long>(sj0 + pj) * nc + ti0 + pi] =
               make_float2(static_cast<float>(re), static_cast<float>(im));
+        if (mirror) {
+          // the transposed pair: trial cell pj as the test cell, its own configuration
+          const int av[3] = {S.vid[pj], S.vid[kTile + pj], S.vid[2 * kTile + pj]};
+          const int bv[3] = {T.vid[pi], T.vid[kTile + pi], T.vid[2 * kTile + pi]};
+          duffy_sl_dp0_warp(S, pj, T, pi, adjacency_config(av, bv, false), rules, k, re, im);
+          if (it == 0)
+            mir[pj * (kTile + 1) + pi] = make_float2(static_cast<float>(re), static_cast<float>(im));
+        }
+      }
+      if (mirror) {
+        // the transposed block, entry (row sj0 + j, column ti0 + i), j fastest: coalesced
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < kTile * kTile; idx += kThreads) {
+          const int i = idx / kTile, j = idx % kTile;
+          if (i < nti && j < nsj)
+            out[static_cast<long long>(ti0 + i) * nc + sj0 + j] = mir[j * (kTile + 1) + i];
+        }
+        __syncthreads();  // mir is reused by the next wavenumber
       }
     }
     __syncthreads();  // the tiles and queues are reused by the next item
@@ -1134,7 +1145,7 @@ size_t sweep_smem_bytes() {
     b = (b + 15) & ~size_t(15);
   }
   return b + 2 * sizeof(unsigned short) * kTile * kTile + kTile * kTile + 2 * sizeof(int) +
-         sizeof(long long) + 32;
+         sizeof(long long) + sizeof(float2) * kTile * (kTile + 1) + 32;
 }
 
 cudaError_t launch_sweep_sl(const SweepArgs& args, const RegularRule& rule,

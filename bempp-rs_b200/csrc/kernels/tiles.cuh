@@ -228,5 +228,20 @@ __device__ __forceinline__ void phase_cos_sin(double theta, float& c, float& s) 
   s = (q == 0) ? sr : (q == 1) ? cr : (q == 2) ? -sr : -cr;
 }
 
+// Tile pair of block b of a lower-triangle launch: pairs (tx, sy) with sy in [ty0, ...) and
+// tx in [sy, ntt), row by row: row m (sy = ty0 + m) starts at m L - m (m - 1) / 2, with
+// L = ntt - ty0 the first row's length.
+__device__ __forceinline__ void lower_tile_pair(int b, int ntt, int ty0, int& tx, int& sy) {
+  const long long L = ntt - ty0, B = b;
+  const double twoL1 = 2.0 * static_cast<double>(L) + 1.0;
+  long long m = static_cast<long long>((twoL1 - sqrt(twoL1 * twoL1 - 8.0 * static_cast<double>(B))) * 0.5);
+  auto start = [&](long long r) { return r * L - r * (r - 1) / 2; };
+  if (m < 0) m = 0;
+  while (m > 0 && start(m) > B) --m;
+  while (m + 1 < L && start(m + 1) <= B) ++m;
+  sy = ty0 + static_cast<int>(m);
+  tx = sy + static_cast<int>(B - start(m));
+}
+
 }  // namespace tiles
 }  // namespace bempp_b200
