@@ -307,6 +307,14 @@ BemppStatus bempp_measure_fma_peak(int fp64, int iters, int reps, double* tflops
   });
 }
 
+long long bempp_lower_tile_pairs(int ntt, int ty0, int ty1, int* tx, int* sy,
+                                 long long capacity) {
+  if (ntt < 0 || ty0 < 0 || ty1 < ty0 || ty1 > ntt) return -1;
+  const long long n = lower_tile_pair_count(ntt, ty0, ty1);
+  for (long long b = 0; b < n && b < capacity; ++b) lower_tile_pair(b, ntt, ty0, ty1, tx[b], sy[b]);
+  return n;
+}
+
 // ------------------------------------------------------------ page-locked outputs ---
 // A cache of page-locked blocks: cudaHostAlloc'ing a gigabyte takes hundreds of
 // milliseconds, so freed blocks are kept for the next result of a similar size (a block
@@ -367,6 +375,8 @@ size_t bempp_host_trim(void) {
   g_host_free_bytes = 0;
   return released;
 }
+
+size_t bempp_device_trim(void) { return device_cache_trim(); }
 
 // ---------------------------------------------------------------------- matrices ---
 size_t matrix_shape0(MatrixT* m) { return m ? m->rows : 0; }

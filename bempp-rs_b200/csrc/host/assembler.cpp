@@ -107,7 +107,7 @@ const GridGeometry& grid_geometry(GridT& g, int device, const RegularRule& rule,
     const size_t S = static_cast<size_t>(cell_stride(static_cast<int>(n)));  // padded rows
     geo->geom.alloc(sizeof(double) * kNumGeomFields * S);
     geo->qpts.alloc(sizeof(double) * 3 * rule.npts * S);
-    geo->qrel.alloc(sizeof(float4) * rule.npts * S);
+    geo->qrel.alloc(sizeof(float4) * qrel_rows(rule.npts) * S);
     geo->vids.alloc(sizeof(int) * 3 * S);
     BEMPP_CUDA(launch_geometry(g.d_points.as<double>(), g.d_cells.as<int>(),
                                static_cast<int>(n), rule, geo->geom.as<double>(),
@@ -329,7 +329,6 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
     sa.out = out;
     sa.unique_entries = dp0 ? 1 : 0;
     sa.pair_values = nullptr;
-    sa.fast = ra.precision == kRegularMixed ? 1 : 0;
   }
   auto run_singular = [&](int lo, int hi, cudaStream_t s) {
     sa.trial_lo = lo;

@@ -46,6 +46,15 @@ void clear_last_error();
                                 std::string(#call) + ": " + cudaGetErrorString(e_));    \
   } while (0)
 
+// Process-wide cache of device blocks behind every DeviceBuffer (device_cache.cpp): a
+// freed block is kept for the next request of a similar size on its device, so that
+// building and freeing grids and spaces again and again makes no cudaMalloc / cudaFree
+// calls (driver calls that can stall behind other processes' allocations).  Returning a
+// block waits for the device to finish its work, as cudaFree does.
+cudaError_t device_cache_alloc(void** ptr, size_t bytes);
+void device_cache_free(void* ptr);
+size_t device_cache_trim();  // releases every cached free block; returns the bytes
+
 // Owning device buffer.
 struct DeviceBuffer {
   void* ptr = nullptr;
@@ -55,7 +64,7 @@ struct DeviceBuffer {
   DeviceBuffer& operator=(const DeviceBuffer&) = delete;
   ~DeviceBuffer() { reset(); }
   void reset() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) device_cache_free(ptr);
     ptr = nullptr;
     bytes = 0;
   }
@@ -63,7 +72,7 @@ struct DeviceBuffer {
     if (n <= bytes && ptr) return;
     reset();
     if (n == 0) return;
-    BEMPP_CUDA(cudaMalloc(&ptr, n));
+    BEMPP_CUDA(device_cache_alloc(&ptr, n));
     bytes = n;
   }
   template <typename T>

@@ -2,8 +2,9 @@
 // launch over many wavenumbers and meshes of uneven size (the regular.cu kernel
 // sweep_sl_dp0), with a small autotuner.
 //
-// Plan.  Work items are (mesh, test tile, trial tile, chunk of wavenumbers), the largest
-// mesh's items first so the dynamic item counter ends with short items.  The launch is
+// Plan.  Work items are (mesh, chunk of wavenumbers, tile pair test tile >= trial tile:
+// the kernel mirrors the symmetric single layer), the largest mesh's items first so the
+// dynamic item counter ends with short items.  The launch is
 // captured once per plan (counter reset + kernel) and replayed with cudaGraphLaunch.
 //
 // Autotuner.  The two free parameters are the wavenumbers per work item (k-chunk: more

@@ -52,7 +52,8 @@ __global__ void __launch_bounds__(kThreads, 3)
   // A_ij = A_ji on far pairs (one cell set and one rule on both sides), so only tile pairs
   // tx >= sy are visited; an off-diagonal tile takes c_ij + c_ji for both orders of its pairs
   int tx, sy;
-  lower_tile_pair(blockIdx.x, (cs.ncells + kTile - 1) / kTile, 0, tx, sy);
+  const int ntt = (cs.ncells + kTile - 1) / kTile;
+  lower_tile_pair(blockIdx.x, ntt, 0, ntt, tx, sy);
   const bool both = tx > sy;
   const int ti0 = tx * kTile, sj0 = sy * kTile;
   const int nti = min(kTile, cs.ncells - ti0), nsj = min(kTile, cs.ncells - sj0);

@@ -34,6 +34,10 @@ enum GeomField : int {
 __host__ __device__ inline int cell_stride(int n) { return (n + 31) & ~31; }
 
 constexpr int kMaxRegularPoints = 37;
+
+// Rows of FP32 offsets of an npts-point rule: points in pairs (a zero point completes an
+// odd rule), so that packed FP32x2 arithmetic reads two trial points per 128-bit load.
+__host__ __device__ inline int qrel_rows(int npts) { return (npts + 1) & ~1; }
 constexpr double kInv4Pi = 0.079577471545947667884;
 
 // Regular (non-singular) rule on the reference triangle (0,0),(1,0),(0,1), passed by
@@ -62,7 +66,9 @@ struct CellSet {
   int stride;           // cell_stride(ncells)
   const double* geom;   // kNumGeomFields * stride
   const double* qpts;   // npts * 3 * stride
-  const float4* qrel;   // npts * stride (mixed precision only)
+  const float4* qrel;   // qrel_rows(npts) * stride (mixed precision only), points in pairs:
+                        // row 2j (x_2j, x_2j+1, y_2j, y_2j+1), row 2j+1 (z_2j, z_2j+1,
+                        // |.|^2_2j, |.|^2_2j+1) of the FP32 offsets from the centroid
   const int* vids;      // 3 * stride
 };
 
@@ -96,17 +102,11 @@ __device__ __forceinline__ double rsqrt_refined(double a) {
   return fma(y * e, fma(e, 0.375, 0.5), y);
 }
 
-// sin(t) and cos(t) in FP64 for moderate |t| (the phases k r of boundary-element
-// kernels): Cody-Waite reduction r = t - n pi/2 with pi/2 split into two doubles (each
-// step one fused multiply-add), Taylor series of cos and sin on |r| <= pi/4 up to r^16
-// and r^17 (truncation below 1e-19), and the quadrant's exchange of sine and cosine.
-// Absolute error about 1e-16 for |t| up to 1e5 (checked against libm on [-40, 40]).
-__device__ __forceinline__ void sincos_cw(double t, double& s, double& c) {
-  const double n = rint(t * 0.63661977236758134308);
-  double r = fma(-n, 1.5707963267948966192, t);
-  r = fma(-n, 6.1232339957367660359e-17, r);
+// sin(r) and cos(r) in FP64 for |r| <= pi/4: Taylor series up to r^17 and r^16
+// (truncation below 1e-19).
+__device__ __forceinline__ void sincos_taylor(double r, double& sr, double& cr) {
   const double z = r * r;
-  double cr = 1.0 / 20922789888000.0;  // 1/16!
+  cr = 1.0 / 20922789888000.0;  // 1/16!
   cr = fma(cr, z, -1.0 / 87178291200.0);
   cr = fma(cr, z, 1.0 / 479001600.0);
   cr = fma(cr, z, -1.0 / 3628800.0);
@@ -115,7 +115,7 @@ __device__ __forceinline__ void sincos_cw(double t, double& s, double& c) {
   cr = fma(cr, z, 1.0 / 24.0);
   cr = fma(cr, z, -0.5);
   cr = fma(cr, z, 1.0);
-  double sr = 1.0 / 355687428096000.0;  // 1/17!
+  sr = 1.0 / 355687428096000.0;  // 1/17!
   sr = fma(sr, z, -1.0 / 1307674368000.0);
   sr = fma(sr, z, 1.0 / 6227020800.0);
   sr = fma(sr, z, -1.0 / 39916800.0);
@@ -124,6 +124,19 @@ __device__ __forceinline__ void sincos_cw(double t, double& s, double& c) {
   sr = fma(sr, z, 1.0 / 120.0);
   sr = fma(sr, z, -1.0 / 6.0);
   sr = r * fma(sr, z, 1.0);
+}
+
+// sin(t) and cos(t) in FP64 for moderate |t| (the phases k r of boundary-element
+// kernels): Cody-Waite reduction r = t - n pi/2 with pi/2 split into two doubles (each
+// step one fused multiply-add), sincos_taylor on |r| <= pi/4, and the quadrant's exchange
+// of sine and cosine.  Absolute error about 1e-16 for |t| up to 1e5 (checked against libm
+// on [-40, 40]).
+__device__ __forceinline__ void sincos_cw(double t, double& s, double& c) {
+  const double n = rint(t * 0.63661977236758134308);
+  double r = fma(-n, 1.5707963267948966192, t);
+  r = fma(-n, 6.1232339957367660359e-17, r);
+  double sr, cr;
+  sincos_taylor(r, sr, cr);
   const int q = static_cast<int>(static_cast<long long>(n) & 3);
   c = (q == 0) ? cr : (q == 1) ? -sr : (q == 2) ? -cr : sr;
   s = (q == 0) ? sr : (q == 1) ? cr : (q == 2) ? -sr : -cr;

@@ -1,7 +1,7 @@
 // Per-cell geometry of flat triangles: the affine map x(xi) = v0 + xi0 t0 + xi1 t1, its
 // Jacobian columns, unit normal, Jacobian determinant |t0 x t1|, centroid, diameter and
 // the physical regular quadrature points (FP64, plus FP32 offsets from the centroid for
-// the mixed-precision kernels).  Restates the ndgrid geometry map that bempp-rs calls at
+// the mixed-precision kernels, stored in pairs of points: CellSet::qrel).  Restates the ndgrid geometry map that bempp-rs calls at
 // src/boundary_assemblers/cell_pair_assemblers.rs:87-108,224-236 for degree-1 cells.
 #include "launch.h"
 
@@ -16,10 +16,11 @@ __global__ void geometry_kernel(const double* __restrict__ points, const int* __
   if (c >= S) return;
   if (c >= n) {  // padding of the last tile
     for (int f = 0; f < kNumGeomFields; ++f) geom[static_cast<int64_t>(f) * S + c] = 0.0;
-    for (int p = 0; p < rule.npts; ++p) {
+    for (int p = 0; p < rule.npts; ++p)
       for (int k = 0; k < 3; ++k) qpts[static_cast<int64_t>(p * 3 + k) * S + c] = 0.0;
-      if (qrel) qrel[static_cast<int64_t>(p) * S + c] = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
+    if (qrel)
+      for (int r = 0; r < qrel_rows(rule.npts); ++r)
+        qrel[static_cast<int64_t>(r) * S + c] = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int i = 0; i < 3; ++i) vids[i * S + c] = -1 - i;
     return;
   }
@@ -49,16 +50,25 @@ __global__ void geometry_kernel(const double* __restrict__ points, const int* __
                                  cen[0], cen[1], cen[2], diam, rad,
                                  a[0] * nrm[0] + a[1] * nrm[1] + a[2] * nrm[2]};
   for (int f = 0; f < kNumGeomFields; ++f) geom[static_cast<int64_t>(f) * S + c] = vals[f];
-  for (int p = 0; p < rule.npts; ++p) {
-    const double x0 = rule.xi[2 * p], x1 = rule.xi[2 * p + 1];
-    float r[3];
-    for (int k = 0; k < 3; ++k) {
-      qpts[static_cast<int64_t>(p * 3 + k) * S + c] = a[k] + x0 * t0[k] + x1 * t1[k];
-      r[k] = static_cast<float>(x0 * t0[k] + x1 * t1[k] + (a[k] - cen[k]));
+  for (int p = 0; p < qrel_rows(rule.npts); ++p) {
+    float r[4] = {0.f, 0.f, 0.f, 0.f};  // the zero point completing an odd rule
+    if (p < rule.npts) {
+      const double x0 = rule.xi[2 * p], x1 = rule.xi[2 * p + 1];
+      for (int k = 0; k < 3; ++k) {
+        qpts[static_cast<int64_t>(p * 3 + k) * S + c] = a[k] + x0 * t0[k] + x1 * t1[k];
+        r[k] = static_cast<float>(x0 * t0[k] + x1 * t1[k] + (a[k] - cen[k]));
+      }
+      r[3] = fmaf(r[0], r[0], fmaf(r[1], r[1], r[2] * r[2]));
     }
-    if (qrel)
-      qrel[static_cast<int64_t>(p) * S + c] =
-          make_float4(r[0], r[1], r[2], fmaf(r[0], r[0], fmaf(r[1], r[1], r[2] * r[2])));
+    if (qrel) {
+      // point p is half (p & 1) of the pair rows 2 (p / 2), 2 (p / 2) + 1
+      float* row0 = reinterpret_cast<float*>(qrel + static_cast<int64_t>(p & ~1) * S + c);
+      float* row1 = reinterpret_cast<float*>(qrel + static_cast<int64_t>((p & ~1) + 1) * S + c);
+      row0[p & 1] = r[0];
+      row0[2 + (p & 1)] = r[1];
+      row1[p & 1] = r[2];
+      row1[2 + (p & 1)] = r[3];
+    }
   }
   vids[c] = i0;
   vids[S + c] = i1;

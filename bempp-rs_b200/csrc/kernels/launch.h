@@ -7,6 +7,7 @@
 #include <stdint.h>
 
 #include "common.cuh"
+#include "tile_order.h"
 
 namespace bempp_b200 {
 
@@ -111,7 +112,6 @@ struct SingularArgs {
   void* out;          // dense column-major output (added into), or null
   int unique_entries; // 1 when every pair owns its entry (DP0 x DP0): plain stores
   double* pair_values;  // if non-null: per-pair local blocks (nbt * nbs [*2 complex])
-  int fast = 0;             // mixed-precision assembly: own FP64 rsqrt / sincos (Helmholtz)
   int trial_lo = 0;         // only pairs whose trial cell lies in [trial_lo, trial_hi)
   int trial_hi = 0x7fffffff;
 };

@@ -338,6 +338,116 @@ __device__ __forceinline__ void far_sums(const Tile& T, int it, const Tile& S, i
   }
 }
 
+// far_sums for rules with an even number of points and no phase reduction (Laplace, or
+// Helmholtz with |k (r - r0)| <= 0.8): trial points 2j and 2j + 1 go through packed FP32x2
+// instructions together (each half rounded as the scalar operation), which halves the
+// issue slots of the inner loop; both points arrive in two 128-bit shared-memory loads
+// (the paired layout of the FP32 offsets).  Even and odd trial points are summed
+// separately and added per test point.
+template <int QT, int KER, int OP, int NBT, int NBS>
+__device__ __forceinline__ void far_sums_x2(const Tile& T, int it, const Tile& S, int js,
+                                            const RegularRule& rule, const FarPair<QT>& fp,
+                                            float blk_re[NBT][NBS], float blk_im[NBT][NBS],
+                                            float& S_re, float& S_im) {
+  static_assert(QT > 0 && QT % 2 == 0, "pairs of trial points");
+  constexpr bool kC = KER == kHelmholtz;
+  constexpr bool kNeedBasis = OP != kHS || kC;
+  constexpr bool kKahan = NBT == 1 && NBS == 1;
+  float cmp_re = 0.f, cmp_im = 0.f;
+  const float2 r0sq2 = f2(fp.r0sq), r0f2 = f2(fp.r0f), kf2 = f2(fp.kf), nkf2 = f2(-fp.kf);
+#pragma unroll 1
+  for (int p = 0; p < QT; ++p) {
+    const float4 a = T.R4(p, it);
+    const float apf = OP == kDL ? fmaf(rule.uf[p], fp.fa1, fmaf(rule.vf[p], fp.fa2, fp.fa0)) : 1.f;
+    // s_pq = A_p + |y_q|^2 + w_p . y_q; Laplace adds |dc|^2 so that it is r^2 itself
+    const float2 wx = f2(fmaf(-2.f, a.x, fp.m2dx)), wy = f2(fmaf(-2.f, a.y, fp.m2dy)),
+                 wz = f2(fmaf(-2.f, a.z, fp.m2dz));
+    const float2 Ap = f2(fmaf(-a.x, fp.m2dx, fmaf(-a.y, fp.m2dy, fmaf(-a.z, fp.m2dz,
+                                                                     a.w + (kC ? 0.f : fp.r0sq)))));
+    float2 u_re[NBS], u_im[NBS], g_re = f2(0.f), g_im = f2(0.f);
+#pragma unroll
+    for (int b = 0; b < NBS; ++b) u_re[b] = u_im[b] = f2(0.f);
+#pragma unroll
+    for (int j = 0; j < QT / 2; ++j) {
+      const float4 A = S.RA(j, js), B = S.RB(j, js);  // the same address in every lane
+      const float2 wq = OP != kADL ? make_float2(rule.wf[2 * j], rule.wf[2 * j + 1])
+                                   : make_float2(fp.wq[2 * j], fp.wq[2 * j + 1]);
+      const float2 s = ffma2(wx, make_float2(A.x, A.y),
+                             ffma2(wy, make_float2(A.z, A.w),
+                                   ffma2(wz, make_float2(B.x, B.y), fadd2(Ap, make_float2(B.z, B.w)))));
+      float2 f, c = f2(1.f), sn = f2(0.f);  // kernel value = f (c + i sn)
+      if (!kC) {
+        const float2 rinv = rsqrt_approx2(s);  // s is r^2 here
+        f = (OP == kSL || OP == kHS) ? fmul2(wq, rinv) : fmul2(wq, fmul2(fmul2(rinv, rinv), rinv));
+      } else {
+        const float2 r2 = fadd2(r0sq2, s);
+        const float2 rinv = rsqrt_approx2(r2);
+        const float2 t = fmul2(fmul2(kf2, s), rcp_approx2(ffma2(r2, rinv, r0f2)));  // k (r - r0)
+        float2 cs, ss;
+        poly_cos_sin2(t, cs, ss);
+        if (OP == kSL || OP == kHS) {
+          f = fmul2(wq, rinv);
+          c = cs;
+          sn = ss;
+        } else {
+          // (1 - ik r) e^{ik r} / r^3 with e^{ik r0} applied per pair
+          const float2 rr = fmul2(r2, rinv);
+          f = fmul2(wq, fmul2(fmul2(rinv, rinv), rinv));
+          c = ffma2(fmul2(kf2, rr), ss, cs);
+          sn = ffma2(fmul2(nkf2, rr), cs, ss);
+        }
+      }
+      if (OP == kHS) {
+        if (kC) {
+          g_re = ffma2(f, c, g_re);
+          g_im = ffma2(f, sn, g_im);
+        } else {
+          g_re = fadd2(g_re, f);
+        }
+      }
+      if (kNeedBasis) {
+        if (NBS == 1) {
+          if (kC) {
+            u_re[0] = ffma2(f, c, u_re[0]);
+            u_im[0] = ffma2(f, sn, u_im[0]);
+          } else {
+            u_re[0] = fadd2(u_re[0], f);
+          }
+        } else {
+          const float2 kre = kC ? fmul2(f, c) : f, kim = fmul2(f, sn);
+#pragma unroll
+          for (int b = 0; b < NBS; ++b) {
+            const float2 phi = make_float2(rule.phif[b][2 * j], rule.phif[b][2 * j + 1]);
+            u_re[b] = ffma2(kre, phi, u_re[b]);
+            if (kC) u_im[b] = ffma2(kim, phi, u_im[b]);
+          }
+        }
+      }
+    }
+    if (OP == kHS) {
+      S_re = fmaf(rule.wf[p], g_re.x + g_re.y, S_re);
+      if (kC) S_im = fmaf(rule.wf[p], g_im.x + g_im.y, S_im);
+    }
+    if (kNeedBasis) {
+      const float wp = rule.wf[p] * apf;
+      if (kKahan) {
+        kahan_add(blk_re[0][0], cmp_re, wp * (u_re[0].x + u_re[0].y));
+        if (kC) kahan_add(blk_im[0][0], cmp_im, wp * (u_im[0].x + u_im[0].y));
+      } else {
+#pragma unroll
+        for (int a = 0; a < NBT; ++a) {
+          const float fa = NBT == 1 ? wp : wp * rule.phif[a][p];
+#pragma unroll
+          for (int b = 0; b < NBS; ++b) {
+            blk_re[a][b] = fmaf(fa, u_re[b].x + u_re[b].y, blk_re[a][b]);
+            if (kC) blk_im[a][b] = fmaf(fa, u_im[b].x + u_im[b].y, blk_im[a][b]);
+          }
+        }
+      }
+    }
+  }
+}
+
 // Phase handling of a launch (Helmholtz far pairs): kPhaseRuntime chooses per warp,
 // kPhaseSmall assumes |k (r - r0)| <= 0.8 for every pair of the launch (the host checks
 // k (max rad_x + max rad_y) <= 0.8), kPhaseGeneral reduces every phase.
@@ -396,13 +506,20 @@ __device__ __forceinline__ void block_fp32(const Tile& T, int it, const Tile& S,
   for (int a = 0; a < NBT; ++a)
 #pragma unroll
     for (int b = 0; b < NBS; ++b) blk_re[a][b] = blk_im[a][b] = 0.f;
+  constexpr bool kPacked = QT > 0 && QT % 2 == 0;
+  auto small = [&] {
+    if constexpr (kPacked)
+      far_sums_x2<QT, KER, OP, NBT, NBS>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
+    else
+      far_sums<QT, KER, OP, NBT, NBS, true>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
+  };
   if (!kC || PH == kPhaseSmall) {
-    far_sums<QT, KER, OP, NBT, NBS, true>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
+    small();
   } else if (PH == kPhaseGeneral) {
     far_sums<QT, KER, OP, NBT, NBS, false>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
   } else {
     if (small_phase)
-      far_sums<QT, KER, OP, NBT, NBS, true>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
+      small();
     else
       far_sums<QT, KER, OP, NBT, NBS, false>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
   }
@@ -471,18 +588,23 @@ __device__ __forceinline__ void mirror_put(double* mir, int it, int js, double r
 enum NearMode : int { kNearInKernel = 0, kNearMasked = 1 };
 
 // Resident CTAs per SM the register allocation must allow: 5 for the FP64 Laplace
-// hypersingular kernel (it fits in 96 registers without spills), 4 elsewhere.
-template <int KER, int OP, bool MIXED>
-constexpr int min_ctas() { return (KER == kLaplace && OP == kHS && !MIXED) ? 5 : 4; }
+// hypersingular kernel (it fits in 96 registers without spills), 6 for the mixed
+// Helmholtz DP0 kernels (80 registers; with no FP64 points in their tiles six CTAs also
+// fit in shared memory), 4 elsewhere.
+template <int KER, int OP, bool MIXED, bool DIRECT>
+constexpr int min_ctas() {
+  return (KER == kLaplace && OP == kHS && !MIXED) ? 5 : (MIXED && DIRECT && KER == kHelmholtz) ? 6 : 4;
+}
 
 template <int QT, int KER, int OP, int NBT, int NBS, bool MIXED, bool DIRECT, int PH, int NM>
-__global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
+__global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT>())
     regular_tiles(CellSet test, SpaceTiles tt, CellSet trial, SpaceTiles st, RegularRule rule,
                   double k, int same_grid, double* __restrict__ out, int64_t ld, int tile_y0,
                   int tile_y1, NearArgs near, int symmetric) {
   constexpr bool kC = KER == kHelmholtz;
   constexpr bool kQueue = MIXED && NM == kNearInKernel;
   constexpr bool kRel = MIXED;  // FP32 offsets staged
+  constexpr bool kPts = !MIXED || NM == kNearInKernel;  // FP64 points staged
   // P1 (or DP1) test space: the lanes' local blocks go through a per-warp stage and are
   // summed per test DOF (lane = DOF) before the accumulator, so that no two lanes of a
   // warp update the same entry (test cells share vertex DOFs)
@@ -496,7 +618,7 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
   // tx >= sy are computed, the blocks with tx > sy also written transposed
   int tx, sy;
   if (symmetric) {
-    lower_tile_pair(blockIdx.x, (test.ncells + kTile - 1) / kTile, tile_y0, tx, sy);
+    lower_tile_pair(blockIdx.x, (test.ncells + kTile - 1) / kTile, tile_y0, tile_y1, tx, sy);
   } else {
     tx = blockIdx.x;
     sy = blockIdx.y + tile_y0;
@@ -537,8 +659,8 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
     inc_ent = cursor + 3 * kTile + 1;
     cursor += 6 * kTile + 1;
   }
-  const Tile T = carve_tile(cursor, Q, kRel, NBT);
-  const Tile S = carve_tile(cursor, Q, kRel, NBS);
+  const Tile T = carve_tile(cursor, Q, kRel, NBT, kPts);
+  const Tile S = carve_tile(cursor, Q, kRel, NBS, kPts);
   // DIRECT, symmetric: the block's entries, [js * (kTile + 1) + it], for the transposed
   // write; padded rows keep both access patterns free of bank conflicts
   double* mir = reinterpret_cast<double*>(cursor);
@@ -552,9 +674,9 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED>())
   __syncthreads();
   if (threadIdx.x == 0) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect_tx(mbar, 2 * bulk_tile_bytes(Q, kRel));
-    stage_tile_bulk(T, test, ti0, Q, kRel, mbar);
-    stage_tile_bulk(S, trial, sj0, Q, kRel, mbar);
+    mbar_expect_tx(mbar, 2 * bulk_tile_bytes(Q, kRel, kPts));
+    stage_tile_bulk(T, test, ti0, Q, kRel, mbar, kPts);
+    stage_tile_bulk(S, trial, sj0, Q, kRel, mbar, kPts);
   }
   if (!DIRECT) {
     for (int w = 0; w < kAcc; ++w)
@@ -831,6 +953,8 @@ __device__ void duffy_sl_dp0_warp(const Tile& T, int it, const Tile& S, int js, 
     v0y[d] = S.G(fCx + d, js) - (t0y[d] + t1y[d]) / 3.0;
   }
   const int off = __ldg(rules.offset + cfg), npts = __ldg(rules.offset + cfg + 1) - off;
+  // |k r| <= k (diam_x + diam_y): no reduction of the phase when that is below pi/4
+  const bool small_phase = k * (T.G(fDiam, it) + S.G(fDiam, js)) <= 0.78;
   double sr = 0.0, si = 0.0;
   for (int ii = lane; ii < npts; ii += 32) {
     const int i = off + ii;
@@ -842,9 +966,12 @@ __device__ void duffy_sl_dp0_warp(const Tile& T, int it, const Tile& S, int js, 
       const double dd = (v0x[d] + xi0 * t0x[d] + xi1 * t1x[d]) - (v0y[d] + et0 * t0y[d] + et1 * t1y[d]);
       r2 += dd * dd;
     }
-    const double rinv = rsqrt(r2);
+    const double rinv = rsqrt_refined(r2);
     double sn, cs;
-    sincos(k * r2 * rinv, &sn, &cs);
+    if (small_phase)
+      sincos_taylor(k * r2 * rinv, sn, cs);
+    else
+      sincos_cw(k * r2 * rinv, sn, cs);
     sr = fma(w * rinv, cs, sr);
     si = fma(w * rinv, sn, si);
   }
@@ -883,10 +1010,12 @@ __global__ void __launch_bounds__(kThreads)
     while (m + 1 < a.nmesh && item >= a.mesh[m + 1].item_begin) ++m;
     const SweepMesh& M = a.mesh[m];
     const long long local = item - M.item_begin;
-    const int nchunks = (a.nk + a.kchunk - 1) / a.kchunk;
-    const int kc = static_cast<int>(local % nchunks);
+    // wavenumber chunk outermost: the items resident at one time write one output
+    // matrix (one chunk of them), in the banded tile-pair order
+    const long long npairs = lower_tile_pair_count(M.ntiles, 0, M.ntiles);
+    const int kc = static_cast<int>(local / npairs);
     int tt, st;
-    lower_tile_pair(static_cast<int>(local / nchunks), M.ntiles, 0, tt, st);
+    lower_tile_pair(local % npairs, M.ntiles, 0, M.ntiles, tt, st);
     const bool mirror = tt > st;
     const int nc = M.cells.ncells;
     const int ti0 = tt * kTile, sj0 = st * kTile;
@@ -968,7 +1097,7 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 size_t smem_bytes(int q, bool rel, bool queue, bool direct, bool cplx, int max_t, int max_s,
-                  int nbt, int nbs, int acc_copies, bool mirror) {
+                  int nbt, int nbs, int acc_copies, bool mirror, bool pts) {
   size_t b = 16;  // the mbarrier
   if (!direct) b += sizeof(double) * static_cast<size_t>(max_t) * max_s * (cplx ? 2 : 1) * acc_copies;
   if (direct && mirror) b += sizeof(double) * kTile * (kTile + 1) * (cplx ? 2 : 1) + 16;
@@ -976,7 +1105,7 @@ size_t smem_bytes(int q, bool rel, bool queue, bool direct, bool cplx, int max_t
     b += sizeof(double) * kWarps * kTile * nbt * nbs * (cplx ? 2 : 1) + 6 * kTile + 1;
   for (int nb : {nbt, nbs}) {
     b = (b + 15) & ~size_t(15);
-    b += sizeof(double) * tile_doubles(q) + sizeof(float) * tile_floats(q, rel) +
+    b += sizeof(double) * tile_doubles(q, pts) + sizeof(float) * tile_floats(q, rel) +
          sizeof(int) * tile_ints(nb);
     b = (b + 15) & ~size_t(15);
   }
@@ -991,7 +1120,7 @@ cudaError_t launch_mode(const CellSet& test, const SpaceTiles& tt, const CellSet
   constexpr int kAcc = (!DIRECT && NBT == 3 && KER != kHelmholtz && !MIXED && OP != kHS) ? kWarps : 1;
   const size_t smem = smem_bytes(rule.npts, MIXED, MIXED && NM == kNearInKernel, DIRECT,
                                  KER == kHelmholtz, tt.max_tile_dofs, st.max_tile_dofs, NBT, NBS,
-                                 kAcc, a.symmetric != 0);
+                                 kAcc, a.symmetric != 0, !MIXED || NM == kNearInKernel);
   auto fn = regular_tiles<QT, KER, OP, NBT, NBS, MIXED, DIRECT, PH, NM>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
@@ -999,9 +1128,8 @@ cudaError_t launch_mode(const CellSet& test, const SpaceTiles& tt, const CellSet
   const int ntt = (test.ncells + kTile - 1) / kTile;
   dim3 grid(ntt, ty1 - ty0);
   if (a.symmetric) {
-    // tile pairs (tx >= sy) of trial tiles [ty0, ty1), one row per trial tile
-    const long long L = ntt - ty0, rows = ty1 - ty0;
-    const long long count = rows * L - rows * (rows - 1) / 2;
+    // tile pairs (tx >= sy) of trial tiles [ty0, ty1), in bands of trial tiles
+    const long long count = lower_tile_pair_count(ntt, ty0, ty1);
     if (count > 0x7fffffffLL) return cudaErrorInvalidValue;
     grid = dim3(static_cast<unsigned>(count), 1);
   }

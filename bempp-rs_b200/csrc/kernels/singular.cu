@@ -17,7 +17,7 @@ namespace {
 constexpr int kThreads = 256;
 
 struct CellData {
-  double v0[3], t0[3], t1[3], n[3], jdet;
+  double v0[3], t0[3], t1[3], n[3], jdet, diam;
 };
 
 __device__ __forceinline__ void load_cell(const CellSet& cs, int c, CellData& d) {
@@ -29,9 +29,13 @@ __device__ __forceinline__ void load_cell(const CellSet& cs, int c, CellData& d)
     d.n[k] = g(cs.geom, kNx + k, n, c);
   }
   d.jdet = g(cs.geom, kJdet, n, c);
+  d.diam = g(cs.geom, kDiam, n, c);
 }
 
-template <int KER, int OP, int NBT, int NBS, bool FAST>
+// FP64 throughout, with the refined hardware reciprocal square root (rsqrt_refined,
+// rinv3_refined) and sincos_cw; a pair whose phases all satisfy |k r| <= pi/4 (k times
+// the sum of the two diameters bounds them) skips the reduction (sincos_taylor).
+template <int KER, int OP, int NBT, int NBS>
 __global__ void __launch_bounds__(kThreads)
     singular_fp64(CellSet test, const int* __restrict__ tdofs, CellSet trial,
                   const int* __restrict__ sdofs, SingularRules rules, SingularPairs pairs,
@@ -48,6 +52,8 @@ __global__ void __launch_bounds__(kThreads)
   load_cell(test, tc, x);
   load_cell(trial, sc, y);
   const int off = __ldg(rules.offset + cfg), npts = __ldg(rules.offset + cfg + 1) - off;
+  const double dv[3] = {x.v0[0] - y.v0[0], x.v0[1] - y.v0[1], x.v0[2] - y.v0[2]};
+  const bool small_phase = kCplx && k * (x.diam + y.diam) <= 0.78;  // same in the whole warp
 
   double blk_re[NBT][NBS], blk_im[NBT][NBS];
   double S_re = 0.0, S_im = 0.0;
@@ -56,33 +62,34 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
     for (int b = 0; b < NBS; ++b) blk_re[a][b] = blk_im[a][b] = 0.0;
 
+  const double2* txi = reinterpret_cast<const double2*>(rules.test_xi);
+  const double2* sxi = reinterpret_cast<const double2*>(rules.trial_xi);
   for (int ii = lane; ii < npts; ii += 32) {
     const int i = off + ii;
-    const double xi0 = __ldg(rules.test_xi + 2 * i), xi1 = __ldg(rules.test_xi + 2 * i + 1);
-    const double et0 = __ldg(rules.trial_xi + 2 * i), et1 = __ldg(rules.trial_xi + 2 * i + 1);
+    const double2 xi = __ldg(txi + i), et = __ldg(sxi + i);
     const double w = __ldg(rules.w + i);
     double d[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c)
-      d[c] = (x.v0[c] + xi0 * x.t0[c] + xi1 * x.t1[c]) - (y.v0[c] + et0 * y.t0[c] + et1 * y.t1[c]);
+      d[c] = fma(xi.x, x.t0[c], fma(xi.y, x.t1[c], fma(-et.x, y.t0[c], fma(-et.y, y.t1[c], dv[c]))));
     const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-    const double rinv = FAST ? rsqrt_refined(r2) : rsqrt(r2);
     double kre, kim = 0.0;  // w * (kernel factor), see the regular kernels
     if (KER == kLaplace) {
       if (OP == kSL || OP == kHS) {
-        kre = w * rinv;
+        kre = w * rsqrt_refined(r2);
       } else {
         const double dn = OP == kDL ? (d[0] * y.n[0] + d[1] * y.n[1] + d[2] * y.n[2])
                                     : -(d[0] * x.n[0] + d[1] * x.n[1] + d[2] * x.n[2]);
-        kre = w * dn * rinv * rinv * rinv;
+        kre = w * dn * rinv3_refined(r2);
       }
     } else {
+      const double rinv = rsqrt_refined(r2);
       const double r = r2 * rinv;
       double sn, cs;
-      if (FAST)
-        sincos_cw(k * r, sn, cs);
+      if (small_phase)
+        sincos_taylor(k * r, sn, cs);
       else
-        sincos(k * r, &sn, &cs);
+        sincos_cw(k * r, sn, cs);
       if (OP == kSL || OP == kHS) {
         kre = w * rinv * cs;
         kim = w * rinv * sn;
@@ -100,16 +107,26 @@ __global__ void __launch_bounds__(kThreads)
       if (kCplx) S_im += kim;
     }
     if (OP != kHS || kCplx) {
-      const double phi[3] = {1.0 - xi0 - xi1, xi0, xi1};
-      const double psi[3] = {1.0 - et0 - et1, et0, et1};
-#pragma unroll
-      for (int a = 0; a < NBT; ++a) {
-        const double fa = NBT == 1 ? 1.0 : phi[a];
+      const double psi[3] = {1.0 - et.x - et.y, et.x, et.y};
+      if (NBT == 1) {
 #pragma unroll
         for (int b = 0; b < NBS; ++b) {
-          const double f = NBS == 1 ? fa : fa * psi[b];
-          blk_re[a][b] = fma(kre, f, blk_re[a][b]);
-          if (kCplx) blk_im[a][b] = fma(kim, f, blk_im[a][b]);
+          const double f = NBS == 1 ? 1.0 : psi[b];
+          blk_re[0][b] = fma(kre, f, blk_re[0][b]);
+          if (kCplx) blk_im[0][b] = fma(kim, f, blk_im[0][b]);
+        }
+      } else {
+        // (kre phi_a) psi_b: three products, then one FMA per block entry
+        const double phi[3] = {1.0 - xi.x - xi.y, xi.x, xi.y};
+#pragma unroll
+        for (int a = 0; a < NBT; ++a) {
+          const double vr = kre * phi[a], vi = kim * phi[a];
+#pragma unroll
+          for (int b = 0; b < NBS; ++b) {
+            const double f = NBS == 1 ? 1.0 : psi[b];
+            blk_re[a][b] = fma(vr, f, blk_re[a][b]);
+            if (kCplx) blk_im[a][b] = fma(vi, f, blk_im[a][b]);
+          }
         }
       }
     }
@@ -223,10 +240,7 @@ cudaError_t launch_one(const CellSet& test, const int* tdofs, const CellSet& tri
                        const SingularArgs& a, cudaStream_t stream) {
   const int warps = kThreads / 32;
   const int blocks = (pairs.npairs + warps - 1) / warps;
-  // FAST: the refined hardware rsqrt and sincos_cw (mixed-precision assemblies; Helmholtz)
-  auto fn = (a.fast && KER == kHelmholtz) ? singular_fp64<KER, OP, NBT, NBS, true>
-                                          : singular_fp64<KER, OP, NBT, NBS, false>;
-  fn<<<blocks, kThreads, 0, stream>>>(
+  singular_fp64<KER, OP, NBT, NBS><<<blocks, kThreads, 0, stream>>>(
       test, tdofs, trial, sdofs, rules, pairs, a.k, static_cast<double*>(a.out), a.ld,
       a.unique_entries, a.pair_values, a.trial_lo, a.trial_hi);
   return cudaGetLastError();

@@ -25,35 +25,49 @@ static_assert(kH - kT0x + 1 == kTileFields && kNx - kT0x == fNx && kJdet - kT0x 
 // Shared-memory image of a tile of kTile cells.
 struct Tile {
   double* pts;  // [(q*3+d) * kTile + c] absolute FP64 points
-  float4* rel;  // [q * kTile + c] FP32 offset from the centroid (x, y, z) and its
-                //   squared length (w) (mixed only)
+  float4* rel;  // [r * kTile + c], r < qrel_rows(q): FP32 offsets from the centroid and
+                //   their squared lengths, points in pairs (CellSet::qrel; mixed only)
   double* geo;  // [f * kTile + c]
   int* vid;     // [v * kTile + c]
   int* ldof;    // [b * kTile + c]
   __device__ __forceinline__ double P(int q, int d, int c) const { return pts[(q * 3 + d) * kTile + c]; }
-  __device__ __forceinline__ float4 R4(int q, int c) const { return rel[q * kTile + c]; }
-  __device__ __forceinline__ float R(int q, int d, int c) const {
-    return reinterpret_cast<const float*>(rel + q * kTile + c)[d];
+  // point q of cell c: (x, y, z, squared length)
+  __device__ __forceinline__ float4 R4(int q, int c) const {
+    const float* a = reinterpret_cast<const float*>(rel + (q & ~1) * kTile + c);
+    const float* b = reinterpret_cast<const float*>(rel + ((q & ~1) + 1) * kTile + c);
+    const int h = q & 1;
+    return make_float4(a[h], a[2 + h], b[h], b[2 + h]);
   }
+  __device__ __forceinline__ float R(int q, int d, int c) const {
+    return reinterpret_cast<const float*>(rel + ((q & ~1) + (d >> 1)) * kTile + c)[2 * (d & 1) + (q & 1)];
+  }
+  // points 2j, 2j+1 of cell c: (x, x', y, y') and (z, z', |.|^2, |.|^2')
+  __device__ __forceinline__ float4 RA(int j, int c) const { return rel[2 * j * kTile + c]; }
+  __device__ __forceinline__ float4 RB(int j, int c) const { return rel[(2 * j + 1) * kTile + c]; }
   __device__ __forceinline__ double G(int f, int c) const { return geo[f * kTile + c]; }
 };
 
-__host__ __device__ inline size_t tile_doubles(int q) { return (3 * q + kTileFields) * kTile; }
-__host__ __device__ inline size_t tile_floats(int q, bool mixed) { return mixed ? 4 * q * kTile : 0; }
+// pts: the tile holds the FP64 quadrature points (every kernel but the masked mixed ones,
+// whose FP64 near pairs are integrated by another kernel)
+__host__ __device__ inline size_t tile_doubles(int q, bool pts = true) {
+  return ((pts ? 3 * q : 0) + kTileFields) * kTile;
+}
+__host__ __device__ inline size_t tile_floats(int q, bool mixed) { return mixed ? 4 * qrel_rows(q) * kTile : 0; }
 __host__ __device__ inline size_t tile_ints(int nb) { return (3 + nb) * kTile; }
 // Bytes of one tile staged by bulk copies (points, geometry, FP32 offsets, vertex ids).
-__host__ __device__ inline unsigned bulk_tile_bytes(int q, bool mixed) {
-  return static_cast<unsigned>(sizeof(double) * tile_doubles(q) + sizeof(float) * tile_floats(q, mixed) +
-                               sizeof(int) * 3 * kTile);
+__host__ __device__ inline unsigned bulk_tile_bytes(int q, bool mixed, bool pts = true) {
+  return static_cast<unsigned>(sizeof(double) * tile_doubles(q, pts) +
+                               sizeof(float) * tile_floats(q, mixed) + sizeof(int) * 3 * kTile);
 }
 
 // Carves a tile out of shared memory at *cursor rounded up to 16 bytes.  Every row of
 // the tile starts on a 16-byte boundary (the bulk copies' requirement).
-__device__ inline Tile carve_tile(unsigned char*& cursor, int q, bool mixed, int nb) {
+__device__ inline Tile carve_tile(unsigned char*& cursor, int q, bool mixed, int nb,
+                                  bool pts = true) {
   Tile t;
   cursor = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(cursor) + 15) & ~uintptr_t(15));
   t.pts = reinterpret_cast<double*>(cursor);
-  t.geo = t.pts + 3 * q * kTile;
+  t.geo = t.pts + (pts ? 3 * q * kTile : 0);
   cursor = reinterpret_cast<unsigned char*>(t.geo + kTileFields * kTile);  // 16-B multiple
   t.rel = reinterpret_cast<float4*>(cursor);
   cursor += sizeof(float) * tile_floats(q, mixed);
@@ -86,9 +100,9 @@ __device__ inline void load_tile(const Tile& t, const CellSet& cs, int c0, int n
     t.pts[idx] = __ldg(cs.qpts + pd * S + c0 + c);
   }
   if (mixed)
-    for (int idx = threadIdx.x; idx < q * kTile; idx += kThreads) {
-      const int c = idx % kTile, p = idx / kTile;
-      t.rel[idx] = __ldg(cs.qrel + p * S + c0 + c);
+    for (int idx = threadIdx.x; idx < qrel_rows(q) * kTile; idx += kThreads) {
+      const int c = idx % kTile, r = idx / kTile;
+      t.rel[idx] = __ldg(cs.qrel + r * S + c0 + c);
     }
   for (int idx = threadIdx.x; idx < kTileFields * kTile; idx += kThreads) {
     const int c = idx % kTile, f = idx / kTile;
@@ -158,15 +172,16 @@ __device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned b
 // Issues the bulk copies of one tile (one thread): every row is 32 cells starting at a
 // multiple of 32 of a padded grid array, so sources are 256-byte aligned.
 __device__ inline void stage_tile_bulk(const Tile& t, const CellSet& cs, int c0, int q, bool mixed,
-                                       uint64_t* m) {
+                                       uint64_t* m, bool pts = true) {
   const int64_t S = cs.stride;
-  for (int pd = 0; pd < 3 * q; ++pd)
-    bulk_copy(t.pts + pd * kTile, cs.qpts + pd * S + c0, sizeof(double) * kTile, m);
+  if (pts)
+    for (int pd = 0; pd < 3 * q; ++pd)
+      bulk_copy(t.pts + pd * kTile, cs.qpts + pd * S + c0, sizeof(double) * kTile, m);
   for (int f = 0; f < kTileFields; ++f)
     bulk_copy(t.geo + f * kTile, cs.geom + (kT0x + f) * S + c0, sizeof(double) * kTile, m);
   if (mixed)
-    for (int p = 0; p < q; ++p)
-      bulk_copy(t.rel + p * kTile, cs.qrel + p * S + c0, sizeof(float4) * kTile, m);
+    for (int r = 0; r < qrel_rows(q); ++r)
+      bulk_copy(t.rel + r * kTile, cs.qrel + r * S + c0, sizeof(float4) * kTile, m);
   for (int v = 0; v < 3; ++v) bulk_copy(t.vid + v * kTile, cs.vids + v * S + c0, sizeof(int) * kTile, m);
 }
 
@@ -201,6 +216,27 @@ __device__ __forceinline__ float rcp_approx(float x) {
   return y;
 }
 
+// Packed FP32x2 arithmetic (sm_100): one instruction, two independently rounded results,
+// the same values as the scalar fmaf / + / *.
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 fadd2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 fmul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 rsqrt_approx2(float2 x) {
+  return make_float2(rsqrt_approx(x.x), rsqrt_approx(x.y));
+}
+__device__ __forceinline__ float2 rcp_approx2(float2 x) {
+  return make_float2(rcp_approx(x.x), rcp_approx(x.y));
+}
+// poly_cos_sin on two arguments
+__device__ __forceinline__ void poly_cos_sin2(float2 t, float2& c, float2& s) {
+  const float2 z = fmul2(t, t);
+  c = ffma2(z, ffma2(z, ffma2(z, ffma2(z, f2(2.43751438e-5f), f2(-1.38866017e-3f)),
+                              f2(4.16666195e-2f)), f2(-0.5f)), f2(1.0f));
+  s = fmul2(t, ffma2(z, ffma2(z, ffma2(z, f2(-1.95052402e-4f), f2(8.33209045e-3f)),
+                              f2(-0.166666538f)), f2(1.0f)));
+}
+
 // cos and sin of an argument of any moderate size: Cody-Waite reduction by multiples of
 // pi/2 (two-part constant) to |r| <= pi/4, the polynomials above there, and the
 // quadrant's exchange of sine and cosine.  FP32 arguments up to a few hundred.
@@ -226,21 +262,6 @@ __device__ __forceinline__ void phase_cos_sin(double theta, float& c, float& s) 
   const int q = static_cast<int>(static_cast<long long>(n) & 3);
   c = (q == 0) ? cr : (q == 1) ? -sr : (q == 2) ? -cr : sr;
   s = (q == 0) ? sr : (q == 1) ? cr : (q == 2) ? -sr : -cr;
-}
-
-// Tile pair of block b of a lower-triangle launch: pairs (tx, sy) with sy in [ty0, ...) and
-// tx in [sy, ntt), row by row: row m (sy = ty0 + m) starts at m L - m (m - 1) / 2, with
-// L = ntt - ty0 the first row's length.
-__device__ __forceinline__ void lower_tile_pair(int b, int ntt, int ty0, int& tx, int& sy) {
-  const long long L = ntt - ty0, B = b;
-  const double twoL1 = 2.0 * static_cast<double>(L) + 1.0;
-  long long m = static_cast<long long>((twoL1 - sqrt(twoL1 * twoL1 - 8.0 * static_cast<double>(B))) * 0.5);
-  auto start = [&](long long r) { return r * L - r * (r - 1) / 2; };
-  if (m < 0) m = 0;
-  while (m > 0 && start(m) > B) --m;
-  while (m + 1 < L && start(m + 1) <= B) ++m;
-  sy = ty0 + static_cast<int>(m);
-  tx = sy + static_cast<int>(B - start(m));
 }
 
 }  // namespace tiles

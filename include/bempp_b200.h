@@ -176,6 +176,11 @@ size_t boundary_assembler_host_copy_stats(BoundaryAssemblerT *assembler, double 
  * TFLOP/s (fp64 != 0: FP64, else FP32), the roofline denominator of the regular
  * quadrature kernels. */
 BemppStatus bempp_measure_fma_peak(int fp64, int iters, int reps, double *tflops);
+/* Addition: the order in which a lower-triangle launch (symmetric operator on one space,
+ * adjoint gradient, batched sweep) visits the tile pairs of trial tiles [ty0, ty1) out of
+ * ntt 32-cell tiles: writes up to `capacity` (test tile, trial tile) pairs to tx / sy and
+ * returns the pair count (host copy of the kernels' decoding, for self-checks). */
+long long bempp_lower_tile_pairs(int ntt, int ty0, int ty1, int *tx, int *sy, long long capacity);
 /* Addition (no counterpart in the reference): page-locked host blocks for dense outputs.
  * A matrix assembled into page-locked memory is written by DMA as its columns finish,
  * with no staging copy.  bempp_host_alloc returns a block of at least `bytes` (NULL and
@@ -185,6 +190,11 @@ BemppStatus bempp_measure_fma_peak(int fp64, int iters, int reps, double *tflops
 void *bempp_host_alloc(size_t bytes);
 void bempp_host_free(void *ptr);
 size_t bempp_host_trim(void);
+/* Addition (no counterpart in the reference): the library keeps the device blocks of
+ * freed grids, spaces and assemblers for reuse (building and freeing them again makes no
+ * cudaMalloc / cudaFree calls); bempp_device_trim releases every cached free block to the
+ * driver and returns the bytes released. */
+size_t bempp_device_trim(void);
 
 /* ------------------------------------------------------------------ matrices ----- */
 /* src/bindings/matrices.rs:6-20 */

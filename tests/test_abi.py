@@ -269,3 +269,35 @@ def test_header_parses_for_cffi():
     assert lib.DType_C64 == 3 and lib.OperatorType_Hypersingular == 3
     assert lib.ReferenceCellType_Triangle == 2 and lib.Continuity_Discontinuous == 1
     assert os.path.exists(_lib.LIBRARY)
+
+
+@pytest.mark.parametrize("ntt,ty0,ty1", [
+    (1, 0, 1), (5, 0, 5), (16, 0, 16), (17, 0, 17), (40, 0, 40), (640, 0, 640),
+    (320, 0, 71), (320, 71, 142), (320, 300, 320), (321, 17, 50), (33, 32, 33),
+])
+def test_lower_tile_pair_order_is_a_bijection(ntt, ty0, ty1):
+    """The tile-pair order of lower-triangle launches visits every pair (tx >= sy,
+    sy in [ty0, ty1)) exactly once, in bands of 16 trial tiles."""
+    n = lib.bempp_lower_tile_pairs(ntt, ty0, ty1, ffi.NULL, ffi.NULL, 0)
+    rows = ty1 - ty0
+    assert n == sum(ntt - s for s in range(ty0, ty1))
+    tx = np.zeros(n, dtype=np.int32)
+    sy = np.zeros(n, dtype=np.int32)
+    assert lib.bempp_lower_tile_pairs(ntt, ty0, ty1, ffi.cast("int*", tx.ctypes.data),
+                                      ffi.cast("int*", sy.ctypes.data), n) == n
+    assert np.all(tx >= sy) and np.all(sy >= ty0) and np.all(sy < ty1) and np.all(tx < ntt)
+    key = tx.astype(np.int64) * ntt + sy
+    assert len(np.unique(key)) == n
+    band = (sy - ty0) // 16
+    assert np.all(np.diff(band) >= 0)  # bands in order
+    if rows > 16:
+        assert band.max() == (rows - 1) // 16
+
+
+def test_lower_tile_pairs_rejects_bad_ranges():
+    assert lib.bempp_lower_tile_pairs(10, 5, 4, ffi.NULL, ffi.NULL, 0) == -1
+    assert lib.bempp_lower_tile_pairs(10, 0, 11, ffi.NULL, ffi.NULL, 0) == -1
+
+
+def test_device_trim_with_nothing_cached():
+    assert lib.bempp_device_trim() == 0

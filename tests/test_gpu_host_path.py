@@ -112,3 +112,38 @@ def test_page_locked_result_outlives_the_next_assembly():
     assert np.array_equal(first, keep)
     assert not np.array_equal(first, second)
 
+
+
+def test_device_blocks_of_freed_grids_are_reused_and_trimmed(output_memory):
+    """Device blocks of a freed grid, space and assembler go to the library's cache: the
+    next ones reuse them (same result), and bempp_device_trim hands them back."""
+    import gc
+
+    import torch
+
+    from bempp._lib import lib
+
+    if output_memory != "page_locked":
+        pytest.skip("one memory kind is enough")
+
+    def once():
+        pts, cells = shapes.icosphere(3)
+        grid = Grid(shapes.radial_perturbation(pts, seed=3), cells)
+        sp = function_space(grid, create_family(Family.Lagrange, 0, Continuity.Discontinuous))
+        opts = BoundaryAssemblerOptions()
+        opts.set_regular_quadrature_degree(ReferenceCellType.Triangle, 6)
+        a = create_laplace_assembler(OPS["single_layer"], opts, np.float64)
+        n = sp.global_size
+        dev = torch.empty((n, n), dtype=torch.float64, device="cuda")
+        a.assemble_into_device(sp, sp, dev, torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        return dev.cpu().numpy()
+
+    lib.bempp_device_trim()
+    first = once()
+    gc.collect()
+    second = once()
+    assert np.array_equal(first, second)
+    gc.collect()
+    assert lib.bempp_device_trim() > 0
+    assert lib.bempp_device_trim() == 0
