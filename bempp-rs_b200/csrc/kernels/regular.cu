@@ -113,10 +113,10 @@ __device__ __forceinline__ void finish_block(const Tile& T, int it, const Tile& 
   }
 }
 
-// FP64 local block of test cell `it` (tile T) and trial cell `js` (tile S).
-// kFast (the FP64 near pairs of mixed-precision assemblies): sincos_cw for the phase.
-template <int QT, int KER, int OP, int NBT, int NBS, bool kUnroll = true, bool kFast = false>
-__device__ __forceinline__ void block_fp64(const Tile& T, int it, const Tile& S, int js,
+// FP64 local block, test points outermost (every operator but the Laplace adjoint double
+// layer).
+template <int QT, int KER, int OP, int NBT, int NBS, bool kUnroll, bool kFast>
+__device__ __forceinline__ void block_fp64_pq(const Tile& T, int it, const Tile& S, int js,
                                         const RegularRule& rule, double k,
                                         double ore[NBT][NBS], double oim[NBT][NBS]) {
   constexpr bool kC = KER == kHelmholtz;
@@ -227,6 +227,66 @@ __device__ __forceinline__ void block_fp64(const Tile& T, int it, const Tile& S,
     }
   }
   finish_block<KER, OP, NBT, NBS>(T, it, S, js, k, blk_re, blk_im, S_re, S_im, ore, oim);
+}
+
+// Laplace adjoint double layer, FP64: the normal factor (y_q - x).n_x depends on the trial
+// point only, so the trial points are the outer loop and the factor multiplies once per
+// trial point (as the double layer's does per test point in block_fp64_pq).
+template <int QT, int NBT, int NBS, bool kUnroll>
+__device__ __forceinline__ void block_fp64_adl_laplace(const Tile& T, int it, const Tile& S,
+                                                       int js, const RegularRule& rule,
+                                                       double ore[NBT][NBS], double oim[NBT][NBS]) {
+  const int Q = QT > 0 ? QT : rule.npts;
+  double blk_re[NBT][NBS], blk_im[NBT][NBS];
+#pragma unroll
+  for (int a = 0; a < NBT; ++a)
+#pragma unroll
+    for (int b = 0; b < NBS; ++b) blk_re[a][b] = blk_im[a][b] = 0.0;
+  // (y_q - x).n_x = -dc.n_x + u_q t0_y.n_x + v_q t1_y.n_x, (u, v) = eta - (1/3, 1/3)
+  const double dcx = T.G(fCx, it) - S.G(fCx, js), dcy = T.G(fCy, it) - S.G(fCy, js),
+               dcz = T.G(fCz, it) - S.G(fCz, js);
+  const double nx = T.G(fNx, it), ny = T.G(fNy, it), nz = T.G(fNz, it);
+  const double f0 = -(dcx * nx + dcy * ny + dcz * nz);
+  const double f1 = S.G(fT0x, js) * nx + S.G(fT0y, js) * ny + S.G(fT0z, js) * nz;
+  const double f2 = S.G(fT1x, js) * nx + S.G(fT1y, js) * ny + S.G(fT1z, js) * nz;
+#pragma unroll 1
+  for (int q = 0; q < Q; ++q) {
+    const double y0 = S.P(q, 0, js), y1 = S.P(q, 1, js), y2 = S.P(q, 2, js);
+    const double bq = fma(rule.u[q], f1, fma(rule.v[q], f2, f0));
+    double v[NBT];
+#pragma unroll
+    for (int a = 0; a < NBT; ++a) v[a] = 0.0;
+#pragma unroll(kUnroll ? 6 : 1)
+    for (int p = 0; p < Q; ++p) {
+      const double dx = T.P(p, 0, it) - y0, dy = T.P(p, 1, it) - y1, dz = T.P(p, 2, it) - y2;
+      const double kern = rinv3_refined(dx * dx + dy * dy + dz * dz);
+      if (NBT == 1) {
+        v[0] = fma(kern, rule.w[p], v[0]);
+      } else {
+#pragma unroll
+        for (int a = 0; a < NBT; ++a) v[a] = fma(kern, rule.wphi[a][p], v[a]);
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < NBS; ++b) {
+      const double f = (NBS == 1 ? rule.w[q] : rule.wphi[b][q]) * bq;
+#pragma unroll
+      for (int a = 0; a < NBT; ++a) blk_re[a][b] = fma(v[a], f, blk_re[a][b]);
+    }
+  }
+  finish_block<kLaplace, kADL, NBT, NBS>(T, it, S, js, 0.0, blk_re, blk_im, 0.0, 0.0, ore, oim);
+}
+
+// FP64 local block of test cell `it` (tile T) and trial cell `js` (tile S).
+// kFast (the FP64 near pairs of mixed-precision assemblies): sincos_cw for the phase.
+template <int QT, int KER, int OP, int NBT, int NBS, bool kUnroll = true, bool kFast = false>
+__device__ __forceinline__ void block_fp64(const Tile& T, int it, const Tile& S, int js,
+                                        const RegularRule& rule, double k,
+                                        double ore[NBT][NBS], double oim[NBT][NBS]) {
+  if constexpr (KER == kLaplace && OP == kADL)
+    block_fp64_adl_laplace<QT, NBT, NBS, kUnroll>(T, it, S, js, rule, ore, oim);
+  else
+    block_fp64_pq<QT, KER, OP, NBT, NBS, kUnroll, kFast>(T, it, S, js, rule, k, ore, oim);
 }
 
 // Per-pair constants of the FP32 far-pair quadrature.
