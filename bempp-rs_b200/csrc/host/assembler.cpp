@@ -292,9 +292,12 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
   ra.out_type = cplx ? kOutC128 : kOutF64;
   ra.ld = nt;
   ra.out = out;
-  // a margin of 1e-6 relative covers the device's own rounding of the radii
-  ra.small_phase = std::fabs(a.k) * (test.grid->max_circumradius() + trial.grid->max_circumradius()) *
-                               (1.0 + 1e-6) <= 0.8 ? 1 : 0;
+  // bound of |k (r - r0)| over every far pair (r0 the centroid distance); a margin of 1e-6
+  // relative covers the device's own rounding of the radii
+  const double phase_bound = std::fabs(a.k) *
+                             (test.grid->max_circumradius() + trial.grid->max_circumradius()) *
+                             (1.0 + 1e-6);
+  ra.small_phase = phase_bound <= 0.8 ? 1 : 0;
   if (ra.precision == kRegularMixed && nt > 0 && ns > 0) {
     const NearField& nf = near_field(*test.grid, *trial.grid);
     ra.near.tile_mask = nf.tile_mask.as<int>();

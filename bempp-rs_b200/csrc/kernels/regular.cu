@@ -413,7 +413,8 @@ __device__ __forceinline__ void far_sums_x2(const Tile& T, int it, const Tile& S
   constexpr bool kC = KER == kHelmholtz;
   constexpr bool kNeedBasis = OP != kHS || kC;
   constexpr bool kKahan = NBT == 1 && NBS == 1;
-  float cmp_re = 0.f, cmp_im = 0.f;
+  float cmp_re = 0.f;
+  float2 acc2 = f2(0.f), cmp2 = f2(0.f);  // kKahan, Helmholtz: (re, im) summed together
   const float2 r0sq2 = f2(fp.r0sq), r0f2 = f2(fp.r0f), kf2 = f2(fp.kf), nkf2 = f2(-fp.kf);
 #pragma unroll 1
   for (int p = 0; p < QT; ++p) {
@@ -490,9 +491,11 @@ __device__ __forceinline__ void far_sums_x2(const Tile& T, int it, const Tile& S
     }
     if (kNeedBasis) {
       const float wp = rule.wf[p] * apf;
-      if (kKahan) {
+      if (kKahan && kC) {
+        const float2 v = fadd2(make_float2(u_re[0].x, u_im[0].x), make_float2(u_re[0].y, u_im[0].y));
+        kahan_add2(acc2, cmp2, fmul2(f2(wp), v));
+      } else if (kKahan) {
         kahan_add(blk_re[0][0], cmp_re, wp * (u_re[0].x + u_re[0].y));
-        if (kC) kahan_add(blk_im[0][0], cmp_im, wp * (u_im[0].x + u_im[0].y));
       } else {
 #pragma unroll
         for (int a = 0; a < NBT; ++a) {
@@ -505,6 +508,10 @@ __device__ __forceinline__ void far_sums_x2(const Tile& T, int it, const Tile& S
         }
       }
     }
+  }
+  if (kKahan && kC) {
+    blk_re[0][0] = acc2.x;
+    blk_im[0][0] = acc2.y;
   }
 }
 
@@ -541,7 +548,7 @@ __device__ __forceinline__ void block_fp32(const Tile& T, int it, const Tile& S,
     fp.fa2 = static_cast<float>(S.G(fT1x, js) * nx + S.G(fT1y, js) * ny + S.G(fT1z, js) * nz);
   }
   float ph_c = 1.f, ph_s = 0.f;
-  bool small_phase = PH != kPhaseGeneral;
+  bool small_phase = PH != kPhaseGeneral;  // kPhaseRuntime: decided per warp below
   fp.r0f = fp.kf = 0.f;
   fp.r0sq = fmaf(fdx, fdx, fmaf(fdy, fdy, fdz * fdz));
   if (kC) {
@@ -568,10 +575,11 @@ __device__ __forceinline__ void block_fp32(const Tile& T, int it, const Tile& S,
     for (int b = 0; b < NBS; ++b) blk_re[a][b] = blk_im[a][b] = 0.f;
   constexpr bool kPacked = QT > 0 && QT % 2 == 0;
   auto small = [&] {
-    if constexpr (kPacked)
+    if constexpr (kPacked) {
       far_sums_x2<QT, KER, OP, NBT, NBS>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
-    else
+    } else {
       far_sums<QT, KER, OP, NBT, NBS, true>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
+    }
   };
   if (!kC || PH == kPhaseSmall) {
     small();

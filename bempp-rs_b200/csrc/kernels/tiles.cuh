@@ -194,15 +194,14 @@ __device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
   sum = t;
 }
 
-// cos(t), sin(t) for |t| <= 0.8: polynomials in z = t^2 of degree 8 (cos) and 7 (sin)
-// with the leading coefficient fixed to 1, fitted by minimising the maximum error on
-// [-0.8, 0.8] (discrete minimax over 6001 points, a linear program); approximation
-// errors 6.5e-11 (cos) and 3.3e-9 (sin), below FP32 rounding.
+// cos(t), sin(t) for |t| <= 0.8: cos t ~ 1 + z P(z) of degree 8 and sin t ~ t (1 + z R(z))
+// of degree 7 in t (z = t^2), discrete minimax fits (fit_phase_polys.py); approximation
+// errors 6.5e-11 (cos) and 2.1e-9 (sin), below FP32 rounding.
 __device__ __forceinline__ void poly_cos_sin(float t, float& c, float& s) {
   const float z = t * t;
-  c = fmaf(z, fmaf(z, fmaf(z, fmaf(z, 2.43751438e-5f, -1.38866017e-3f), 4.16666195e-2f), -0.5f),
-           1.0f);
-  s = t * fmaf(z, fmaf(z, fmaf(z, -1.95052402e-4f, 8.33209045e-3f), -0.166666538f), 1.0f);
+  c = fmaf(z, fmaf(z, fmaf(z, fmaf(z, 2.437514408e-5f, -1.388660219e-3f), 4.166661828e-2f),
+                   -4.999999968e-1f), 1.0f);
+  s = t * fmaf(z, fmaf(z, fmaf(z, -1.948277516e-4f, 8.331875683e-3f), -1.666664881e-1f), 1.0f);
 }
 
 __device__ __forceinline__ float rsqrt_approx(float x) {
@@ -231,10 +230,17 @@ __device__ __forceinline__ float2 rcp_approx2(float2 x) {
 // poly_cos_sin on two arguments
 __device__ __forceinline__ void poly_cos_sin2(float2 t, float2& c, float2& s) {
   const float2 z = fmul2(t, t);
-  c = ffma2(z, ffma2(z, ffma2(z, ffma2(z, f2(2.43751438e-5f), f2(-1.38866017e-3f)),
-                              f2(4.16666195e-2f)), f2(-0.5f)), f2(1.0f));
-  s = fmul2(t, ffma2(z, ffma2(z, ffma2(z, f2(-1.95052402e-4f), f2(8.33209045e-3f)),
-                              f2(-0.166666538f)), f2(1.0f)));
+  c = ffma2(z, ffma2(z, ffma2(z, ffma2(z, f2(2.437514408e-5f), f2(-1.388660219e-3f)),
+                              f2(4.166661828e-2f)), f2(-4.999999968e-1f)), f2(1.0f));
+  s = fmul2(t, ffma2(z, ffma2(z, ffma2(z, f2(-1.948277516e-4f), f2(8.331875683e-3f)),
+                              f2(-1.666664881e-1f)), f2(1.0f)));
+}
+// Kahan-compensated sum of two independent streams (sum.x, sum.y) at once
+__device__ __forceinline__ void kahan_add2(float2& sum, float2& comp, float2 v) {
+  const float2 y = ffma2(comp, f2(-1.0f), v);    // v - comp
+  const float2 t = fadd2(sum, y);
+  comp = ffma2(y, f2(-1.0f), ffma2(sum, f2(-1.0f), t));  // (t - sum) - y
+  sum = t;
 }
 
 // cos and sin of an argument of any moderate size: Cody-Waite reduction by multiples of

@@ -23,6 +23,10 @@ MIXED_TOL = 1e-6
     ("helmholtz", "double_layer", 8.0),
     ("helmholtz", "adjoint_double_layer", 8.0),
     ("helmholtz", "single_layer", 20.0),   # |k delta| > 0.8 somewhere: sincosf branch
+    # k (max rad_x + max rad_y) = 0.39 and 0.78: small-phase launches (no reduction)
+    ("helmholtz", "single_layer", 2.0),
+    ("helmholtz", "single_layer", 4.0),
+    ("helmholtz", "double_layer", 4.0),
 ])
 def test_mixed_dp0_matches_oracle(kernel, op, k):
     pts, cells = shapes.icosphere(3)
@@ -52,6 +56,8 @@ def test_mixed_far_from_origin():
     ("laplace", "hypersingular", 0.0),
     ("helmholtz", "double_layer", 8.0),
     ("helmholtz", "hypersingular", 8.0),
+    ("helmholtz", "adjoint_double_layer", 4.0),
+    ("helmholtz", "hypersingular", 2.0),
 ])
 def test_mixed_p1_matches_oracle(kernel, op, k):
     pts, cells = shapes.icosphere(3)
