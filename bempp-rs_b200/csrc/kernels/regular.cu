@@ -1065,12 +1065,14 @@ __global__ void __launch_bounds__(kThreads)
   int* counts = reinterpret_cast<int*>(adjc + kTile * kTile);  // near, adjacent
   long long* s_item = reinterpret_cast<long long*>(counts + 2);
   float2* mir = reinterpret_cast<float2*>(s_item + 1);  // [js * (kTile + 1) + it]
+  unsigned* skip = reinterpret_cast<unsigned*>(mir + kTile * (kTile + 1));  // [it]: bit js
   const int it = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (;;) {
     if (threadIdx.x == 0) {
       *s_item = static_cast<long long>(atomicAdd(a.counter, 1ull));
       counts[0] = counts[1] = 0;
     }
+    if (threadIdx.x < kTile) skip[threadIdx.x] = 0u;
     __syncthreads();
     const long long item = *s_item;
     if (item >= a.nitems) break;
@@ -1091,33 +1093,36 @@ __global__ void __launch_bounds__(kThreads)
     load_tile(T, M.cells, ti0, nti, Q, true, nullptr, 1);
     load_tile(S, M.cells, sj0, nsj, Q, true, nullptr, 1);
     __syncthreads();
-    // classify the tile pair once: vertex-sharing and near pairs are queued
+    // classify the tile pair once: vertex-sharing and near pairs are queued, and marked in
+    // the test cell's skip word for the far-pair loop of every wavenumber
     if (it < nti) {
       const int av[3] = {T.vid[it], T.vid[kTile + it], T.vid[2 * kTile + it]};
+      unsigned bits = 0u;
       for (int js = warp; js < nsj; js += kWarps) {
         const int bv[3] = {S.vid[js], S.vid[kTile + js], S.vid[2 * kTile + js]};
         if (share_vertex(av[0], av[1], av[2], bv[0], bv[1], bv[2])) {
           const int slot = atomicAdd(counts + 1, 1);
           adjq[slot] = static_cast<unsigned short>(it | (js << 8));
           adjc[slot] = static_cast<unsigned char>(adjacency_config(av, bv, ti0 + it == sj0 + js));
+          bits |= 1u << js;
         } else if (near_pair(T, it, S, js)) {
           const int slot = atomicAdd(counts, 1);
           nearq[slot] = static_cast<unsigned short>(it | (js << 8));
+          bits |= 1u << js;
         }
       }
+      if (bits) atomicOr(skip + it, bits);
     }
     __syncthreads();
     const int nnear = counts[0], nadj = counts[1];
+    const unsigned skip_it = it < nti ? skip[it] : ~0u;
     const int k0 = kc * a.kchunk, k1 = min(a.nk, k0 + a.kchunk);
     for (int kk = k0; kk < k1; ++kk) {
       const double k = a.ks[kk];
       float2* out = M.out + static_cast<long long>(kk) * nc * nc;
       if (it < nti) {
-        const int a0 = T.vid[it], a1 = T.vid[kTile + it], a2 = T.vid[2 * kTile + it];
         for (int js = warp; js < nsj; js += kWarps) {
-          if (share_vertex(a0, a1, a2, S.vid[js], S.vid[kTile + js], S.vid[2 * kTile + js]) ||
-              near_pair(T, it, S, js))
-            continue;
+          if ((skip_it >> js) & 1u) continue;
           double ore[1][1], oim[1][1];
           block_fp32<6, kHelmholtz, kSL, 1, 1, kPhaseRuntime>(T, it, S, js, rule, k, ore, oim);
           const float2 v = make_float2(static_cast<float>(ore[0][0]), static_cast<float>(oim[0][0]));
@@ -1341,7 +1346,7 @@ size_t sweep_smem_bytes() {
     b = (b + 15) & ~size_t(15);
   }
   return b + 2 * sizeof(unsigned short) * kTile * kTile + kTile * kTile + 2 * sizeof(int) +
-         sizeof(long long) + sizeof(float2) * kTile * (kTile + 1) + 32;
+         sizeof(long long) + sizeof(float2) * kTile * (kTile + 1) + sizeof(unsigned) * kTile + 32;
 }
 
 cudaError_t launch_sweep_sl(const SweepArgs& args, const RegularRule& rule,
