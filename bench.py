@@ -302,7 +302,7 @@ def north_star(args):
     outs = {}
     for prec in ("fp64", "mixed"):
         wl = Workload(w, prec)
-        ms, _ = wl.timed(max(2, args.steps // 2), 2)
+        ms, _ = wl.timed(max(3, args.steps), 2)
         ph = wl.phase_ms()["single_layer"]
         res[prec] = {"ms_per_assembly": ms, "entries_per_s": wl.entries_per_step / (ms * 1e-3),
                      "regular_ms": ph[2] if len(ph) > 2 else None, "phase_ms": ph}
