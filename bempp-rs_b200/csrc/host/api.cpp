@@ -228,6 +228,34 @@ BemppStatus boundary_assembler_assemble_into_memory_ex(BoundaryAssemblerT* a, Sp
   });
 }
 
+BemppStatus potential_assemble_into_memory(BoundaryAssemblerT* a, SpaceT* space,
+                                           const double* points, size_t npoints, void* data) {
+  return guarded([&] {
+    require(a, "assembler");
+    require(space, "space");
+    if (npoints == 0 || space->ndofs == 0) return;
+    require(points, "points");
+    require(data, "output");
+    std::lock_guard<std::mutex> lock(a->mu);
+    assemble_potential_host(*a, *space, points, static_cast<int64_t>(npoints), data);
+  });
+}
+
+BemppStatus potential_assemble_into_device(BoundaryAssemblerT* a, SpaceT* space,
+                                           const double* device_points, size_t npoints,
+                                           void* device_data, void* stream) {
+  return guarded([&] {
+    require(a, "assembler");
+    require(space, "space");
+    if (npoints == 0 || space->ndofs == 0) return;
+    require(device_points, "points");
+    require(device_data, "output");
+    std::lock_guard<std::mutex> lock(a->mu);
+    assemble_potential_device(*a, *space, device_points, static_cast<int64_t>(npoints),
+                              device_data, static_cast<cudaStream_t>(stream));
+  });
+}
+
 void boundary_assembler_assemble_into_memory(BoundaryAssemblerT* a, SpaceT* trial,
                                              SpaceT* test, void* data) {
   boundary_assembler_assemble_into_memory_ex(a, trial, test, data);

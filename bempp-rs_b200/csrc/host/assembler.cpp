@@ -437,6 +437,68 @@ const GridGeometry& sweep_geometry(GridT& g, int device, const RegularRule& rule
   return grid_geometry(g, device, rule, nullptr, launches);
 }
 
+namespace {
+void check_potential(const BoundaryAssemblerT& a, const SpaceT& space, int64_t npoints) {
+  if (a.op != kSL && a.op != kDL)
+    throw Error(kUnsupported, "potential operators: single and double layer only");
+  if (npoints < 0 || npoints > 0x7fffffff) throw Error(kInvalidArgument, "point count");
+  if (space.nbasis != 1 && space.nbasis != 3)
+    throw Error(kUnsupported, "potential operators: DP0 and P1 spaces");
+}
+}  // namespace
+
+void assemble_potential_device(BoundaryAssemblerT& a, SpaceT& space, const double* d_points,
+                               int64_t npoints, void* d_out, cudaStream_t stream) {
+  check_potential(a, space, npoints);
+  const int device = current_device();
+  const auto qit = a.options.regular.find(kTriangle);
+  if (qit == a.options.regular.end())
+    throw Error(kInvalidArgument, "no regular quadrature degree for triangles");
+  const RegularRule rule = simplex_rule(static_cast<int>(qit->second));
+  a.launches = 0;
+  ensure_space_device(space, device);
+  const GridGeometry& geo = grid_geometry(*space.grid, device, rule, stream, a.launches);
+  const bool single = a.dtype == 0 || a.dtype == 2;
+  const bool cplx = a.kernel == kHelmholtz;
+  const size_t reals = static_cast<size_t>(npoints) * space.ndofs * (cplx ? 2 : 1);
+  if (reals == 0) return;
+  void* out = d_out;
+  if (single) {
+    a.convert.alloc(sizeof(double) * reals);
+    out = a.convert.ptr;
+  }
+  if (space.nbasis == 3) {  // P1 DOF columns are sums over the cells of the DOF
+    BEMPP_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * reals, stream));
+    ++a.launches;
+  }
+  BEMPP_CUDA(launch_potential(a.kernel, a.op, d_points, static_cast<int>(npoints),
+                              cell_set(*space.grid, geo), space.d_dofs.as<int>(), space.nbasis,
+                              rule, a.k, static_cast<double*>(out), npoints, stream));
+  ++a.launches;
+  if (single) {
+    BEMPP_CUDA(launch_convert_to_single(static_cast<const double*>(out), d_out, reals, stream));
+    ++a.launches;
+  }
+}
+
+void assemble_potential_host(BoundaryAssemblerT& a, SpaceT& space, const double* points,
+                             int64_t npoints, void* data) {
+  check_potential(a, space, npoints);
+  const bool cplx = a.kernel == kHelmholtz;
+  const size_t esize = (a.dtype == 0 || a.dtype == 2) ? (cplx ? 8 : 4) : (cplx ? 16 : 8);
+  const size_t bytes = static_cast<size_t>(npoints) * space.ndofs * esize;
+  if (bytes == 0) return;
+  if (!a.stream) BEMPP_CUDA(cudaStreamCreateWithFlags(&a.stream, cudaStreamNonBlocking));
+  DeviceBuffer d_points, d_out;
+  d_points.alloc(sizeof(double) * 3 * static_cast<size_t>(npoints));
+  d_out.alloc(bytes);
+  BEMPP_CUDA(cudaMemcpyAsync(d_points.ptr, points, sizeof(double) * 3 * npoints,
+                             cudaMemcpyHostToDevice, a.stream));
+  assemble_potential_device(a, space, d_points.as<double>(), npoints, d_out.ptr, a.stream);
+  BEMPP_CUDA(cudaMemcpyAsync(data, d_out.ptr, bytes, cudaMemcpyDeviceToHost, a.stream));
+  BEMPP_CUDA(cudaStreamSynchronize(a.stream));
+}
+
 SingularRules sweep_rules(int device, int order) {
   const DeviceRules& dr = device_rules(device, order);
   return SingularRules{dr.offset.as<int>(), dr.test_xi.as<double>(), dr.trial_xi.as<double>(),

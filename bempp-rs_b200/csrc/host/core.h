@@ -268,5 +268,13 @@ void helmholtz_sl_sweep_device(GridT* const* grids, size_t ngrids, const double*
 struct SweepTuning;
 // Singular part as CSR (host).
 MatrixT* assemble_singular_csr(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test);
+// Off-surface potential operator (single or double layer of the assembler's kernel) of
+// `space` at npoints device points (npoints x 3, row-major): column-major npoints x ndofs
+// device output in the assembler's dtype (potential.cu).
+void assemble_potential_device(BoundaryAssemblerT& a, SpaceT& space, const double* d_points,
+                               int64_t npoints, void* d_out, cudaStream_t stream);
+// The same from host points into host memory.
+void assemble_potential_host(BoundaryAssemblerT& a, SpaceT& space, const double* points,
+                             int64_t npoints, void* data);
 
 }  // namespace bempp_b200

@@ -134,6 +134,14 @@ cudaError_t assemble_regular_dp0_noalloc(const RegularArgs& args, const RegularR
 
 // Adjoint gradient of Re(lambda^H A mu) for the Helmholtz single layer on DP0 (adjoint.cu):
 // grad_points (npoints x 3) and totals = {J, dJ/dk}; grad_cell is F x 9 scratch.
+// Off-surface potential operators (potential.cu): out[i + ld * dof] for the npoints x 3
+// row-major FP64 points and the trial space's DOFs; op kSL or kDL; P1 adds into the output
+// (zero it first), DP0 stores.
+cudaError_t launch_potential(int kernel, int op, const double* points, int npoints,
+                             const CellSet& trial, const int* dofs, int nbasis,
+                             const RegularRule& rule, double k, double* out, int64_t ld,
+                             cudaStream_t stream);
+
 cudaError_t launch_adjoint_sl(const CellSet& cs, const RegularRule& rule,
                               const SingularRules& rules, const SingularPairs& pairs, double k,
                               const double* lam, const double* mu, double* grad_cell,

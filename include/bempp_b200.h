@@ -172,6 +172,21 @@ size_t boundary_assembler_last_launch_count(BoundaryAssemblerT *assembler);
  * copy groups, assembly chunks, host copy threads, ms spent taking the destination's page
  * faults ahead of the copies]; returns the number written (<= n). */
 size_t boundary_assembler_host_copy_stats(BoundaryAssemblerT *assembler, double *out, size_t n);
+/* Addition: off-surface potential operators, the single and double layer potentials of
+ * the assembler's kernel (OperatorType SingleLayer or DoubleLayer; others fail with
+ * BemppStatus_Unsupported).  out[i + npoints * j] = sum over the cells of DOF j of
+ * jdet int psi_j(y) K(x_i, y) dy by the regular rule of the assembler's options, with
+ * K = G(x, y) (single layer) or n_y . grad_y G(x, y) (double layer), G = 1/(4 pi r) or
+ * e^{ikr}/(4 pi r); column-major npoints x ndofs in the assembler's dtype.  `points` is
+ * npoints x 3, row-major FP64.  Replaces the evaluator the reference declares in
+ * src/boundary_evaluators.rs (an empty file; its bempp-cl comparisons are the commented
+ * tests at tests/compare_to_bempp_cl.rs:208-320).  The points must lie off the surface. */
+BemppStatus potential_assemble_into_memory(BoundaryAssemblerT *assembler, SpaceT *space,
+                                           const double *points, size_t npoints, void *data);
+/* The same with device points and a device output, enqueued on `stream`. */
+BemppStatus potential_assemble_into_device(BoundaryAssemblerT *assembler, SpaceT *space,
+                                           const double *device_points, size_t npoints,
+                                           void *device_data, void *stream);
 /* Addition: measured CUDA-core fused multiply-add throughput of the current device in
  * TFLOP/s (fp64 != 0: FP64, else FP32), the roofline denominator of the regular
  * quadrature kernels. */

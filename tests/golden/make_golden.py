@@ -10,8 +10,11 @@ Run in a checkout that has the reference at REFERENCE (default /root/reference):
 
     python tests/golden/make_golden.py
 
-It writes tests/golden/bempp_cl_octahedron.json.  The fixture is committed; the tests
-never read the reference tree.
+It writes tests/golden/bempp_cl_octahedron.json and, from the four potential-operator
+tests that the file keeps commented out (lines 208-320: single and double layer
+potentials of the Laplace and the k = 3 Helmholtz kernel, DP0, at the points (2, 0, 0),
+(0, 2, 0), (0, 0, 2)), tests/golden/bempp_cl_octahedron_potentials.json.  The fixtures
+are committed; the tests never read the reference tree.
 """
 
 from __future__ import annotations
@@ -24,6 +27,16 @@ import sys
 REFERENCE = os.environ.get("REFERENCE", "/root/reference")
 SRC = os.path.join(REFERENCE, "tests", "compare_to_bempp_cl.rs")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "bempp_cl_octahedron.json")
+OUT_POT = os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                       "bempp_cl_octahedron_potentials.json")
+
+# commented test name -> (kernel, operator)
+POTENTIAL_TESTS = {
+    "test_laplace_single_layer_potential_dp0": ("laplace", "single_layer"),
+    "test_helmholtz_single_layer_potential_dp0": ("helmholtz", "single_layer"),
+    "test_laplace_double_layer_potential_dp0": ("laplace", "double_layer"),
+    "test_helmholtz_double_layer_potential_dp0": ("helmholtz", "double_layer"),
+}
 
 # test name -> (kernel, operator, space degree, continuous)
 TESTS = {
@@ -85,6 +98,38 @@ def main():
     with open(OUT, "w") as f:
         json.dump(out, f, indent=1)
     print(f"wrote {len(out['cases'])} cases to {OUT}")
+    potentials(src)
+
+
+def potentials(src: str):
+    """The commented potential tests: from_cl[dof][point], compared with matrix[point, dof]."""
+    lines = src.splitlines()
+    out = {"source": "bempp-rs tests/compare_to_bempp_cl.rs (commented tests)", "cases": []}
+    for i, line in enumerate(lines):
+        m = re.match(r"\s*//\s*fn (test_\w+_potential_dp0)\(\)", line)
+        if not m or m.group(1) not in POTENTIAL_TESTS:
+            continue
+        body = []
+        for line2 in lines[i + 1:]:
+            t = re.sub(r"^\s*//\s?", "", line2)
+            if t.startswith("}"):
+                break
+            body.append(t)
+        body = "\n".join(body)
+        kernel, op = POTENTIAL_TESTS[m.group(1)]
+        mat = parse_matrix(re.search(r"let from_cl = (\[\[.*?\]\]);", body, re.S).group(1))
+        eps = float(re.search(r"epsilon = ([0-9.eE-]+)", body).group(1))
+        k_m = re.search(r"helmholtz::assembler::\w+\(([0-9.]+)\)", body)
+        pts = [[0.0] * 3 for _ in range(3)]
+        for a, b, v in re.findall(r"points\.get_mut\(\[(\d), (\d)\]\)\.unwrap\(\) = ([0-9.]+);", body):
+            pts[int(b)][int(a)] = float(v)  # column b of the 3 x npoints array is point b
+        out["cases"].append({"name": m.group(1), "line": i + 1, "kernel": kernel, "operator": op,
+                             "wavenumber": float(k_m.group(1)) if k_m else None,
+                             "epsilon": eps, "points": pts, "matrix": mat})
+    assert len(out["cases"]) == len(POTENTIAL_TESTS), [c["name"] for c in out["cases"]]
+    with open(OUT_POT, "w") as f:
+        json.dump(out, f, indent=1)
+    print(f"wrote {len(out['cases'])} cases to {OUT_POT}")
 
 
 if __name__ == "__main__":

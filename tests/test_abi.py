@@ -301,3 +301,18 @@ def test_lower_tile_pairs_rejects_bad_ranges():
 
 def test_device_trim_with_nothing_cached():
     assert lib.bempp_device_trim() == 0
+
+
+def test_potential_of_a_hypersingular_assembler_is_unsupported():
+    """potential_assemble_into_memory checks the operator before touching the device."""
+    pts, cells = shapes.regular_sphere(0)
+    grid = Grid(pts, cells)
+    sp = function_space(grid, create_family(Family.Lagrange, 1, Continuity.Standard))
+    a = create_laplace_assembler(OperatorType.Hypersingular, BoundaryAssemblerOptions())
+    x = np.array([[2.0, 0.0, 0.0]])
+    out = np.empty((1, sp.global_size))
+    st = lib.potential_assemble_into_memory(a._rs_assembler, sp._rs_space,
+                                            ffi.cast("double*", x.ctypes.data), 1,
+                                            ffi.cast("void*", out.ctypes.data))
+    assert st == lib.BemppStatus_Unsupported
+    assert "single and double layer" in _lib.last_error()

@@ -49,3 +49,35 @@ def test_singular_part_is_subset_of_dense():
         sing = oracle.assemble(pts, cells, "laplace", op, parts=2, **kw)
         np.testing.assert_allclose(reg + sing, dense, rtol=0, atol=1e-15)
         assert np.count_nonzero(sing) > 0
+
+
+@pytest.fixture(scope="module")
+def golden_potentials():
+    import json
+    import os
+
+    path = os.path.join(os.path.dirname(__file__), "golden", "bempp_cl_octahedron_potentials.json")
+    with open(path) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("index", range(4))
+def test_potential_oracle_matches_bempp_cl(golden_potentials, index):
+    """The four potential-operator comparisons that tests/compare_to_bempp_cl.rs keeps
+    commented out (lines 208-320): single and double layer potentials (Laplace, Helmholtz
+    k = 3) of DP0 on the octahedron at three points, from_cl[dof][point] against
+    matrix[point, dof], absolute epsilon 1e-3, default 37-point rule."""
+    from oracle import potential
+
+    case = golden_potentials["cases"][index]
+    pts, cells = shapes.regular_sphere(0)
+    p = potential.potential(case["points"], pts, cells, case["kernel"], case["operator"],
+                            k=case["wavenumber"] or 0.0)
+    ref = np.array(case["matrix"])
+    if ref.ndim == 3:
+        ref = ref[..., 0] + 1j * ref[..., 1]
+    ref = ref.T  # [point, dof]
+    assert p.shape == ref.shape
+    assert np.abs(p.real - ref.real).max() <= case["epsilon"]
+    if np.iscomplexobj(ref):
+        assert np.abs(p.imag - ref.imag).max() <= case["epsilon"]
