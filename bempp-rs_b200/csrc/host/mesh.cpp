@@ -15,6 +15,9 @@
 #include <cmath>
 #include <cstring>
 
+#include <functional>
+#include <thread>
+#include <string>
 #include "core.h"
 
 void GridT::build_topology() {
@@ -124,60 +127,93 @@ std::vector<std::vector<int64_t>> cell_colouring(const SpaceT& s) {
 // Singular pair enumeration; pairs grouped by configuration (as cell_pairs[config] in
 // make_cell_blocks), vertices visited in increasing order.
 void build_singular_pairs(GridT& g, SingularPairList& out) {
+  // Candidate pairs are enumerated vertex by vertex, each kept by its smallest shared
+  // vertex.  Contiguous vertex ranges go to host threads; concatenating their per-
+  // configuration lists in range order gives exactly the serial order (configuration,
+  // then vertex, then test cell, then trial cell).
   const int ncfg = static_cast<int>(singular_configurations().size());
-  std::vector<std::vector<std::pair<int, int>>> by_cfg(ncfg);
-  for (auto& b : by_cfg) b.reserve(static_cast<size_t>(g.ncells) / 2 + 16);
+  const int64_t nv = g.npoints;
+  const int nthreads = static_cast<int>(std::max<int64_t>(
+      1, std::min<int64_t>({static_cast<int64_t>(std::thread::hardware_concurrency()), 16,
+                            nv / 1024})));
+  std::vector<std::vector<std::vector<std::pair<int, int>>>> parts(
+      nthreads, std::vector<std::vector<std::pair<int, int>>>(ncfg));
   const int* cells = g.cells.data();
-  for (int64_t v = 0; v < g.npoints; ++v)
-    for (int tc : g.vertex_cells[v])
-      for (int sc : g.vertex_cells[v]) {
-        // shared vertices as (test local, trial local), trial local ascending; the pair
-        // belongs to its smallest shared vertex
-        int ts[3], ss[3], n = 0;
-        bool smallest = true;
-        for (int si = 0; si < 3 && smallest; ++si)
-          for (int ti = 0; ti < 3; ++ti)
-            if (cells[3 * tc + ti] == cells[3 * sc + si]) {
-              if (cells[3 * tc + ti] < v) {
-                smallest = false;
-                break;
+  std::vector<std::string> errors(nthreads);
+  auto work = [&](int t) {
+    auto& by_cfg = parts[t];
+    const int64_t v0 = nv * t / nthreads, v1 = nv * (t + 1) / nthreads;
+    for (auto& b : by_cfg) b.reserve(static_cast<size_t>((v1 - v0) * 2) + 16);
+    for (int64_t v = v0; v < v1; ++v)
+      for (int tc : g.vertex_cells[v])
+        for (int sc : g.vertex_cells[v]) {
+          // shared vertices as (test local, trial local), trial local ascending; the pair
+          // belongs to its smallest shared vertex
+          int ts[3], ss[3], n = 0;
+          bool smallest = true;
+          for (int si = 0; si < 3 && smallest; ++si)
+            for (int ti = 0; ti < 3; ++ti)
+              if (cells[3 * tc + ti] == cells[3 * sc + si]) {
+                if (cells[3 * tc + ti] < v) {
+                  smallest = false;
+                  break;
+                }
+                ts[n] = ti;
+                ss[n] = si;
+                ++n;
               }
-              ts[n] = ti;
-              ss[n] = si;
-              ++n;
-            }
-        if (!smallest) continue;
-        // configuration index in the order of singular_configurations(): 9 vertex pairings
-        // (test * 3 + trial), 18 edge pairings (edges opposite et / es, two orientations),
-        // identical cells last
-        int cfg;
-        if (n == 1) {
-          cfg = ts[0] * 3 + ss[0];
-        } else if (n == 2) {
-          const int et = 3 - ts[0] - ts[1], es = 3 - ss[0] - ss[1];
-          cfg = 9 + (et * 3 + es) * 2 + (ts[0] < ts[1] ? 0 : 1);
-        } else if (n == 3 && ts[0] == 0 && ts[1] == 1 && ts[2] == 2) {
-          cfg = 27;
-        } else {
-          throw Error(kInternal, "unknown adjacency configuration");
+          if (!smallest) continue;
+          // configuration index in the order of singular_configurations(): 9 vertex
+          // pairings (test * 3 + trial), 18 edge pairings (edges opposite et / es, two
+          // orientations), identical cells last
+          int cfg = -1;
+          if (n == 1) {
+            cfg = ts[0] * 3 + ss[0];
+          } else if (n == 2) {
+            const int et = 3 - ts[0] - ts[1], es = 3 - ss[0] - ss[1];
+            cfg = 9 + (et * 3 + es) * 2 + (ts[0] < ts[1] ? 0 : 1);
+          } else if (n == 3 && ts[0] == 0 && ts[1] == 1 && ts[2] == 2) {
+            cfg = 27;
+          }
+          if (cfg < 0 || cfg >= ncfg) {
+            errors[t] = "unknown adjacency configuration";
+            return;
+          }
+          by_cfg[cfg].push_back({tc, sc});
         }
-        if (cfg >= ncfg) throw Error(kInternal, "unknown adjacency configuration");
-        by_cfg[cfg].push_back({tc, sc});
-      }
-  size_t total = 0;
-  for (const auto& b : by_cfg) total += b.size();
-  out.test_cell.clear();
-  out.trial_cell.clear();
-  out.config.clear();
-  out.test_cell.reserve(total);
-  out.trial_cell.reserve(total);
-  out.config.reserve(total);
-  for (int c = 0; c < ncfg; ++c)
-    for (auto& p : by_cfg[c]) {
-      out.test_cell.push_back(p.first);
-      out.trial_cell.push_back(p.second);
-      out.config.push_back(c);
+  };
+  auto run = [&](const std::function<void(int)>& fn) {
+    if (nthreads == 1) {
+      fn(0);
+      return;
     }
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthreads; ++t) pool.emplace_back(fn, t);
+    for (auto& th : pool) th.join();
+  };
+  run(work);
+  for (const auto& e : errors)
+    if (!e.empty()) throw Error(kInternal, e);
+  // slice of (configuration c, thread t) in the output: configuration-major, then threads
+  std::vector<size_t> start(static_cast<size_t>(ncfg) * nthreads + 1, 0);
+  for (int c = 0; c < ncfg; ++c)
+    for (int t = 0; t < nthreads; ++t)
+      start[c * nthreads + t + 1] = start[c * nthreads + t] + parts[t][c].size();
+  const size_t total = start.back();
+  out.test_cell.resize(total);
+  out.trial_cell.resize(total);
+  out.config.resize(total);
+  run([&](int t) {
+    for (int c = 0; c < ncfg; ++c) {
+      size_t o = start[c * nthreads + t];
+      for (const auto& p : parts[t][c]) {
+        out.test_cell[o] = p.first;
+        out.trial_cell[o] = p.second;
+        out.config[o] = c;
+        ++o;
+      }
+    }
+  });
 }
 
 // Tile layout for the scatter kernel: tiles of `tile` consecutive cells, their sorted
