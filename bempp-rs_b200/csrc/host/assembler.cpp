@@ -317,13 +317,20 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
   SingularArgs sa;
   SingularRules rules{};
   SingularPairs pairs{};
-  if (singular) {
+  // the pair list and the Duffy rules are built at the first singular launch, so that on
+  // a fresh grid the host builds them while the first regular kernel runs
+  bool pairs_ready = false;
+  auto ensure_pairs = [&] {
+    if (pairs_ready) return;
     SingularPairList& pl = grid_pairs(*test.grid, device);
     const DeviceRules& dr = device_rules(device, order);
     rules = SingularRules{dr.offset.as<int>(), dr.test_xi.as<double>(), dr.trial_xi.as<double>(),
                           dr.w.as<double>()};
     pairs = SingularPairs{static_cast<int>(pl.test_cell.size()), pl.d_test.as<int>(),
                           pl.d_trial.as<int>(), pl.d_config.as<int>()};
+    pairs_ready = true;
+  };
+  if (singular) {
     sa.kernel = a.kernel;
     sa.op = a.op;
     sa.k = a.k;
@@ -334,6 +341,7 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
     sa.pair_values = nullptr;
   }
   auto run_singular = [&](int lo, int hi, cudaStream_t s) {
+    ensure_pairs();
     sa.trial_lo = lo;
     sa.trial_hi = hi;
     BEMPP_CUDA(launch_singular(tcs, test.d_dofs.as<int>(), test.nbasis, scs,
