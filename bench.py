@@ -11,7 +11,9 @@ Other workloads: ``helmholtz_sl`` (Helmholtz single layer, k = 8, DP0, complex12
 perturbed 20,480-triangle sphere, 419 M entries) and ``laplace_sl`` (Laplace single layer,
 DP0, f64, 1,280-triangle icosphere).  The default run also measures the Helmholtz
 single-layer FP64 and mixed-precision assemblies and reports their speed ratio and the
-mixed result's relative Frobenius error against the FP64 result (``north_star`` key).
+mixed result's relative Frobenius error against the FP64 result (``helmholtz_sl_fp64_vs_mixed``
+key, with the Helmholtz DL / ADL / HS P1 operators), the adjoint gradient against one
+forward assembly (``adjoint``) and the batched wavenumber sweep (``sweep``).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload p1|helmholtz_sl|laplace_sl] [--precision fp64|mixed]
@@ -303,7 +305,7 @@ class Workload:
         return t0.elapsed_time(t1) / steps, launches
 
 
-def north_star(args):
+def helmholtz_sl_fp64_vs_mixed(args):
     """Helmholtz SL (k=8, DP0, 20,480 triangles): FP64 vs mixed assembly time and error."""
     import torch
 
@@ -372,7 +374,7 @@ def helmholtz_p1_ops(args):
 
 
 def adjoint_timing(args):
-    """Config 5: gradient of Re(lambda^H A mu) (Helmholtz SL, DP0, k = 5, perturbed
+    """Adjoint gradient of Re(lambda^H A mu) (Helmholtz SL, DP0, k = 5, perturbed
     5,120-triangle icosphere) against one FP64 forward assembly, device times."""
     import torch
 
@@ -456,7 +458,7 @@ def adjoint_timing(args):
 
 
 def sweep_timing(args):
-    """Config 4: Helmholtz SL DP0 sweep, 32 wavenumbers in [1, 20], three stretched
+    """Batched Helmholtz SL DP0 sweep, 32 wavenumbers in [1, 20], three stretched
     icospheres (1,280 / 5,120 / 20,480 triangles, axes U(0.8, 1.2) with seeds 1280 / 5120 /
     20480); complex64 outputs (114 GB) resident in HBM; one graph launch per sweep."""
     import torch
@@ -543,7 +545,7 @@ def run_ours(args):
     value = world * wl.entries_per_step / (ms_per_step * 1e-3)
 
     mixed_same = None
-    if rank == 0 and not args.skip_north_star and args.precision == "fp64":
+    if rank == 0 and not args.skip_comparisons and args.precision == "fp64":
         # the same workload with FP32 far pairs: speed and error against the FP64 result
         ref = [o.clone() for o in wl.outs]
         wm = Workload(w, "mixed", args.level)
@@ -628,10 +630,10 @@ def run_ours(args):
     }
 
     ns = adj = swp = None
-    if rank == 0 and args.workload == "p1" and not args.skip_north_star:
+    if rank == 0 and args.workload == "p1" and not args.skip_comparisons:
         del wl.outs
         torch.cuda.empty_cache()
-        ns = north_star(args)
+        ns = helmholtz_sl_fp64_vs_mixed(args)
         adj = adjoint_timing(args)
         torch.cuda.empty_cache()
         swp = None if args.skip_sweep else sweep_timing(args)
@@ -654,7 +656,7 @@ def run_ours(args):
         if mixed_same is not None:
             line["mixed_same_workload"] = mixed_same
         if ns is not None:
-            line["north_star"] = ns
+            line["helmholtz_sl_fp64_vs_mixed"] = ns
         if adj is not None:
             line["adjoint"] = adj
         if swp is not None:
@@ -745,7 +747,8 @@ def main():
     ap.add_argument("--cpu-sample-cells", type=int, default=160)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
-    ap.add_argument("--skip-north-star", action="store_true")
+    ap.add_argument("--skip-comparisons", action="store_true",
+                    help="skip the mixed-precision, Helmholtz, adjoint and sweep measurements")
     ap.add_argument("--skip-sweep", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
