@@ -413,8 +413,7 @@ __device__ __forceinline__ void far_sums_x2(const Tile& T, int it, const Tile& S
   constexpr bool kC = KER == kHelmholtz;
   constexpr bool kNeedBasis = OP != kHS || kC;
   constexpr bool kKahan = NBT == 1 && NBS == 1;
-  float cmp_re = 0.f;
-  float2 acc2 = f2(0.f), cmp2 = f2(0.f);  // kKahan, Helmholtz: (re, im) summed together
+  float cmp_re = 0.f, cmp_im = 0.f;
   const float2 r0sq2 = f2(fp.r0sq), r0f2 = f2(fp.r0f), kf2 = f2(fp.kf), nkf2 = f2(-fp.kf);
 #pragma unroll 1
   for (int p = 0; p < QT; ++p) {
@@ -491,11 +490,9 @@ __device__ __forceinline__ void far_sums_x2(const Tile& T, int it, const Tile& S
     }
     if (kNeedBasis) {
       const float wp = rule.wf[p] * apf;
-      if (kKahan && kC) {
-        const float2 v = fadd2(make_float2(u_re[0].x, u_im[0].x), make_float2(u_re[0].y, u_im[0].y));
-        kahan_add2(acc2, cmp2, fmul2(f2(wp), v));
-      } else if (kKahan) {
+      if (kKahan) {
         kahan_add(blk_re[0][0], cmp_re, wp * (u_re[0].x + u_re[0].y));
+        if (kC) kahan_add(blk_im[0][0], cmp_im, wp * (u_im[0].x + u_im[0].y));
       } else {
 #pragma unroll
         for (int a = 0; a < NBT; ++a) {
@@ -508,10 +505,6 @@ __device__ __forceinline__ void far_sums_x2(const Tile& T, int it, const Tile& S
         }
       }
     }
-  }
-  if (kKahan && kC) {
-    blk_re[0][0] = acc2.x;
-    blk_im[0][0] = acc2.y;
   }
 }
 

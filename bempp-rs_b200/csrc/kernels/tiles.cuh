@@ -235,14 +235,6 @@ __device__ __forceinline__ void poly_cos_sin2(float2 t, float2& c, float2& s) {
   s = fmul2(t, ffma2(z, ffma2(z, ffma2(z, f2(-1.948277516e-4f), f2(8.331875683e-3f)),
                               f2(-1.666664881e-1f)), f2(1.0f)));
 }
-// Kahan-compensated sum of two independent streams (sum.x, sum.y) at once
-__device__ __forceinline__ void kahan_add2(float2& sum, float2& comp, float2 v) {
-  const float2 y = ffma2(comp, f2(-1.0f), v);    // v - comp
-  const float2 t = fadd2(sum, y);
-  comp = ffma2(y, f2(-1.0f), ffma2(sum, f2(-1.0f), t));  // (t - sum) - y
-  sum = t;
-}
-
 // cos and sin of an argument of any moderate size: Cody-Waite reduction by multiples of
 // pi/2 (two-part constant) to |r| <= pi/4, the polynomials above there, and the
 // quadrant's exchange of sine and cosine.  FP32 arguments up to a few hundred.
