@@ -1,12 +1,18 @@
-"""Boundary assembly.
+"""Dense boundary-operator assembly on the GPU, from Python.
 
-Mirrors python/bempp/assembly/boundary.py of bempp-rs: ``BoundaryAssemblerOptions``,
-``BoundaryAssembler.assemble`` (dense, Fortran order), ``assemble_singular`` (SciPy
-CSR) and ``create_laplace_assembler`` keep their names, arguments and errors.
-Additions: ``create_helmholtz_assembler`` (the C function exists in the reference,
-src/bindings/boundary_assemblers.rs:168-210, but had no Python wrapper),
-``set_precision`` (FP64 or mixed FP32/FP64 regular quadrature), ``assemble_into_device``
-(a device buffer, e.g. a torch CUDA tensor, filled on a CUDA stream), and phase timing.
+The public names, arguments and ValueError texts follow bempp-rs's
+``python/bempp/assembly/boundary.py`` (``BoundaryAssemblerOptions``,
+``BoundaryAssembler.assemble`` returning a Fortran-ordered numpy matrix,
+``assemble_singular`` returning SciPy CSR, ``create_laplace_assembler``), so code written
+against the reference runs unchanged.  Beyond the reference:
+
+* ``create_helmholtz_assembler`` wraps the C factory that the reference exports
+  (src/bindings/boundary_assemblers.rs:168-210) but never wrapped in Python;
+* ``set_precision`` picks FP64 or mixed FP32/FP64 regular quadrature;
+* ``assemble_into_device`` fills a device buffer (a torch CUDA tensor, say) on a CUDA
+  stream without a host round trip, and ``check_device`` reports whether such an
+  assembly completed;
+* phase timing, launch counts and host-copy statistics for measurement.
 """
 
 from __future__ import annotations
@@ -37,7 +43,7 @@ _real = {np.float32: np.float32, np.float64: np.float64, np.complex64: np.float3
 
 
 def _convert_to_scipy(rs_sparse_mat, dtype: typing.Type[np.floating]) -> csr_matrix:
-    """Convert a library CSR matrix to a SciPy CSR matrix (and free it)."""
+    """Copy a library-owned CSR MatrixT into SciPy arrays, then release the MatrixT."""
     if rs_sparse_mat == _ffi.NULL:
         raise RuntimeError(_last_error())
     shape = (_lib.matrix_shape0(rs_sparse_mat), _lib.matrix_shape1(rs_sparse_mat))
@@ -52,7 +58,7 @@ def _convert_to_scipy(rs_sparse_mat, dtype: typing.Type[np.floating]) -> csr_mat
 
 
 class OperatorType(Enum):
-    """Operator type."""
+    """Which boundary operator to assemble (values of the C enum OperatorType)."""
 
     SingleLayer = _lib.OperatorType_SingleLayer
     DoubleLayer = _lib.OperatorType_DoubleLayer
@@ -119,7 +125,10 @@ def _host_output(shape, dtype):
 
 
 class BoundaryAssemblerOptions(object):
-    """Boundary assembler options."""
+    """Quadrature and precision settings of an assembler.
+
+    Once an assembler has been created from an options object, the object is frozen:
+    the setters raise ValueError."""
 
     def __init__(self):
         self._read_only = False
@@ -131,7 +140,8 @@ class BoundaryAssemblerOptions(object):
             self._rs_options = None
 
     def set_regular_quadrature_degree(self, cell: ReferenceCellType, degree: int):
-        """Set the (non-singular) quadrature degree for a cell type."""
+        """Number of points of the rule used on well-separated cell pairs of this cell
+        type (the reference calls it the degree)."""
         if self._read_only:
             raise ValueError("Cannot edit options already being used by an assembler")
         if not _lib.boundary_assembler_options_has_regular_quadrature_degree(
@@ -143,7 +153,7 @@ class BoundaryAssemblerOptions(object):
         )
 
     def regular_quadrature_degree(self, cell: ReferenceCellType) -> int:
-        """Get the (non-singular) quadrature degree for a cell type."""
+        """Points of the regular rule on this cell type."""
         if not _lib.boundary_assembler_options_has_regular_quadrature_degree(
             self._rs_options, cell.value
         ):
@@ -155,7 +165,7 @@ class BoundaryAssemblerOptions(object):
     def set_singular_quadrature_degree(
         self, cell0: ReferenceCellType, cell1: ReferenceCellType, degree: int
     ):
-        """Set the singular quadrature degree for a cell type."""
+        """1-D Gauss order of the Duffy rules used on cell pairs that share a vertex."""
         if self._read_only:
             raise ValueError("Cannot edit options already being used by an assembler")
         if not _lib.boundary_assembler_options_has_singular_quadrature_degree(
@@ -167,7 +177,7 @@ class BoundaryAssemblerOptions(object):
         )
 
     def singular_quadrature_degree(self, cell0: ReferenceCellType, cell1: ReferenceCellType) -> int:
-        """Get the singular quadrature degree for a cell type."""
+        """1-D Gauss order of the Duffy rules of this pair of cell types."""
         if not _lib.boundary_assembler_options_has_singular_quadrature_degree(
             self._rs_options, cell0.value, cell1.value
         ):
@@ -177,13 +187,14 @@ class BoundaryAssemblerOptions(object):
         )
 
     def set_batch_size(self, batch_size: int):
-        """Set the batch size."""
+        """Cell-block size option (kept for API compatibility; the GPU kernels tile
+        cells in blocks of 32 whatever it is)."""
         if self._read_only:
             raise ValueError("Cannot edit options already being used by an assembler")
         _lib.boundary_assembler_options_set_batch_size(self._rs_options, batch_size)
 
     def batch_size(self) -> int:
-        """Get the batch size."""
+        """The cell-block size option."""
         return _lib.boundary_assembler_options_get_batch_size(self._rs_options)
 
     def set_precision(self, precision: Precision):
@@ -198,10 +209,10 @@ class BoundaryAssemblerOptions(object):
 
 
 class BoundaryAssembler(object):
-    """Boundary assembler."""
+    """Assembles one operator (kernel, operator type, scalar type) for pairs of spaces."""
 
     def __init__(self, options: BoundaryAssemblerOptions, rs_assembler, owned: bool = True):
-        """Initialise."""
+        """Wrap a BoundaryAssemblerT; freezes ``options``."""
         if rs_assembler == _ffi.NULL:
             raise ValueError(_last_error())
         self.options = options
@@ -210,7 +221,6 @@ class BoundaryAssembler(object):
         self._owned = owned
 
     def __del__(self):
-        """Delete."""
         if getattr(self, "_owned", False):
             _lib.boundary_assembler_t_free(self._rs_assembler)
 
@@ -222,7 +232,8 @@ class BoundaryAssembler(object):
     def assemble(
         self, trial_space: FunctionSpace, test_space: FunctionSpace
     ) -> npt.NDArray[np.floating]:
-        """Assemble operator into a dense matrix."""
+        """The dense test x trial matrix as a Fortran-ordered numpy array (page-locked
+        when large, so that finished columns arrive by DMA while the rest is computed)."""
         self._check_spaces(trial_space, test_space)
         output = _host_output((test_space.global_size, trial_space.global_size), self.dtype)
         _check(
@@ -237,15 +248,17 @@ class BoundaryAssembler(object):
         return output
 
     def assemble_into_device(self, trial_space: FunctionSpace, test_space: FunctionSpace,
-                             out, stream=None):
-        """Assemble into a device buffer (addition).
+                             out, stream=None, check: bool = False):
+        """Fill a device buffer with the dense matrix (addition).
 
-        ``out`` is a CUDA tensor (or any object with ``data_ptr()``) holding
-        test.global_size x trial.global_size elements of the assembler's dtype in
-        column-major order (a torch tensor of shape (n_trial, n_test), or the transpose
-        view of an (n_test, n_trial) tensor with Fortran strides).  ``stream`` is a
-        cudaStream_t as an int (e.g. ``torch.cuda.current_stream().cuda_stream``);
-        None uses the legacy default stream.  Returns once the work is enqueued.
+        ``out`` is anything with ``data_ptr()`` (a torch CUDA tensor) or a raw device
+        address, with room for test.global_size x trial.global_size elements of the
+        assembler's dtype stored column by column: a torch tensor of shape
+        (n_trial, n_test) is the natural fit.  ``stream`` is a cudaStream_t as an int
+        (``torch.cuda.current_stream().cuda_stream``); None means the legacy default
+        stream.  The call returns as soon as the work is enqueued; with ``check=True``
+        it waits for the stream and raises if the assembly did not complete
+        (``check_device``).
         """
         self._check_spaces(trial_space, test_space)
         ptr = out.data_ptr() if hasattr(out, "data_ptr") else int(out)
@@ -255,11 +268,14 @@ class BoundaryAssembler(object):
                 _ffi.cast("void*", ptr), _ffi.cast("void*", int(stream or 0))),
             "assemble_into_device",
         )
+        if check:
+            check_device(stream)
 
     def assemble_singular(
         self, trial_space: FunctionSpace, test_space: FunctionSpace
     ) -> csr_matrix:
-        """Assemble the singular part of an operator into a CSR matrix."""
+        """Only the entries of cell pairs that share a vertex (the Duffy-rule part), as
+        SciPy CSR; an empty matrix when every such entry is negligible."""
         self._check_spaces(trial_space, test_space)
         return _convert_to_scipy(
             _lib.boundary_assembler_assemble_singular(
@@ -296,7 +312,7 @@ class BoundaryAssembler(object):
 
     @property
     def dtype(self):
-        """Data type."""
+        """Scalar type of the matrices this assembler produces."""
         return _dtypes[_lib.boundary_assembler_dtype(self._rs_assembler)]
 
 
@@ -305,7 +321,7 @@ def create_laplace_assembler(
     options: typing.Optional[BoundaryAssemblerOptions] = None,
     dtype: typing.Type[np.floating] = np.float64,
 ):
-    """Create a Laplace assembler."""
+    """Assembler of a Laplace operator (f32 or f64), G(x, y) = 1 / (4 pi |x - y|)."""
     options = BoundaryAssemblerOptions() if options is None else options
     return BoundaryAssembler(
         options,
@@ -321,7 +337,8 @@ def create_helmholtz_assembler(
     options: typing.Optional[BoundaryAssemblerOptions] = None,
     dtype: typing.Type[np.complexfloating] = np.complex128,
 ):
-    """Create a Helmholtz assembler (wraps helmholtz_boundary_assembler_new)."""
+    """Assembler of a Helmholtz operator (c64 or c128) with wavenumber ``wavenumber``,
+    G(x, y) = exp(i k |x - y|) / (4 pi |x - y|)."""
     options = BoundaryAssemblerOptions() if options is None else options
     real = np.float32 if dtype == np.complex64 else np.float64
     k = np.array([wavenumber], dtype=real)
@@ -333,3 +350,10 @@ def create_helmholtz_assembler(
             _rtypes[dtype]
         ),
     )
+
+
+def check_device(stream=None):
+    """Wait for ``stream`` and raise RuntimeError if a device-memory assembly launched
+    since the last check did not complete: a block of the regular kernels gave up waiting
+    for its shared-memory tile copies (a bounded wait) and wrote none of its entries."""
+    _check(_lib.bempp_device_status(_ffi.cast("void*", int(stream or 0))), "device assembly")

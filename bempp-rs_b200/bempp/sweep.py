@@ -15,15 +15,8 @@ from bempp._lib import check as _check
 from bempp._lib import ffi as _ffi
 from bempp._lib import lib as _lib
 from bempp.assembly.boundary import BoundaryAssemblerOptions
-from bempp.function_space import recreate_grid
+from bempp.function_space import grid_handle
 from ndelement.reference_cell import ReferenceCellType
-
-
-def _grid_handle(grid):
-    if not hasattr(grid, "_bempp_rs_grid"):
-        grid._bempp_rs_grid = recreate_grid(grid)
-        grid._bempp_rs_grid_refcount = 1
-    return grid._bempp_rs_grid
 
 
 def helmholtz_single_layer_sweep(grids, wavenumbers, outputs=None, stream=None,
@@ -31,7 +24,8 @@ def helmholtz_single_layer_sweep(grids, wavenumbers, outputs=None, stream=None,
     import torch
 
     ks = np.ascontiguousarray(wavenumbers, dtype=np.float64)
-    handles = [_grid_handle(g) for g in grids]
+    owners = [grid_handle(g) for g in grids]  # held until the call returns
+    handles = [o.ptr for o in owners]
     if outputs is None:
         outputs = [torch.empty((len(ks), len(g.cells), len(g.cells)), dtype=torch.complex64,
                                device="cuda") for g in grids]

@@ -214,6 +214,25 @@ BemppStatus boundary_assembler_assemble_into_device(BoundaryAssemblerT* a, Space
   });
 }
 
+BemppStatus bempp_device_status(void* stream) {
+  return guarded([&] {
+    BEMPP_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    unsigned n = 0;
+    BEMPP_CUDA(take_stage_timeouts(&n));
+    if (n)
+      throw Error(kIncomplete, std::to_string(n) +
+                                   " tile blocks timed out staging their input; their entries "
+                                   "were not written");
+  });
+}
+
+BemppStatus bempp_set_stage_wait_limit(int32_t polls) {
+  return guarded([&] {
+    if (polls < 0) throw Error(kInvalidArgument, "the poll count must be >= 0");
+    BEMPP_CUDA(set_stage_poll_limit(polls));
+  });
+}
+
 BemppStatus boundary_assembler_assemble_into_memory_ex(BoundaryAssemblerT* a, SpaceT* trial,
                                                        SpaceT* test, void* data) {
   return guarded([&] {
@@ -506,6 +525,24 @@ void space_cell_dofs(SpaceT* s, size_t cell, uintptr_t* dofs) {
     dofs[b] = static_cast<uintptr_t>(s->cell_dofs[cell * s->nbasis + b]);
 }
 
+size_t space_cell_colouring(SpaceT* s, size_t* colours) {
+  size_t n = 0;
+  guarded([&] {
+    require(s, "space");
+    std::vector<std::vector<int64_t>> groups;
+    {
+      std::lock_guard<std::mutex> lock(s->grid->mu);
+      s->grid->build_topology();
+      groups = cell_colouring(*s);
+    }
+    n = groups.size();
+    if (colours)
+      for (size_t c = 0; c < groups.size(); ++c)
+        for (int64_t cell : groups[c]) colours[cell] = c;
+  });
+  return n;
+}
+
 size_t space_global_dof_index(SpaceT* s, size_t local_dof_index) {
   (void)s;
   return local_dof_index;  // serial space: global numbering = local numbering
@@ -563,6 +600,16 @@ static GridT* make_grid(const void* points, size_t npoints, size_t gdim, DType d
   return out;
 }
 
+// ndgrid's single-element grid arrays (src/bindings/ndgrid.rs:18-56).  Layout as ndgrid's
+// SingleElementGrid exposes it: per dimension d = 0..tdim, entity_counts[d] entities;
+// downward_connectivity[d][sd] (sd = 0..d) holds, for each entity of dimension d, its
+// downward_connectivity_shape0[d][sd] sub-entities of dimension sd contiguously (a
+// column-major shape0 x count array).  Used here: cell -> vertex ([2][0], 3 per cell),
+// cell -> edge ([2][1], 3 per cell, local edge i opposite local vertex i) and edge ->
+// vertex ([1][0], 2 per edge).  The topology's vertex ids decide adjacency and vertex
+// DOFs (they may differ from the point indices of `cells`, e.g. when two points at one
+// position are one vertex); the edge numbering is kept.  Entity ids and the upward
+// connectivity carry nothing the assembly needs.
 GridT* single_element_grid_borrowed_create_bempp(
     size_t tdim, const size_t* id_sizes, const size_t* const* id_pointers,
     const ReferenceCellType* entity_types, const size_t* entity_counts,
@@ -574,9 +621,6 @@ GridT* single_element_grid_borrowed_create_bempp(
     size_t geometry_degree) {
   (void)id_sizes;
   (void)id_pointers;
-  (void)entity_counts;
-  (void)downward_connectivity;
-  (void)downward_connectivity_shape0;
   (void)upward_connectivity;
   (void)upward_connectivity_lens;
   if (tdim != 2 || (entity_types && entity_types[2] != ReferenceCellType_Triangle)) {
@@ -587,7 +631,60 @@ GridT* single_element_grid_borrowed_create_bempp(
     set_last_error("only flat (degree-1) cells are supported");
     return nullptr;
   }
-  return make_grid(points, npoints, gdim, dtype, cells, ncells, points_per_cell);
+  GridT* g = make_grid(points, npoints, gdim, dtype, cells, ncells, points_per_cell);
+  if (!g || !downward_connectivity) return g;
+  const BemppStatus st = guarded([&] {
+    require(entity_counts, "entity_counts");
+    require(downward_connectivity_shape0, "downward_connectivity_shape0");
+    const size_t nv = entity_counts[0], ne = entity_counts[1];
+    if (entity_counts[2] != ncells)
+      throw Error(kInvalidArgument, "entity_counts[2] differs from the number of cells");
+    if (nv > static_cast<size_t>(INT32_MAX) || ne > static_cast<size_t>(INT32_MAX))
+      throw Error(kUnsupported, "too many topological entities for 32-bit ids");
+    auto conn = [&](int d, int sd, size_t per) -> const size_t* {
+      if (!downward_connectivity[d] || !downward_connectivity_shape0[d])
+        throw Error(kInvalidArgument, "missing downward connectivity of dimension " + std::to_string(d));
+      if (downward_connectivity_shape0[d][sd] != per)
+        throw Error(kInvalidArgument, "downward connectivity [" + std::to_string(d) + "][" +
+                                          std::to_string(sd) + "] must have " +
+                                          std::to_string(per) + " entries per entity");
+      return require(downward_connectivity[d][sd], "downward connectivity array");
+    };
+    const size_t* cv = conn(2, 0, 3);
+    g->topo.resize(3 * ncells);
+    for (size_t i = 0; i < 3 * ncells; ++i) {
+      if (cv[i] >= nv) throw Error(kInvalidArgument, "cell -> vertex index out of range");
+      g->topo[i] = static_cast<int>(cv[i]);
+    }
+    g->nvertices = static_cast<int64_t>(nv);
+    if (ne > 0 && downward_connectivity[2][1] && downward_connectivity[1]) {
+      const size_t* ce = conn(2, 1, 3);
+      const size_t* ev = conn(1, 0, 2);
+      g->given_edge_vertices.resize(2 * ne);
+      for (size_t i = 0; i < 2 * ne; ++i) {
+        if (ev[i] >= nv) throw Error(kInvalidArgument, "edge -> vertex index out of range");
+        g->given_edge_vertices[i] = static_cast<int>(ev[i]);
+      }
+      g->given_cell_edges.resize(3 * ncells);
+      for (size_t c = 0; c < ncells; ++c)
+        for (int i = 0; i < 3; ++i) {
+          const size_t e = ce[3 * c + i];
+          if (e >= ne) throw Error(kInvalidArgument, "cell -> edge index out of range");
+          // local edge i joins the cell's two vertices other than vertex i
+          const int a = g->topo[3 * c + (i + 1) % 3], b = g->topo[3 * c + (i + 2) % 3];
+          const int u = g->given_edge_vertices[2 * e], v = g->given_edge_vertices[2 * e + 1];
+          if (!((u == a && v == b) || (u == b && v == a)))
+            throw Error(kInvalidArgument, "cell -> edge connectivity disagrees with the "
+                                          "cell -> vertex connectivity");
+          g->given_cell_edges[3 * c + i] = static_cast<int>(e);
+        }
+    }
+  });
+  if (st != BemppStatus_Ok) {
+    delete g;
+    return nullptr;
+  }
+  return g;
 }
 
 GridT* bempp_grid_from_points_cells(const void* points, size_t npoints, DType dtype,
@@ -742,10 +839,17 @@ BemppStatus bempp_assemble_regular_dp0_noalloc(
     ra.out_type = kernel == kHelmholtz ? kOutC128 : kOutF64;
     ra.ld = static_cast<int64_t>(test_ncells);
     ra.out = out;
-    BEMPP_CUDA(assemble_regular_dp0_noalloc(ra, rule, test_points, test_cells,
-                                            static_cast<int>(test_ncells), trial_points,
-                                            trial_cells, static_cast<int>(trial_ncells),
-                                            static_cast<cudaStream_t>(stream)));
+    if (test_npoints > static_cast<size_t>(INT32_MAX) || trial_npoints > static_cast<size_t>(INT32_MAX))
+      throw Error(kInvalidArgument, "more points than int32 vertex indices can address");
+    unsigned bad = 0;
+    BEMPP_CUDA(assemble_regular_dp0_noalloc(
+        ra, rule, test_points, static_cast<int>(test_npoints), test_cells,
+        static_cast<int>(test_ncells), trial_points, static_cast<int>(trial_npoints), trial_cells,
+        static_cast<int>(trial_ncells), &bad, static_cast<cudaStream_t>(stream)));
+    if (bad != 0)
+      throw Error(kInvalidArgument, std::to_string(bad) +
+                                        " cell vertex index(es) outside [0, npoints); nothing "
+                                        "was assembled");
   });
 }
 

@@ -92,6 +92,7 @@ void ensure_grid_device(GridT& g, int device) {
     throw Error(kUnsupported, "grid too large for 32-bit cell indices");
   g.d_points.upload(g.points);
   g.d_cells.upload(g.cells);
+  if (!g.topo.empty()) g.d_topo.upload(g.topo);
   g.device = device;
 }
 
@@ -110,6 +111,7 @@ const GridGeometry& grid_geometry(GridT& g, int device, const RegularRule& rule,
     geo->qrel.alloc(sizeof(float4) * qrel_rows(rule.npts) * S);
     geo->vids.alloc(sizeof(int) * 3 * S);
     BEMPP_CUDA(launch_geometry(g.d_points.as<double>(), g.d_cells.as<int>(),
+                               g.topo.empty() ? nullptr : g.d_topo.as<int>(),
                                static_cast<int>(n), rule, geo->geom.as<double>(),
                                geo->qpts.as<double>(), geo->qrel.as<float4>(),
                                geo->vids.as<int>(), stream));

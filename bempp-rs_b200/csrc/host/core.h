@@ -26,7 +26,8 @@ enum Status : int32_t {
   kOutOfMemory = 3,
   kCudaError = 4,
   kNoDevice = 5,
-  kInternal = 6
+  kInternal = 6,
+  kIncomplete = 7
 };
 
 struct Error : std::runtime_error {
@@ -144,14 +145,25 @@ using bempp_b200::DeviceBuffer;
 struct GridT {
   uint64_t uid = 0;            // unique per grid object (plans keyed by it)
   std::vector<double> points;  // npoints x 3
-  std::vector<int> cells;      // ncells x 3 (triangle vertices)
+  std::vector<int> cells;      // ncells x 3 (triangle vertices as point indices: geometry)
   int64_t npoints = 0, ncells = 0;
+  // Topology vertex of each cell corner (ncells x 3), when the grid came with ndgrid's
+  // cell -> vertex connectivity; empty: the point indices of `cells` are the vertices.
+  // Adjacency (singular pairs, near-field vertex tests) and vertex DOFs use these ids.
+  std::vector<int> topo;
+  int64_t nvertices = 0;
+  // ndgrid's cell -> edge connectivity (local edge i opposite local vertex i) and edge ->
+  // vertex connectivity, when given; build_topology then keeps ndgrid's edge numbering.
+  std::vector<int> given_cell_edges;    // ncells x 3
+  std::vector<int> given_edge_vertices; // nedges x 2
+  const int* vtx() const { return topo.empty() ? cells.data() : topo.data(); }
+  int64_t nverts() const { return topo.empty() ? npoints : nvertices; }
   uint8_t dtype = 1;
   std::vector<std::vector<int>> vertex_cells;  // upward connectivity, increasing cell index
   std::vector<std::pair<int, int>> edges;      // unique edges (v0 < v1)
   std::vector<std::array<int, 3>> cell_edges;  // local edge i opposite local vertex i
   int device = -1;
-  DeviceBuffer d_points, d_cells;
+  DeviceBuffer d_points, d_cells, d_topo;
   std::map<int, std::unique_ptr<bempp_b200::GridGeometry>> geometry;  // keyed by regular npts
   std::unique_ptr<bempp_b200::SingularPairList> pairs;
   DeviceBuffer adjoint_scratch;  // per-cell vertex gradients of the adjoint kernel

@@ -246,7 +246,10 @@ void host_copy(const Group& g, const void* slot, void* dst) {
 void check_stage_timeouts() {
   unsigned n = 0;
   BEMPP_CUDA(take_stage_timeouts(&n));
-  if (n) throw Error(kCudaError, std::to_string(n) + " tile blocks timed out staging their input");
+  if (n)
+    throw Error(kIncomplete, std::to_string(n) +
+                                 " tile blocks timed out staging their input; their entries "
+                                 "were not written");
 }
 
 // True when both ends of [p, p + bytes) are page-locked host memory known to CUDA

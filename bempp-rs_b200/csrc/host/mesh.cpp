@@ -22,9 +22,23 @@
 
 void GridT::build_topology() {
   if (!vertex_cells.empty() || ncells == 0) return;
-  vertex_cells.assign(npoints, {});
+  const int* vx = vtx();
+  vertex_cells.assign(nverts(), {});
   for (int64_t c = 0; c < ncells; ++c)
-    for (int i = 0; i < 3; ++i) vertex_cells[cells[3 * c + i]].push_back(static_cast<int>(c));
+    for (int i = 0; i < 3; ++i) vertex_cells[vx[3 * c + i]].push_back(static_cast<int>(c));
+  if (!given_cell_edges.empty()) {
+    // ndgrid's own edge numbering (validated when the grid was created)
+    const int64_t ne = static_cast<int64_t>(given_edge_vertices.size() / 2);
+    edges.resize(ne);
+    for (int64_t e = 0; e < ne; ++e) {
+      const int a = given_edge_vertices[2 * e], b = given_edge_vertices[2 * e + 1];
+      edges[e] = {std::min(a, b), std::max(a, b)};
+    }
+    cell_edges.resize(ncells);
+    for (int64_t c = 0; c < ncells; ++c)
+      for (int i = 0; i < 3; ++i) cell_edges[c][i] = given_cell_edges[3 * c + i];
+    return;
+  }
   // edges: numbered in first-visit order over cells and local edges [1,2], [0,2], [0,1]
   // (an open-addressing hash table of the packed vertex pairs)
   cell_edges.resize(ncells);
@@ -35,7 +49,7 @@ void GridT::build_topology() {
   std::vector<int> vals(cap, -1);
   for (int64_t c = 0; c < ncells; ++c)
     for (int e = 0; e < 3; ++e) {
-      const int a = cells[3 * c + local[e][0]], b = cells[3 * c + local[e][1]];
+      const int a = vx[3 * c + local[e][0]], b = vx[3 * c + local[e][1]];
       const uint64_t key = (static_cast<uint64_t>(std::min(a, b)) << 32) | static_cast<uint32_t>(std::max(a, b));
       size_t h = static_cast<size_t>((key * 0x9E3779B97F4A7C15ull) >> 17) & (cap - 1);
       while (keys[h] != key && keys[h] != ~uint64_t(0)) h = (h + 1) & (cap - 1);
@@ -61,7 +75,7 @@ SpaceT* make_space(GridT* grid, const ElementFamilyT& fam) {
   s->continuous = fam.continuity == 0 && fam.degree >= 1;
   s->dtype = fam.dtype;
   const int64_t nc = grid->ncells;
-  s->entity_dofs[0].assign(grid->npoints, {});
+  s->entity_dofs[0].assign(grid->nverts(), {});
   s->entity_dofs[1].assign(grid->edges.size(), {});
   s->entity_dofs[2].assign(nc, {});
   if (fam.degree == 0) {
@@ -79,7 +93,7 @@ SpaceT* make_space(GridT* grid, const ElementFamilyT& fam) {
     int64_t size = 0;
     for (int64_t c = 0; c < nc; ++c)
       for (int i = 0; i < 3; ++i) {
-        auto& ed = s->entity_dofs[0][grid->cells[3 * c + i]];
+        auto& ed = s->entity_dofs[0][grid->vtx()[3 * c + i]];
         if (ed.empty()) ed.push_back(size++);
         s->cell_dofs[3 * c + i] = ed[0];
       }
@@ -101,12 +115,12 @@ std::vector<std::vector<int64_t>> cell_colouring(const SpaceT& s) {
   const GridT& g = *s.grid;
   const bool vertex_based = s.continuous;
   std::vector<std::vector<int64_t>> colours;
-  std::vector<std::vector<int>> entity_colours(vertex_based ? g.npoints : g.ncells);
+  std::vector<std::vector<int>> entity_colours(vertex_based ? g.nverts() : g.ncells);
   for (int64_t c = 0; c < g.ncells; ++c) {
     int ents[3];
     int ne = 0;
     if (vertex_based)
-      for (int i = 0; i < 3; ++i) ents[ne++] = g.cells[3 * c + i];
+      for (int i = 0; i < 3; ++i) ents[ne++] = g.vtx()[3 * c + i];
     else
       ents[ne++] = static_cast<int>(c);
     int col = 0;
@@ -132,13 +146,13 @@ void build_singular_pairs(GridT& g, SingularPairList& out) {
   // configuration lists in range order gives exactly the serial order (configuration,
   // then vertex, then test cell, then trial cell).
   const int ncfg = static_cast<int>(singular_configurations().size());
-  const int64_t nv = g.npoints;
+  const int64_t nv = g.nverts();
   const int nthreads = static_cast<int>(std::max<int64_t>(
       1, std::min<int64_t>({static_cast<int64_t>(std::thread::hardware_concurrency()), 16,
                             nv / 1024})));
   std::vector<std::vector<std::vector<std::pair<int, int>>>> parts(
       nthreads, std::vector<std::vector<std::pair<int, int>>>(ncfg));
-  const int* cells = g.cells.data();
+  const int* cells = g.vtx();  // topology vertices
   std::vector<std::string> errors(nthreads);
   auto work = [&](int t) {
     auto& by_cfg = parts[t];

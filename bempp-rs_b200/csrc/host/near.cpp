@@ -72,7 +72,7 @@ std::vector<TileBall> tile_balls(const std::vector<CellBall>& cells) {
 bool share_vertex(const GridT& a, int64_t i, const GridT& b, int64_t j) {
   for (int u = 0; u < 3; ++u)
     for (int v = 0; v < 3; ++v)
-      if (a.cells[3 * i + u] == b.cells[3 * j + v]) return true;
+      if (a.vtx()[3 * i + u] == b.vtx()[3 * j + v]) return true;
   return false;
 }
 

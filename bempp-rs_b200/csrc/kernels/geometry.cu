@@ -8,7 +8,8 @@
 namespace bempp_b200 {
 
 __global__ void geometry_kernel(const double* __restrict__ points, const int* __restrict__ cells,
-                                int n, RegularRule rule, double* __restrict__ geom,
+                                const int* __restrict__ topo, int n, RegularRule rule,
+                                double* __restrict__ geom,
                                 double* __restrict__ qpts, float4* __restrict__ qrel,
                                 int* __restrict__ vids) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -70,19 +71,20 @@ __global__ void geometry_kernel(const double* __restrict__ points, const int* __
       row1[2 + (p & 1)] = r[3];
     }
   }
-  vids[c] = i0;
-  vids[S + c] = i1;
-  vids[2 * S + c] = i2;
+  // vertex ids for adjacency tests: the topology's when it has its own numbering
+  vids[c] = topo ? topo[3 * c] : i0;
+  vids[S + c] = topo ? topo[3 * c + 1] : i1;
+  vids[2 * S + c] = topo ? topo[3 * c + 2] : i2;
 }
 
-cudaError_t launch_geometry(const double* points, const int* cells, int ncells,
-                            const RegularRule& rule, double* geom, double* qpts, float4* qrel,
-                            int* vids, cudaStream_t stream) {
+cudaError_t launch_geometry(const double* points, const int* cells, const int* topo,
+                            int ncells, const RegularRule& rule, double* geom, double* qpts,
+                            float4* qrel, int* vids, cudaStream_t stream) {
   if (ncells <= 0) return cudaSuccess;
   int threads = 128;
   int blocks = (cell_stride(ncells) + threads - 1) / threads;
-  geometry_kernel<<<blocks, threads, 0, stream>>>(points, cells, ncells, rule, geom, qpts,
-                                                  qrel, vids);
+  geometry_kernel<<<blocks, threads, 0, stream>>>(points, cells, topo, ncells, rule, geom,
+                                                  qpts, qrel, vids);
   return cudaGetLastError();
 }
 

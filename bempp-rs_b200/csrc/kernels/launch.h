@@ -11,15 +11,19 @@
 
 namespace bempp_b200 {
 
-// Per-cell FP64 geometry, regular quadrature points and vertex ids of a flat-triangle
-// grid (points: npoints x 3 FP64; cells: ncells x 3 int32).
 // Number of regular-kernel blocks since the last call whose shared-memory tile copies
 // did not complete within their bounded wait (and that wrote nothing); resets it.
 cudaError_t take_stage_timeouts(unsigned* count);
+// Polls of the regular kernels' first wait for their tile copies on the current device
+// (default kStagePolls; a test hook: 0 makes every block give up and write nothing).
+cudaError_t set_stage_poll_limit(int polls);
 
-cudaError_t launch_geometry(const double* points, const int* cells, int ncells,
-                            const RegularRule& rule, double* geom, double* qpts, float4* qrel,
-                            int* vids, cudaStream_t stream);
+// Per-cell FP64 geometry, regular quadrature points and vertex ids of a flat-triangle
+// grid (points: npoints x 3 FP64; cells: ncells x 3 int32 point indices; topo: ncells x 3
+// topology vertex ids for the adjacency tests, or null when they are the point indices).
+cudaError_t launch_geometry(const double* points, const int* cells, const int* topo,
+                            int ncells, const RegularRule& rule, double* geom, double* qpts,
+                            float4* qrel, int* vids, cudaStream_t stream);
 
 // Arithmetic of the regular far-pair quadrature.
 enum RegularPrecision : int { kRegularFP64 = 0, kRegularMixed = 1 };
@@ -123,14 +127,17 @@ cudaError_t launch_singular(const CellSet& test, const int* test_dofs, int nbt,
 
 // Allocation-free regular DP0 assembly between two distinct meshes (noalloc.cu); the
 // scratch lives in a static device array of noalloc_max_cells() cells per mesh and
-// noalloc_max_points() regular points.
+// noalloc_max_points() regular points.  The vertex indices are checked on the device
+// first (the call waits for that check): *bad_indices receives the number outside
+// [0, npoints), and when it is non-zero nothing else is launched.
 int noalloc_max_cells();
 int noalloc_max_points();
 cudaError_t assemble_regular_dp0_noalloc(const RegularArgs& args, const RegularRule& rule,
-                                         const double* test_points, const int* test_cells,
-                                         int test_ncells, const double* trial_points,
+                                         const double* test_points, int test_npoints,
+                                         const int* test_cells, int test_ncells,
+                                         const double* trial_points, int trial_npoints,
                                          const int* trial_cells, int trial_ncells,
-                                         cudaStream_t stream);
+                                         unsigned* bad_indices, cudaStream_t stream);
 
 // Adjoint gradient of Re(lambda^H A mu) for the Helmholtz single layer on DP0 (adjoint.cu):
 // grad_points (npoints x 3) and totals = {J, dJ/dk}; grad_cell is F x 9 scratch.

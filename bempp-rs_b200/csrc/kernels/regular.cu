@@ -53,6 +53,10 @@ constexpr float kSmallPhaseMax = 0.8f;
 
 // Blocks whose tile copies did not complete within the bounded wait (never expected).
 __device__ unsigned g_stage_timeouts = 0;
+// Polls of a block's first wait for its tile copies.  Tests lower it to make that wait
+// run out; the second wait, which drains the copies before the block returns, always
+// polls kStagePolls times.
+__device__ int g_stage_poll_limit = tiles::kStagePolls;
 using namespace tiles;
 
 // Curls of the basis functions of a flat cell: t1 d0(phi) - t0 d1(phi); zero for DP0.
@@ -753,7 +757,7 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT>())
                                     : __ldg(tt.inc_ent + static_cast<int64_t>(tx) * 3 * kTile + i - (3 * kTile + 1));
   }
   if (kQueue && threadIdx.x == 0) *qcount = 0;
-  const bool staged = mbar_wait_bounded(mbar, 0);
+  const bool staged = mbar_wait_bounded(mbar, 0, g_stage_poll_limit);
   if (__syncthreads_or(!staged)) {
     // the copies did not complete in time: record it, give them a last bounded wait and
     // leave this block's entries unwritten (the host reports the failure)
@@ -1323,6 +1327,10 @@ cudaError_t dispatch(const CellSet& test, const SpaceTiles& tt, const CellSet& t
 }  // namespace
 
 int scatter_tile_cells() { return kTile; }
+
+cudaError_t set_stage_poll_limit(int polls) {
+  return cudaMemcpyToSymbol(g_stage_poll_limit, &polls, sizeof(int));
+}
 
 cudaError_t take_stage_timeouts(unsigned* count) {
   cudaError_t e = cudaMemcpyFromSymbol(count, g_stage_timeouts, sizeof(unsigned));

@@ -151,10 +151,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* m, unsigned parity) {
   return done != 0;
 }
 
-// Waits for the mbarrier phase with the given parity, giving up after a bounded number
-// of polls (each poll suspends for a hardware-defined interval): true when it completed.
-__device__ inline bool mbar_wait_bounded(uint64_t* m, unsigned parity) {
-  for (int i = 0; i < (1 << 22); ++i)
+constexpr int kStagePolls = 1 << 22;
+
+// Waits for the mbarrier phase with the given parity, giving up after `polls` polls (each
+// poll suspends for a hardware-defined interval): true when it completed.
+__device__ inline bool mbar_wait_bounded(uint64_t* m, unsigned parity, int polls = kStagePolls) {
+  for (int i = 0; i < polls; ++i)
     if (mbar_try_wait(m, parity)) return true;
   return false;
 }

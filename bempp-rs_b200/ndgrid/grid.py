@@ -8,9 +8,14 @@ from ndelement.reference_cell import ReferenceCellType
 
 
 class Grid:
-    """Triangle grid in 3D: points (npoints x 3) and cells (ncells x 3 point indices)."""
+    """Triangle grid in 3D: points (npoints x 3) and cells (ncells x 3 point indices).
 
-    def __init__(self, points, cells):
+    ``cell_vertices`` (optional, ncells x 3) gives the topology's vertex of each cell
+    corner when it differs from the point index, as in an ndgrid grid whose topology
+    joins coincident points; the grid is then handed to the library through ndgrid's
+    single-element-grid arrays (``topology_arrays``)."""
+
+    def __init__(self, points, cells, cell_vertices=None):
         self.points = np.ascontiguousarray(points, dtype=np.float64)
         self.cells = np.ascontiguousarray(cells, dtype=np.uint64)
         if self.points.ndim != 2 or self.points.shape[1] != 3:
@@ -19,6 +24,37 @@ class Grid:
             raise ValueError("cells must be ncells x 3")
         if len(self.cells) and int(self.cells.max()) >= len(self.points):
             raise ValueError("cell vertex index out of range")
+        self.cell_vertices = None
+        if cell_vertices is not None:
+            cv = np.ascontiguousarray(cell_vertices, dtype=np.uint64)
+            if cv.shape != self.cells.shape:
+                raise ValueError("cell_vertices must be ncells x 3")
+            self.cell_vertices = cv
+
+    def topology_arrays(self):
+        """ndgrid-style topology of the grid: entity counts per dimension, cell -> vertex
+        and cell -> edge connectivity (3 per cell; local edge i opposite local vertex i)
+        and edge -> vertex connectivity (2 per edge).  Vertices are ``cell_vertices``
+        (or the point indices); edges are numbered in first-visit order over the cells
+        and their local edges."""
+        cv = self.cells if self.cell_vertices is None else self.cell_vertices
+        nv = int(cv.max()) + 1 if len(cv) else 0
+        index = {}
+        cell_edges = np.zeros_like(cv)
+        edge_vertices = []
+        for c, tri in enumerate(cv.tolist()):
+            for i in range(3):
+                a, b = tri[(i + 1) % 3], tri[(i + 2) % 3]
+                key = (min(a, b), max(a, b))
+                e = index.get(key)
+                if e is None:
+                    e = index[key] = len(edge_vertices)
+                    edge_vertices.append(key)
+                cell_edges[c, i] = e
+        ev = np.array(edge_vertices, dtype=np.uint64).reshape(-1, 2)
+        return {"entity_counts": np.array([nv, len(ev), len(cv)], dtype=np.uint64),
+                "cell_vertices": np.ascontiguousarray(cv), "cell_edges": cell_edges,
+                "edge_vertices": ev}
 
     @property
     def topology_dim(self) -> int:
@@ -30,9 +66,11 @@ class Grid:
 
     def entity_count(self, cell: ReferenceCellType) -> int:
         if cell == ReferenceCellType.Point:
-            return len(np.unique(self.cells))
+            cv = self.cells if self.cell_vertices is None else self.cell_vertices
+            return len(np.unique(cv))
         if cell == ReferenceCellType.Interval:
-            e = np.sort(self.cells[:, [1, 2, 0, 2, 0, 1]].reshape(-1, 2), axis=1)
+            cv = self.cells if self.cell_vertices is None else self.cell_vertices
+            e = np.sort(cv[:, [1, 2, 0, 2, 0, 1]].reshape(-1, 2), axis=1)
             return len(np.unique(e, axis=0))
         if cell == ReferenceCellType.Triangle:
             return len(self.cells)

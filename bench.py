@@ -382,7 +382,7 @@ def adjoint_timing(args):
     from bempp._lib import check, ffi, lib
     from bempp.assembly.boundary import (BoundaryAssemblerOptions, OperatorType,
                                          create_helmholtz_assembler)
-    from bempp.function_space import recreate_grid
+    from bempp.function_space import grid_handle
     from ndelement.reference_cell import ReferenceCellType
 
     k = 5.0
@@ -400,7 +400,7 @@ def adjoint_timing(args):
     stream = torch.cuda.current_stream().cuda_stream
     gopts = BoundaryAssemblerOptions()
     gopts.set_regular_quadrature_degree(ReferenceCellType.Triangle, Q_REGULAR)
-    g = grid._bempp_rs_grid  # the grid handle shared by the space
+    g = grid_handle(grid).ptr  # the grid handle shared by the space
     tot = torch.zeros(2, dtype=torch.float64, device="cuda")
     grad = torch.zeros((len(pts), 3), dtype=torch.float64, device="cuda")
 

@@ -74,7 +74,8 @@ enum {
   BemppStatus_OutOfMemory = 3,
   BemppStatus_CudaError = 4,
   BemppStatus_NoDevice = 5,
-  BemppStatus_Internal = 6
+  BemppStatus_Internal = 6,
+  BemppStatus_Incomplete = 7
 };
 typedef int32_t BemppStatus;
 
@@ -158,6 +159,18 @@ BemppStatus boundary_assembler_assemble_into_memory_ex(BoundaryAssemblerT *assem
 BemppStatus boundary_assembler_assemble_into_device(BoundaryAssemblerT *assembler,
                                                     SpaceT *trial_space, SpaceT *test_space,
                                                     void *device_data, void *stream);
+/* Addition: completion check of device-memory assemblies.  Waits for `stream` (a
+ * cudaStream_t; NULL = legacy default stream), then reports whether any block of the
+ * regular kernels launched on the current device since the last check gave up waiting for
+ * its shared-memory tile copies (a bounded wait; never expected): such a block writes none
+ * of its entries, and the call returns BemppStatus_Incomplete with the block count in
+ * bempp_last_error().  Resets the count.  The host-memory entry points make this check
+ * themselves. */
+BemppStatus bempp_device_status(void *stream);
+/* Addition, a test hook: the number of polls of the regular kernels' first wait for their
+ * tile copies on the current device (default 4194304; 0 makes every block give up at once
+ * and write nothing, after a second full-length wait that drains its copies). */
+BemppStatus bempp_set_stage_wait_limit(int32_t polls);
 /* Addition: record CUDA events around each phase of the next assemblies and read the
  * last durations in milliseconds: [geometry, output clear, regular, singular (+ final
  * conversion)]; returns the number of phases written (at most n).  Reading waits for
@@ -255,6 +268,12 @@ size_t space_global_size(SpaceT *space);
 bool space_has_cell_dofs(SpaceT *space, size_t cell);
 size_t space_cell_dofs_size(SpaceT *space, size_t cell);
 void space_cell_dofs(SpaceT *space, size_t cell, uintptr_t *dofs);
+/* Addition: the greedy cell colouring of FunctionSpace::cell_colouring
+ * (src/function.rs:281-351, which has no C binding in the reference): cells in grid order
+ * take the lowest colour not yet used by a cell sharing one of their DOF entities
+ * (vertices for continuous spaces, the cell itself otherwise).  Writes each cell's colour
+ * to colours[cell] (ncells entries; NULL to query) and returns the number of colours. */
+size_t space_cell_colouring(SpaceT *space, size_t *colours);
 /* src/bindings/space.rs:167-187 */
 size_t space_global_dof_index(SpaceT *space, size_t local_dof_index);
 bool space_is_owned(SpaceT *space, size_t local_dof_index);
@@ -332,15 +351,20 @@ BemppStatus bempp_sweep_last_tuning(int32_t *kchunk, int32_t *blocks_per_sm, dou
  * allocate GPU memory.  It allocates nothing: every input and the output are the
  * caller's device buffers, and the scratch it needs (per-cell geometry and quadrature
  * points) is a fixed static device array held by each GPU that loads the library.
- * Inputs: points (n x 3 FP64) and cells (n x 3 int32, indices < npoints) of each mesh,
- * in device memory.  Output: n_test_cells x n_trial_cells column-major, FP64 (Laplace)
- * or interleaved complex128 (Helmholtz).  Every pair uses the regular rule of
- * `regular_points` points and there is no singular part (the two meshes are treated as
- * different grids), as in boundary_assembler_assemble_into_device with spaces on two
- * grid objects.  Limits: at most 8192 cells per mesh and 12 regular points; larger
- * sizes are rejected with BemppStatus_InvalidArgument.  The first call on a device looks
- * up the array's device address; make that call before any stream capture.  Calls share
- * the array: calls that overlap on the GPU race and must be serialised by the caller. */
+ * Inputs: points (n x 3 FP64) and cells (n x 3 int32) of each mesh, in device memory.
+ * Output: n_test_cells x n_trial_cells column-major, FP64 (Laplace) or interleaved
+ * complex128 (Helmholtz).  Every pair uses the regular rule of `regular_points` points
+ * and there is no singular part (the two meshes are treated as different grids), as in
+ * boundary_assembler_assemble_into_device with spaces on two grid objects.  Limits: at
+ * most 8192 cells per mesh and 12 regular points; larger sizes are rejected with
+ * BemppStatus_InvalidArgument.  Vertex indices are checked on the device against
+ * test_npoints / trial_npoints before any point is read: the call waits for that check
+ * (and for the work queued before it on `stream`) and returns BemppStatus_InvalidArgument,
+ * having written nothing, if an index lies outside [0, npoints); the assembly itself is
+ * then enqueued and the call returns.  The first call on a device looks up the array's
+ * device address; make that call before any stream capture, and do not call it on a
+ * device after cudaDeviceReset.  Calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
 BemppStatus bempp_assemble_regular_dp0_noalloc(
     int32_t kernel, OperatorType operator_type, double k, Precision precision,
     size_t regular_points, const double *test_points, size_t test_npoints,

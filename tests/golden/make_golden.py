@@ -6,9 +6,9 @@ Source: tests/compare_to_bempp_cl.rs of bempp-rs (the eight active tests at line
 compares entry (i, j) of bempp-rs's matrix with ``from_cl[perm[i]][perm[j]]`` (perm is
 the identity for DP0) within an absolute ``epsilon``.
 
-Run in a checkout that has the reference at REFERENCE (default /root/reference):
+Give the root of a bempp-rs checkout as the one argument:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <path to bempp-rs>
 
 It writes tests/golden/bempp_cl_octahedron.json and, from the four potential-operator
 tests that the file keeps commented out (lines 208-320: single and double layer
@@ -24,8 +24,6 @@ import os
 import re
 import sys
 
-REFERENCE = os.environ.get("REFERENCE", "/root/reference")
-SRC = os.path.join(REFERENCE, "tests", "compare_to_bempp_cl.rs")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "bempp_cl_octahedron.json")
 OUT_POT = os.path.join(os.path.dirname(os.path.abspath(__file__)),
                        "bempp_cl_octahedron_potentials.json")
@@ -64,8 +62,8 @@ def parse_matrix(text: str):
     return rows
 
 
-def main():
-    src = open(SRC).read()
+def main(reference: str):
+    src = open(os.path.join(reference, "tests", "compare_to_bempp_cl.rs")).read()
     # only the active (non-commented) tests
     active = "\n".join(line for line in src.splitlines() if not line.lstrip().startswith("//"))
     out = {"source": "bempp-rs tests/compare_to_bempp_cl.rs", "cases": []}
@@ -133,4 +131,6 @@ def potentials(src: str):
 
 
 if __name__ == "__main__":
-    sys.exit(main())
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path to a bempp-rs checkout>")
+    sys.exit(main(sys.argv[1]))

@@ -316,3 +316,137 @@ def test_potential_of_a_hypersingular_assembler_is_unsupported():
                                             ffi.cast("void*", out.ctypes.data))
     assert st == lib.BemppStatus_Unsupported
     assert "single and double layer" in _lib.last_error()
+
+
+# ------------------------------------------------------------------ colouring ---
+def _colouring_checks(grid, space, vertex_disjoint):
+    """The checks of tests/test_space.rs:181-246: every cell in exactly one colour, and
+    (continuous spaces) no two cells of one colour share a vertex."""
+    colouring = space.cell_colouring()[ReferenceCellType.Triangle]
+    cells = [c for group in colouring for c in group]
+    assert sorted(cells) == list(range(len(grid.cells)))  # a partition
+    if vertex_disjoint:
+        cv = grid.cells if grid.cell_vertices is None else grid.cell_vertices
+        for group in colouring:
+            verts = cv[group].ravel()
+            assert len(np.unique(verts)) == len(verts)
+    return colouring
+
+
+def test_colouring_p1():
+    grid = regular_sphere(2)
+    space = function_space(grid, create_family(Family.Lagrange, 1, Continuity.Standard))
+    colouring = _colouring_checks(grid, space, True)
+    assert len(colouring) > 1
+
+
+def test_colouring_dp0_is_one_colour():
+    grid = regular_sphere(2)
+    space = function_space(grid, create_family(Family.Lagrange, 0, Continuity.Discontinuous))
+    assert len(_colouring_checks(grid, space, False)) == 1
+
+
+@pytest.mark.parametrize("degree,cont", [(0, False), (1, True), (1, False)])
+def test_colouring_matches_oracle(degree, cont):
+    pts, cells = shapes.icosphere(2)
+    grid = Grid(pts, cells)
+    space = function_space(grid, create_family(
+        Family.Lagrange, degree, Continuity.Standard if cont else Continuity.Discontinuous))
+    colouring = space.cell_colouring()[ReferenceCellType.Triangle]
+    ours = np.zeros(len(cells), dtype=np.int64)
+    for c, group in enumerate(colouring):
+        ours[group] = c
+    ref, n = oracle.colouring(pts, cells, degree, cont)
+    assert n == len(colouring)
+    assert np.array_equal(ours, ref)
+
+
+# ---------------------------------------------- ndgrid-shaped grid ingestion ---
+def _seam_mesh(level=2):
+    """An icosphere whose cells with an odd index refer to duplicated copies of their
+    points (same coordinates, new point indices); the topology still joins each copy
+    with its original vertex, as an ndgrid grid built with merged vertices would."""
+    pts, cells = shapes.icosphere(level)
+    pts = shapes.radial_perturbation(pts, seed=level)
+    npts = len(pts)
+    dup_cells = cells.copy()
+    odd = np.arange(1, len(cells), 2)
+    dup_cells[odd] += npts
+    points = np.vstack([pts, pts])
+    return points, dup_cells, cells, pts
+
+
+def _pairs(g):
+    n = lib.bempp_grid_singular_pairs(g, ffi.NULL, ffi.NULL, ffi.NULL)
+    t = np.zeros(n, dtype=np.uintp)
+    s = np.zeros(n, dtype=np.uintp)
+    c = np.zeros(n, dtype=np.uintp)
+    lib.bempp_grid_singular_pairs(g, ffi.cast("size_t*", t.ctypes.data),
+                                  ffi.cast("size_t*", s.ctypes.data),
+                                  ffi.cast("size_t*", c.ctypes.data))
+    return set(zip(t.tolist(), s.tolist(), c.tolist()))
+
+
+def test_ndgrid_topology_joins_duplicated_points():
+    """single_element_grid_borrowed_create_bempp with ndgrid's connectivity arrays: the
+    topology's vertices (not the point indices) decide the P1 DOFs, the colouring and the
+    vertex-sharing pairs, so the seam mesh numbers exactly like the merged mesh."""
+    from bempp.function_space import grid_handle
+
+    points, dup_cells, cells, pts = _seam_mesh()
+    seam = Grid(points, dup_cells, cell_vertices=cells)
+    merged = Grid(pts, cells)
+    plain = Grid(points, dup_cells)  # the same arrays without the topology
+    p1 = create_family(Family.Lagrange, 1, Continuity.Standard)
+    s_seam, s_merged, s_plain = (function_space(g, p1) for g in (seam, merged, plain))
+    assert s_seam.global_size == s_merged.global_size == len(pts)
+    assert s_plain.global_size > len(pts)  # without the topology every copy is a vertex
+    ref, n = oracle.cell_dofs(pts, cells, 1, True)
+    assert np.array_equal(np.array([s_seam.cell_dofs(c) for c in range(len(cells))]), ref)
+    a = s_seam.cell_colouring()[ReferenceCellType.Triangle]
+    b = s_merged.cell_colouring()[ReferenceCellType.Triangle]
+    assert a == b
+    assert _pairs(grid_handle(seam).ptr) == _pairs(grid_handle(merged).ptr)
+    assert len(_pairs(grid_handle(plain).ptr)) < len(_pairs(grid_handle(merged).ptr))
+
+
+def test_ndgrid_topology_with_renumbered_vertices():
+    """A topology whose vertex ids are a permutation of the point indices changes nothing
+    the assembly sees: DOFs (first visit) and vertex-sharing pairs are unchanged."""
+    from bempp.function_space import grid_handle
+
+    pts, cells = shapes.icosphere(2)
+    perm = np.random.default_rng(3).permutation(len(pts))
+    renum = Grid(pts, cells, cell_vertices=perm[cells])
+    plain = Grid(pts, cells)
+    p1 = create_family(Family.Lagrange, 1, Continuity.Standard)
+    a, b = function_space(renum, p1), function_space(plain, p1)
+    assert all(a.cell_dofs(c) == b.cell_dofs(c) for c in range(len(cells)))
+    assert _pairs(grid_handle(renum).ptr) == _pairs(grid_handle(plain).ptr)
+    # vertex DOFs are looked up by the topology's vertex id
+    for c in range(0, len(cells), 11):
+        for i in range(3):
+            assert a.get_local_dof_numbers(0, int(perm[cells[c, i]])) == [b.cell_dofs(c)[i]]
+
+
+def test_ndgrid_topology_is_validated():
+    points, dup_cells, cells, pts = _seam_mesh(1)
+    grid = Grid(points, dup_cells, cell_vertices=cells)
+    t = grid.topology_arrays()
+    # an edge list that disagrees with the cells' vertices is refused
+    from bempp.function_space import _ndgrid_create
+
+    t["edge_vertices"][0] = t["edge_vertices"][1]
+    grid.topology_arrays = lambda: t
+    g = _ndgrid_create(grid, np.ascontiguousarray(points), np.ascontiguousarray(dup_cells,
+                                                                               dtype=np.uintp))
+    assert g == ffi.NULL
+    assert "disagrees" in _lib.last_error()
+    # a cell -> vertex id beyond entity_counts[0]
+    t2 = Grid(points, dup_cells, cell_vertices=cells).topology_arrays()
+    t2["entity_counts"][0] = len(pts) - 1
+    grid.topology_arrays = lambda: t2
+    g = _ndgrid_create(grid, np.ascontiguousarray(points), np.ascontiguousarray(dup_cells,
+                                                                               dtype=np.uintp))
+    assert g == ffi.NULL
+    assert "out of range" in _lib.last_error()

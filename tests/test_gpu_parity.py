@@ -125,23 +125,39 @@ def test_gpu_matches_oracle_ico3(kernel, op, sp):
     assert rel_err(a, o) <= FP64_TOL
 
 
-def test_different_grid_objects_have_no_singular_part():
+def oracle_two_grids(g_test, g_trial, kernel, op, k=0.0, q=6):
+    """DP0 x DP0 matrix between cells of two different grids from the oracle: assemble
+    the union grid (g_test's cells, then g_trial's) for g_test's rows and keep the block
+    of g_trial's columns.  Vertices are not shared between the two parts, so that block
+    holds regular-rule entries only, as the assembler computes for two grid objects."""
+    n1 = len(g_test.points)
+    pts = np.vstack([g_test.points, g_trial.points])
+    cells = np.vstack([g_test.cells.astype(np.int64), g_trial.cells.astype(np.int64) + n1])
+    nc = len(g_test.cells)
+    full = oracle_assemble(Grid(pts, cells), kernel, op, k, q=q, test_subset=np.arange(nc))
+    return full[:nc, nc:]
+
+
+@pytest.mark.parametrize("kernel,op,k", [("laplace", "single_layer", 0.0),
+                                         ("laplace", "adjoint_double_layer", 0.0),
+                                         ("helmholtz", "double_layer", 4.0)])
+def test_different_grid_objects_have_no_singular_part(kernel, op, k):
     """Spaces on two grid objects: no pair is skipped and no Duffy rule is used, as
-    equal_grids (pointer equality) in bempp-rs."""
-    pts, cells = shapes.icosphere(1)
-    g1 = Grid(pts + np.array([3.0, 0.0, 0.0]), cells)
-    g2 = Grid(pts, cells)
+    equal_grids (pointer equality) in bempp-rs; here the grids even coincide, so the
+    regular rule also meets the coincident and touching pairs."""
+    pts, cells = shapes.icosphere(2)
+    g1 = Grid(shapes.radial_perturbation(pts, seed=5), cells)
+    g2 = Grid(g1.points.copy(), cells)
     opts = BoundaryAssemblerOptions()
     opts.set_regular_quadrature_degree(ReferenceCellType.Triangle, 6)
-    a = create_laplace_assembler(OperatorType.SingleLayer, opts)
+    a = (create_laplace_assembler(OPS[op], opts) if kernel == "laplace"
+         else create_helmholtz_assembler(OPS[op], k, opts))
     s1 = function_space(g1, create_family(Family.Lagrange, 0, Continuity.Discontinuous))
     s2 = function_space(g2, create_family(Family.Lagrange, 0, Continuity.Discontinuous))
     m = a.assemble(s2, s1)  # trial on g2, test on g1
-    # regular rule on every pair: compare with a direct numpy evaluation
-    from bempp.shapes import icosphere  # noqa: F401
-    o = oracle_assemble(g1, "laplace", "single_layer", q=6, parts=1)  # same-grid regular part
+    o = oracle_two_grids(g1, g2, kernel, op, k)
     assert m.shape == o.shape
-    assert np.all(np.isfinite(m)) and np.all(m > 0)
+    assert rel_err(m, o) <= FP64_TOL
 
 
 def test_singular_csr_matches_dense():
@@ -177,3 +193,69 @@ def test_one_space_symmetric_operators_match_oracle(kernel, op, k, sp):
     o = oracle_assemble(grid, kernel, op, k, test=sp, trial=sp)
     assert rel_err(a, o) <= FP64_TOL
 
+
+
+# ------------------------------------------------- singular part as CSR (row f1) ---
+@pytest.mark.parametrize("kernel,op,k,sp", [
+    ("laplace", "single_layer", 0.0, "dp0"),
+    ("laplace", "double_layer", 0.0, "p1"),
+    ("laplace", "adjoint_double_layer", 0.0, "dp1"),
+    ("laplace", "hypersingular", 0.0, "p1"),
+    ("helmholtz", "single_layer", 3.0, "p1"),
+    ("helmholtz", "hypersingular", 3.0, "p1"),
+])
+def test_singular_csr_matches_oracle_singular_part(kernel, op, k, sp):
+    """assemble_singular (src/boundary_assemblers.rs:121-155) against the oracle's
+    singular part alone (parts=2): the same entries, summed over the pairs that share
+    them, within the FP64 tolerance."""
+    pts, cells = shapes.icosphere(2)
+    grid = Grid(shapes.radial_perturbation(pts, seed=21), cells)
+    opts = BoundaryAssemblerOptions()
+    opts.set_regular_quadrature_degree(ReferenceCellType.Triangle, 6)
+    a = (create_laplace_assembler(OPS[op], opts) if kernel == "laplace"
+         else create_helmholtz_assembler(OPS[op], k, opts))
+    fam = create_family(Family.Lagrange, SPACES[sp][0],
+                        Continuity.Standard if SPACES[sp][1] else Continuity.Discontinuous)
+    s = function_space(grid, fam)
+    csr = a.assemble_singular(s, s)
+    o = oracle_assemble(grid, kernel, op, k, SPACES[sp], SPACES[sp], parts=2)
+    assert csr.shape == o.shape
+    assert csr.nnz > 0
+    assert rel_err(csr.toarray(), o) <= FP64_TOL
+
+
+def test_singular_csr_of_a_negligible_part_is_empty():
+    """src/boundary_assemblers.rs:130-145: when no singular entry exceeds 1e-10 in
+    magnitude the result is an empty CSR matrix of the right shape (a sphere of radius
+    1e-4: every entry is below 1e-10); spaces on two grid objects have no singular part."""
+    pts, cells = shapes.icosphere(1)
+    small = Grid(pts * 1e-4, cells)
+    a = create_laplace_assembler(OperatorType.SingleLayer)
+    s = function_space(small, create_family(Family.Lagrange, 0, Continuity.Discontinuous))
+    csr = a.assemble_singular(s, s)
+    assert csr.shape == (len(cells), len(cells)) and csr.nnz == 0
+    assert np.all(csr.indptr == 0)
+    dense = a.assemble(s, s)
+    assert 0 < np.abs(dense).max() < 1e-10  # the entries exist, they are just negligible
+    g1, g2 = Grid(pts, cells), Grid(pts + 3.0, cells)
+    fam = create_family(Family.Lagrange, 1, Continuity.Standard)
+    csr = a.assemble_singular(function_space(g2, fam), function_space(g1, fam))
+    assert csr.nnz == 0 and csr.shape == (len(pts), len(pts))
+
+
+# ------------------------------------------- ndgrid topology at the boundary (f2) ---
+@pytest.mark.parametrize("kernel,op,sp", [("laplace", "single_layer", "dp0"),
+                                          ("laplace", "hypersingular", "p1"),
+                                          ("helmholtz", "double_layer", "p1")])
+def test_seam_mesh_through_ndgrid_topology_matches_merged_mesh(kernel, op, sp):
+    """Half of the cells refer to duplicated points; the ndgrid topology joins each copy
+    with its original vertex.  The assembler must see the merged surface: singular pairs
+    across the seam and shared P1 DOFs, i.e. the oracle's matrix of the merged mesh."""
+    pts, cells = shapes.icosphere(2)
+    pts = shapes.radial_perturbation(pts, seed=2)
+    dup = cells.copy()
+    dup[1::2] += len(pts)
+    seam = Grid(np.vstack([pts, pts]), dup, cell_vertices=cells)
+    a = gpu_assemble(seam, kernel, op, 4.0, SPACES[sp], SPACES[sp])
+    o = oracle_assemble(Grid(pts, cells), kernel, op, 4.0, SPACES[sp], SPACES[sp])
+    assert rel_err(a, o) <= FP64_TOL
