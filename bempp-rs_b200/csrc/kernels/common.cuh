@@ -126,6 +126,29 @@ __device__ __forceinline__ void sincos_taylor(double r, double& sr, double& cr) 
   sr = r * fma(sr, z, 1.0);
 }
 
+// sin(t) and cos(t) in FP64 for |t| <= 0.8 (pair-referenced phases k (r - r0) of the
+// FP64 regular kernels): Taylor series up to t^15 and t^16; truncation below 7e-17.
+__device__ __forceinline__ void sincos_small(double t, double& s, double& c) {
+  const double z = t * t;
+  c = 1.0 / 20922789888000.0;  // 1/16!
+  c = fma(c, z, -1.0 / 87178291200.0);
+  c = fma(c, z, 1.0 / 479001600.0);
+  c = fma(c, z, -1.0 / 3628800.0);
+  c = fma(c, z, 1.0 / 40320.0);
+  c = fma(c, z, -1.0 / 720.0);
+  c = fma(c, z, 1.0 / 24.0);
+  c = fma(c, z, -0.5);
+  c = fma(c, z, 1.0);
+  double p = -1.0 / 1307674368000.0;  // -1/15!
+  p = fma(p, z, 1.0 / 6227020800.0);
+  p = fma(p, z, -1.0 / 39916800.0);
+  p = fma(p, z, 1.0 / 362880.0);
+  p = fma(p, z, -1.0 / 5040.0);
+  p = fma(p, z, 1.0 / 120.0);
+  p = fma(p, z, -1.0 / 6.0);
+  s = fma(t * z, p, t);
+}
+
 // sin(t) and cos(t) in FP64 for moderate |t| (the phases k r of boundary-element
 // kernels): Cody-Waite reduction r = t - n pi/2 with pi/2 split into two doubles (each
 // step one fused multiply-add), sincos_taylor on |r| <= pi/4, and the quadrant's exchange

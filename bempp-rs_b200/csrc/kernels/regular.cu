@@ -117,9 +117,16 @@ __device__ __forceinline__ void finish_block(const Tile& T, int it, const Tile& 
   }
 }
 
+// How an FP64 Helmholtz block forms e^{ikr}: CUDA's sincos (any phase), the in-tree
+// Cody-Waite sincos_cw (the FP64 near pairs of mixed assemblies), or referenced to the
+// pair, e^{ikr} = e^{ik r0} e^{ik (r - r0)} with r0 = |c_x - c_y|: e^{ik r0} once per pair
+// and e^{ik (r - r0)} from the Taylor series of sincos_small, valid when
+// k (rad_x + rad_y) <= 0.8 bounds every |k (r - r0)| (checked on the host).
+enum F64Phase : int { kF64Sincos = 0, kF64Reduced = 1, kF64Referenced = 2 };
+
 // FP64 local block, test points outermost (every operator but the Laplace adjoint double
 // layer).
-template <int QT, int KER, int OP, int NBT, int NBS, bool kUnroll, bool kFast>
+template <int QT, int KER, int OP, int NBT, int NBS, bool kUnroll, int FPH>
 __device__ __forceinline__ void block_fp64_pq(const Tile& T, int it, const Tile& S, int js,
                                         const RegularRule& rule, double k,
                                         double ore[NBT][NBS], double oim[NBT][NBS]) {
@@ -147,6 +154,15 @@ __device__ __forceinline__ void block_fp64_pq(const Tile& T, int it, const Tile&
     f0 = (OP == kDL ? 1.0 : -1.0) * (dcx * nx + dcy * ny + dcz * nz);
     f1 = D.G(fT0x, cd) * nx + D.G(fT0y, cd) * ny + D.G(fT0z, cd) * nz;
     f2 = D.G(fT1x, cd) * nx + D.G(fT1y, cd) * ny + D.G(fT1z, cd) * nz;
+  }
+  // reference distance of the pair and its phase (kF64Referenced)
+  double kr0 = 0.0, ph_c = 1.0, ph_s = 0.0;
+  if (kC && FPH == kF64Referenced) {
+    const double dcx = T.G(fCx, it) - S.G(fCx, js), dcy = T.G(fCy, it) - S.G(fCy, js),
+                 dcz = T.G(fCz, it) - S.G(fCz, js);
+    const double r0sq = dcx * dcx + dcy * dcy + dcz * dcz;
+    kr0 = k * (r0sq * rsqrt_refined(r0sq));
+    sincos_cw(kr0, ph_s, ph_c);
   }
 #pragma unroll 1
   for (int p = 0; p < Q; ++p) {
@@ -182,7 +198,9 @@ __device__ __forceinline__ void block_fp64_pq(const Tile& T, int it, const Tile&
       {
         const double r = r2 * rinv;
         double sn, cs;
-        if (kFast)
+        if (FPH == kF64Referenced)
+          sincos_small(fma(k, r, -kr0), sn, cs);  // e^{ik (r - r0)}
+        else if (FPH == kF64Reduced)
           sincos_cw(k * r, sn, cs);
         else
           sincos(k * r, &sn, &cs);
@@ -229,6 +247,21 @@ __device__ __forceinline__ void block_fp64_pq(const Tile& T, int it, const Tile&
         }
       }
     }
+  }
+  if (kC && FPH == kF64Referenced) {
+    // apply the pair's reference phase e^{ik r0}
+    const double re = S_re * ph_c - S_im * ph_s, im = S_re * ph_s + S_im * ph_c;
+    S_re = re;
+    S_im = im;
+#pragma unroll
+    for (int a = 0; a < NBT; ++a)
+#pragma unroll
+      for (int b = 0; b < NBS; ++b) {
+        const double br = blk_re[a][b] * ph_c - blk_im[a][b] * ph_s;
+        const double bi = blk_re[a][b] * ph_s + blk_im[a][b] * ph_c;
+        blk_re[a][b] = br;
+        blk_im[a][b] = bi;
+      }
   }
   finish_block<KER, OP, NBT, NBS>(T, it, S, js, k, blk_re, blk_im, S_re, S_im, ore, oim);
 }
@@ -281,16 +314,16 @@ __device__ __forceinline__ void block_fp64_adl_laplace(const Tile& T, int it, co
   finish_block<kLaplace, kADL, NBT, NBS>(T, it, S, js, 0.0, blk_re, blk_im, 0.0, 0.0, ore, oim);
 }
 
-// FP64 local block of test cell `it` (tile T) and trial cell `js` (tile S).
-// kFast (the FP64 near pairs of mixed-precision assemblies): sincos_cw for the phase.
-template <int QT, int KER, int OP, int NBT, int NBS, bool kUnroll = true, bool kFast = false>
+// FP64 local block of test cell `it` (tile T) and trial cell `js` (tile S); FPH: how the
+// Helmholtz phase is formed (F64Phase).
+template <int QT, int KER, int OP, int NBT, int NBS, bool kUnroll = true, int FPH = kF64Sincos>
 __device__ __forceinline__ void block_fp64(const Tile& T, int it, const Tile& S, int js,
                                         const RegularRule& rule, double k,
                                         double ore[NBT][NBS], double oim[NBT][NBS]) {
   if constexpr (KER == kLaplace && OP == kADL)
     block_fp64_adl_laplace<QT, NBT, NBS, kUnroll>(T, it, S, js, rule, ore, oim);
   else
-    block_fp64_pq<QT, KER, OP, NBT, NBS, kUnroll, kFast>(T, it, S, js, rule, k, ore, oim);
+    block_fp64_pq<QT, KER, OP, NBT, NBS, kUnroll, FPH>(T, it, S, js, rule, k, ore, oim);
 }
 
 // Per-pair constants of the FP32 far-pair quadrature.
@@ -804,7 +837,8 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT>())
         if (MIXED)
           block_fp32<QT, KER, OP, NBT, NBS, PH>(T, it, S, js, rule, k, ore, oim);
         else
-          block_fp64<QT, KER, OP, NBT, NBS>(T, it, S, js, rule, k, ore, oim);
+          block_fp64<QT, KER, OP, NBT, NBS, true,
+                     PH == kPhaseSmall ? kF64Referenced : kF64Sincos>(T, it, S, js, rule, k, ore, oim);
         have = true;
         if (DIRECT) {
           if (kC)
@@ -945,7 +979,7 @@ __global__ void __launch_bounds__(kThreads)
   stage_cell(T, lane, test, pr.x, Q);  // this lane's column only: no synchronisation
   stage_cell(S, lane, trial, pr.y, Q);
   double ore[NBT][NBS], oim[NBT][NBS];
-  block_fp64<QT, KER, OP, NBT, NBS, false, true>(T, lane, S, lane, rule, k, ore, oim);
+  block_fp64<QT, KER, OP, NBT, NBS, false, kF64Reduced>(T, lane, S, lane, rule, k, ore, oim);
   if (DIRECT) {
     const int64_t o = static_cast<int64_t>(pr.y) * ld + pr.x;
     if (kC)
@@ -1243,6 +1277,11 @@ cudaError_t launch_one(const CellSet& test, const SpaceTiles& tt, const CellSet&
   if (ny <= 0) return cudaSuccess;
   const int ty0 = a.trial_tile0, ty1 = a.trial_tile0 + ny;
   if constexpr (!MIXED) {
+    // FP64 Helmholtz: phases referenced to the pair (kPhaseSmall) when the host's bound
+    // allows it, else CUDA's sincos of every phase
+    if (KER == kHelmholtz && !a.small_phase)
+      return launch_mode<QT, KER, OP, NBT, NBS, false, DIRECT, kPhaseGeneral, kNearInKernel>(
+          test, tt, trial, st, rule, a, ty0, ty1, stream);
     return launch_mode<QT, KER, OP, NBT, NBS, false, DIRECT, kPhaseSmall, kNearInKernel>(
         test, tt, trial, st, rule, a, ty0, ty1, stream);
   } else {

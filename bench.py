@@ -312,8 +312,13 @@ def helmholtz_sl_fp64_vs_mixed(args):
     w = WORKLOADS["helmholtz_sl"]
     res = {}
     outs = {}
+    sample = None
     for prec in ("fp64", "mixed"):
         wl = Workload(w, prec)
+        if sample is None and not args.skip_cpu:  # CPU baseline leg: oracle rows (checker)
+            sample = oracle_row_sample("helmholtz", w["ops"], w["k"], w["space"], wl.points,
+                                       wl.cells, args.cpu_sample_cells, 1)
+            res["cpu_baseline"] = cpu_baseline(w, wl.points, wl.cells, wl.n, args, sample)
         ms, _ = wl.timed(max(3, args.steps), 2)
         ph = wl.phase_ms()["single_layer"]
         res[prec] = {"ms_per_assembly": ms, "entries_per_s": wl.entries_per_step / (ms * 1e-3),
@@ -329,6 +334,9 @@ def helmholtz_sl_fp64_vs_mixed(args):
                                  "frac": ach / peak if (ach and peak) else None,
                                  "peak_source": "bempp_measure_fma_peak (FMA chains on this GPU)"}
         outs[prec] = wl.outs[0]
+        if sample is not None:
+            res[prec]["rel_frobenius_error_vs_oracle_rows"] = rows_error(wl.outs[0], sample,
+                                                                         "single_layer")
         del wl
         torch.cuda.empty_cache()
     err = (torch.linalg.norm(outs["mixed"] - outs["fp64"]) / torch.linalg.norm(outs["fp64"])).item()
@@ -358,6 +366,12 @@ def helmholtz_p1_ops(args):
     w.update(space="p1", ops=["double_layer", "adjoint_double_layer", "hypersingular"])
     out = {}
     wls = {prec: Workload(w, prec) for prec in ("fp64", "mixed")}
+    sample = None
+    if not args.skip_cpu:  # CPU baseline leg: oracle rows of each operator (checker)
+        wl0 = wls["fp64"]
+        sample = oracle_row_sample("helmholtz", w["ops"], w["k"], w["space"], wl0.points,
+                                   wl0.cells, 27, 2)
+        out["cpu_baseline"] = cpu_baseline(w, wl0.points, wl0.cells, wl0.n, args, sample)
     for prec, wl in wls.items():
         wl.timed(1, 2)
         out[prec] = {name: ph[2] for name, ph in wl.phase_ms().items()}  # regular ms
@@ -366,6 +380,10 @@ def helmholtz_p1_ops(args):
     out["rel_frobenius_error_vs_fp64"] = {
         name: (torch.linalg.norm(a - b) / torch.linalg.norm(b)).item()
         for name, a, b in zip(w["ops"], wls["mixed"].outs, wls["fp64"].outs)}
+    if sample is not None:
+        out["rel_frobenius_error_vs_oracle_rows"] = {
+            prec: {name: rows_error(o, sample, name) for name, o in zip(w["ops"], wl.outs)}
+            for prec, wl in wls.items()}
     out["speedup_mixed_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
     out["workload"] = "helmholtz_dl_adl_hs_p1_ico5_k8_c128"
     del wls
@@ -493,13 +511,27 @@ def sweep_timing(args):
     ms = e0.elapsed_time(e1) / reps
     entries = sum(len(ks) * len(g.cells) ** 2 for g in grids)
     kc, bps, probe = last_tuning()
+    check = None
+    if not args.skip_cpu:
+        # CPU baseline leg as the checker: oracle rows (16 seeded rows per mesh) at the
+        # smallest, a middle and the largest wavenumber of every mesh
+        errs = {}
+        for g, out in zip(grids, outs):
+            pts = g.points
+            cells = g.cells.astype(np.int64)
+            for j in (0, len(ks) // 2, len(ks) - 1):
+                smp = oracle_row_sample("helmholtz", ["single_layer"], float(ks[j]), "dp0", pts,
+                                        cells, 16, j)
+                errs[f"{len(cells)}_k{ks[j]:.3f}"] = rows_error(out[j], smp, "single_layer")
+        check = {"rel_frobenius_error_vs_oracle_rows": errs, "max": max(errs.values()),
+                 "rows_per_matrix": 16}
     del outs
     torch.cuda.empty_cache()
     return {"workload": "helmholtz_sl_dp0_sweep_32k_ico3_4_5_c64", "entries": entries,
             "ms_per_sweep": ms, "entries_per_s": entries / (ms * 1e-3),
             "first_call_s": first_s, "tuning": {"k_per_item": kc, "ctas_per_sm": bps,
                                                 "probe_ms_per_item": probe},
-            "launches_per_sweep": 1}
+            "launches_per_sweep": 1, "parity": check}
 
 
 def run_ours(args):
@@ -544,6 +576,19 @@ def run_ours(args):
     ms_per_step = max_over_ranks(ms_per_step, world)
     value = world * wl.entries_per_step / (ms_per_step * 1e-3)
 
+    # CPU baseline leg: oracle rows of a seeded DOF sample (timed), also the checker of the
+    # GPU's rows of the same DOFs
+    sample = parity = None
+    if rank == 0 and not args.skip_cpu:
+        nrows = args.cpu_sample_cells // 6 if w["space"] == "p1" else args.cpu_sample_cells
+        sample = oracle_row_sample(w["kernel"], w["ops"], w["k"], w["space"], wl.points,
+                                   wl.cells, nrows, 0)
+        parity = {"rel_frobenius_error_vs_oracle_rows": {
+                      op: rows_error(out, sample, op) for op, out in zip(w["ops"], wl.outs)},
+                  "rows": len(sample["rows"]),
+                  "note": "complete rows of seeded test DOFs, GPU output of the timed run "
+                          "against the CPU FP64 oracle"}
+
     mixed_same = None
     if rank == 0 and not args.skip_comparisons and args.precision == "fp64":
         # the same workload with FP32 far pairs: speed and error against the FP64 result
@@ -555,6 +600,9 @@ def run_ours(args):
         mixed_same = {"ms_per_step": ms_mixed, "entries_per_s": wm.entries_per_step / (ms_mixed * 1e-3),
                       "speedup_vs_fp64": ms_per_step / ms_mixed,
                       "rel_frobenius_error_vs_fp64": dict(zip(w["ops"], errs))}
+        if sample is not None:
+            mixed_same["rel_frobenius_error_vs_oracle_rows"] = {
+                op: rows_error(out, sample, op) for op, out in zip(w["ops"], wm.outs)}
         del wm, ref
         torch.cuda.empty_cache()
 
@@ -653,6 +701,8 @@ def run_ours(args):
                        "l2": "flushed between steps (256 MiB write); outputs exceed L2"},
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "clocks": clocks,
         }
+        if parity is not None:
+            line["parity"] = parity
         if mixed_same is not None:
             line["mixed_same_workload"] = mixed_same
         if ns is not None:
@@ -661,8 +711,8 @@ def run_ours(args):
             line["adjoint"] = adj
         if swp is not None:
             line["sweep"] = swp
-        if not args.skip_cpu:
-            line["cpu_baseline"] = cpu_baseline(w, wl.points, wl.cells, wl.n, args)
+        if sample is not None:
+            line["cpu_baseline"] = cpu_baseline(w, wl.points, wl.cells, wl.n, args, sample)
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -670,63 +720,137 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def cpu_baseline(w, points, cells, n, args):
-    """CPU FP64 oracle on a bounded sample: the regular part for a subset of test cells
-    (all trial cells) plus the full singular part, scaled to the whole workload."""
+# ----------------------------------------------------------------- CPU baseline leg ---
+# The only part of this file that runs the oracle (oracle/, the CPU FP64 restatement of the
+# bempp-rs algorithm: OpenMP over 128 x 128 cell blocks, -O3 -march=native): it times the
+# CPU on samples of the workloads and on one complete step (--impl reference), and the
+# complete rows it computes are the checker of the GPU's rows (*_vs_oracle keys).
+
+def _space_degree(space):
+    return (1, True) if space == "p1" else (0, False)
+
+
+def oracle_row_sample(kernel, ops, k, space, points, cells, nrows, seed):
+    """Complete rows of ``nrows`` seeded test DOFs of each operator, from the oracle on all
+    host threads: {"rows", "oracle_rows": {op: rows x n}, "seconds": {op: s},
+    "regular_seconds", "singular_seconds", "test_cells", "threads"}.  The regular part is
+    assembled for the cells holding those DOFs (which completes their rows), the singular
+    part for the whole grid; their sum gives the rows, and the regular time scales with
+    the number of test cells while the singular time is that of the whole step."""
     from oracle import oracle
 
+    deg, cont = _space_degree(space)
     threads = os.cpu_count() or 1
-    nsub = min(args.cpu_sample_cells, len(cells))
-    rng = np.random.default_rng(0)
-    subset = np.sort(rng.choice(len(cells), size=nsub, replace=False))
-    deg = 1 if w["space"] == "p1" else 0
-    kw = dict(k=w["k"], test_degree=deg, test_continuous=bool(deg), trial_degree=deg,
-              trial_continuous=bool(deg), q_regular=Q_REGULAR, q_singular=ORDER,
-              nthreads=threads)
-    t_reg = t_sing = 0.0
-    for op in w["ops"]:
+    dofs, n = oracle.cell_dofs(points, cells, deg, cont)
+    rows = np.sort(np.random.default_rng(seed).choice(n, size=min(nrows, n), replace=False))
+    sub = np.flatnonzero(np.isin(dofs, rows).any(axis=1))
+    out = {"rows": rows, "oracle_rows": {}, "seconds": {}, "regular_seconds": {},
+           "singular_seconds": {}, "test_cells": int(len(sub)), "threads": threads, "n": n}
+    kw = dict(k=k, test_degree=deg, test_continuous=cont, trial_degree=deg,
+              trial_continuous=cont, q_regular=Q_REGULAR, q_singular=ORDER, nthreads=threads)
+    for op in ops:
         t = time.perf_counter()
-        oracle.assemble(points, cells, w["kernel"], op, parts=1, test_subset=subset, **kw)
-        t_reg += time.perf_counter() - t
-        t = time.perf_counter()
-        oracle.assemble(points, cells, w["kernel"], op, parts=2, **kw)
-        t_sing += time.perf_counter() - t
-    est = t_reg * len(cells) / nsub + t_sing
-    return {"value": len(w["ops"]) * n * n / est, "unit": "entries/s", "cores": threads,
-            "kind": "port",
-            "sample": f"regular part of {len(w['ops'])} operator(s) for {nsub} of {len(cells)} "
-                      f"test cells (x all trial cells) scaled by {len(cells) / nsub:.1f}, plus "
-                      "the full singular part; CPU FP64 restatement of the bempp-rs algorithm "
-                      "(OpenMP over 128x128 blocks, -O3 -march=native)",
-            "seconds_estimated_full_step": est}
+        reg = oracle.assemble(points, cells, kernel, op, parts=1, test_subset=sub, **kw)[rows]
+        t1 = time.perf_counter()
+        sing = oracle.assemble(points, cells, kernel, op, parts=2, **kw)[rows]
+        t2 = time.perf_counter()
+        out["regular_seconds"][op] = t1 - t
+        out["singular_seconds"][op] = t2 - t1
+        out["seconds"][op] = t2 - t
+        out["oracle_rows"][op] = reg + sing
+    return out
+
+
+def rows_error(out_tensor, sample, op):
+    """Relative Frobenius error of the GPU's rows (column-major device matrix held as a
+    (n_trial, n_test) tensor) against the oracle's rows of the same DOFs."""
+    import torch
+
+    idx = torch.as_tensor(sample["rows"], device=out_tensor.device)
+    got = out_tensor[:, idx].T.to(torch.complex128 if out_tensor.is_complex() else torch.float64)
+    ref = sample["oracle_rows"][op]
+    got = got.cpu().numpy()
+    return float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+
+
+def cpu_rate(sample, ncells, nops, n):
+    """CPU entries/s of the whole workload estimated from a row sample: the regular time
+    scaled by (all cells / sampled test cells) plus the singular time of the whole grid."""
+    est = (sum(sample["regular_seconds"].values()) * ncells / sample["test_cells"] +
+           sum(sample["singular_seconds"].values()))
+    return nops * n * n / est
+
+
+def cpu_baseline(w, points, cells, n, args, sample=None):
+    """CPU baseline of the headline workload on a bounded sample (about 10-30 s of CPU
+    work): complete rows of a seeded DOF subset of every operator, scaled."""
+    if sample is None:
+        nrows = args.cpu_sample_cells // 6 if w["space"] == "p1" else args.cpu_sample_cells
+        sample = oracle_row_sample(w["kernel"], w["ops"], w["k"], w["space"], points, cells,
+                                   nrows, 0)
+    return {"value": cpu_rate(sample, len(cells), len(w["ops"]), n), "unit": "entries/s",
+            "cores": sample["threads"], "kind": "port",
+            "sample": f"complete rows of {len(sample['rows'])} seeded test DOFs of each of "
+                      f"{len(w['ops'])} operator(s): the regular part for the "
+                      f"{sample['test_cells']} of {len(cells)} test cells holding them (x all "
+                      f"trial cells), time scaled by {len(cells) / sample['test_cells']:.1f}, "
+                      "plus the whole singular part; CPU FP64 restatement of the bempp-rs "
+                      "algorithm (OpenMP over 128x128 blocks, -O3 -march=native)",
+            "sample_seconds": sum(sample["seconds"].values())}
 
 
 def run_reference(args):
+    """The reference arm: the CPU FP64 restatement of the bempp-rs algorithm (the reference
+    itself needs a Rust toolchain, absent here) on all host cores.  It times ONE complete
+    step of the workload (every operator, every row: the value), then --steps sampled steps
+    as a cross-check of the sample-based estimate; warm-up steps are sampled steps."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    w = WORKLOADS[args.workload]
-    points, cells = workload_mesh(w, args.level)
     from oracle import oracle
 
-    deg = 1 if w["space"] == "p1" else 0
-    n = oracle.space_size(points, cells, deg, bool(deg))
-    vals, base = [], None
-    for _ in range(args.steps):
-        base = cpu_baseline(w, points, cells, n, args)
-        vals.append(base["value"])
-    value = statistics.median(vals)
+    w = WORKLOADS[args.workload]
+    points, cells = workload_mesh(w, args.level)
+    deg, cont = _space_degree(w["space"])
+    threads = os.cpu_count() or 1
+    n = oracle.space_size(points, cells, deg, cont)
+    nrows = args.cpu_sample_cells // 6 if w["space"] == "p1" else args.cpu_sample_cells
+    for i in range(args.warmup):  # untimed: small samples (library load, page-in, caches)
+        oracle_row_sample(w["kernel"], w["ops"], w["k"], w["space"], points, cells,
+                          max(1, nrows // 16), i)
+    t = time.perf_counter()
+    for op in w["ops"]:
+        oracle.assemble(points, cells, w["kernel"], op, k=w["k"], test_degree=deg,
+                        test_continuous=cont, trial_degree=deg, trial_continuous=cont,
+                        q_regular=Q_REGULAR, q_singular=ORDER, nthreads=threads)
+    full_s = time.perf_counter() - t
     eps = len(w["ops"]) * n * n
+    value = eps / full_s
+    est = []
+    for i in range(min(args.steps, 2)):
+        smp = oracle_row_sample(w["kernel"], w["ops"], w["k"], w["space"], points, cells, nrows,
+                                100 + i)
+        est.append(cpu_rate(smp, len(cells), len(w["ops"]), n))
+    est_med = statistics.median(est) if est else None
+    sample_desc = (f"one complete step timed: all {len(w['ops'])} operator(s), {n} x {n} each, "
+                   f"{full_s:.1f} s on {threads} threads; cross-check: {len(est)} sampled steps "
+                   f"(complete rows of {nrows} seeded test DOFs per operator, scaled) estimate "
+                   f"{est_med:.4g} entries/s, {est_med / value:.3f} x the measured full step"
+                   if est_med else f"one complete step timed ({full_s:.1f} s)")
     line = {
         "metric": w["metric"], "value": value, "unit": "entries/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": eps / value * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": full_s * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "c128" if w["kernel"] == "helmholtz" else "f64",
         "data": "synthetic (seeded icosphere)", "impl": "reference",
         "config": {"workload": w["name"], "triangles": len(cells), "dofs": n,
                    "operators": w["ops"], "regular_points": Q_REGULAR, "duffy_order": ORDER,
                    "entries_per_step": eps, "parallelism": "host cores"},
-        "cpu_baseline": {**base, "value": value},
+        "full_steps_timed": 1,
+        "sampled_estimate": {"median": est_med, "values": est,
+                             "ratio_to_full_step": (est_med / value) if est_med else None},
+        "cpu_baseline": {"value": value, "unit": "entries/s", "cores": threads, "kind": "port",
+                         "sample": sample_desc},
         "e2e": {"value": value, "unit": "entries/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -744,7 +868,8 @@ def main():
     ap.add_argument("--level", type=int, default=None, help="icosphere refinement override")
     ap.add_argument("--k", type=float, default=None, help="wavenumber override (Helmholtz)")
     ap.add_argument("--once", action="store_true")
-    ap.add_argument("--cpu-sample-cells", type=int, default=160)
+    ap.add_argument("--cpu-sample-cells", type=int, default=640,
+                    help="test DOFs (DP0) or 6 x test DOFs (P1) of the CPU row samples")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-comparisons", action="store_true",

@@ -143,11 +143,11 @@ def oracle_two_grids(g_test, g_trial, kernel, op, k=0.0, q=6):
                                          ("helmholtz", "double_layer", 4.0)])
 def test_different_grid_objects_have_no_singular_part(kernel, op, k):
     """Spaces on two grid objects: no pair is skipped and no Duffy rule is used, as
-    equal_grids (pointer equality) in bempp-rs; here the grids even coincide, so the
-    regular rule also meets the coincident and touching pairs."""
+    equal_grids (pointer equality) in bempp-rs; the second sphere is shifted by less
+    than its radius, so the regular rule also meets close and intersecting cell pairs."""
     pts, cells = shapes.icosphere(2)
     g1 = Grid(shapes.radial_perturbation(pts, seed=5), cells)
-    g2 = Grid(g1.points.copy(), cells)
+    g2 = Grid(shapes.radial_perturbation(pts, seed=6) + np.array([0.5, 0.2, 0.0]), cells)
     opts = BoundaryAssemblerOptions()
     opts.set_regular_quadrature_degree(ReferenceCellType.Triangle, 6)
     a = (create_laplace_assembler(OPS[op], opts) if kernel == "laplace"
