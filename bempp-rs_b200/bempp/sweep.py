@@ -43,10 +43,17 @@ def helmholtz_single_layer_sweep(grids, wavenumbers, outputs=None, stream=None,
     return outputs
 
 
+def set_tuning(kchunk: int = 0, blocks_per_sm: int = 4, tile_shape: int = 1):
+    """Fix the sweep's launch parameters (kchunk = 0: autotune again)."""
+    _check(_lib.bempp_sweep_set_tuning(kchunk, blocks_per_sm, tile_shape), "sweep tuning")
+
+
 def last_tuning():
-    """(wavenumbers per work item, CTAs per SM, probe ms per item) of the last sweep."""
+    """(wavenumbers per work item, CTAs per SM, probe ms per (tile pair, wavenumber),
+    tile shape) of the last sweep."""
     k = _ffi.new("int32_t*")
     b = _ffi.new("int32_t*")
+    s = _ffi.new("int32_t*")
     t = _ffi.new("double*")
-    _check(_lib.bempp_sweep_last_tuning(k, b, t), "sweep tuning")
-    return int(k[0]), int(b[0]), float(t[0])
+    _check(_lib.bempp_sweep_last_tuning(k, b, s, t), "sweep tuning")
+    return int(k[0]), int(b[0]), float(t[0]), int(s[0])

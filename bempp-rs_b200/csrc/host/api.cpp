@@ -15,12 +15,6 @@ using namespace bempp_b200;
 
 namespace bempp_b200 {
 void build_singular_pairs(GridT& g, SingularPairList& out);
-struct SweepTuning {
-  int kchunk = 8;
-  int blocks_per_sm = 4;
-  double probe_ms = 0.0;
-};
-SweepTuning last_sweep_tuning();
 }
 
 struct BoundaryAssemblerOptionsT {
@@ -792,11 +786,17 @@ BemppStatus bempp_helmholtz_single_layer_dp0_sweep_device(GridT* const* grids, s
   });
 }
 
-BemppStatus bempp_sweep_last_tuning(int32_t* kchunk, int32_t* blocks_per_sm, double* probe_ms) {
+BemppStatus bempp_sweep_set_tuning(int32_t kchunk, int32_t blocks_per_sm, int32_t tile_shape) {
+  return guarded([&] { set_sweep_tuning(kchunk, blocks_per_sm, tile_shape); });
+}
+
+BemppStatus bempp_sweep_last_tuning(int32_t* kchunk, int32_t* blocks_per_sm, int32_t* tile_shape,
+                                    double* probe_ms) {
   return guarded([&] {
     const SweepTuning t = last_sweep_tuning();
     if (kchunk) *kchunk = t.kchunk;
     if (blocks_per_sm) *blocks_per_sm = t.blocks_per_sm;
+    if (tile_shape) *tile_shape = t.tile_shape;
     if (probe_ms) *probe_ms = t.probe_ms;
   });
 }

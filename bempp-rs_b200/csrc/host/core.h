@@ -277,7 +277,16 @@ void helmholtz_sl_gradient_device(GridT& g, const Options& opts, double k, const
 // column-major ncells_i^2 matrices, wavenumber-major.
 void helmholtz_sl_sweep_device(GridT* const* grids, size_t ngrids, const double* ks, size_t nk,
                                const Options& opts, void* const* outs, cudaStream_t stream);
-struct SweepTuning;
+// Launch parameters the sweep's autotuner chose (sweep.cpp).
+struct SweepTuning {
+  int kchunk = 8;         // wavenumbers per work item
+  int blocks_per_sm = 4;  // CTAs per SM of the persistent grid
+  int tile_shape = 1;     // a work item covers tile_shape x tile_shape 32-cell tile pairs
+  double probe_ms = 0.0;  // probe milliseconds per (tile pair, wavenumber)
+};
+SweepTuning last_sweep_tuning();
+// Fixes the sweep's launch parameters (kchunk <= 0: autotune again).
+void set_sweep_tuning(int kchunk, int blocks_per_sm, int tile_shape);
 // Singular part as CSR (host).
 MatrixT* assemble_singular_csr(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test);
 // Off-surface potential operator (single or double layer of the assembler's kernel) of

@@ -7,11 +7,16 @@
 // dynamic item counter ends with short items.  The launch is
 // captured once per plan (counter reset + kernel) and replayed with cudaGraphLaunch.
 //
-// Autotuner.  The two free parameters are the wavenumbers per work item (k-chunk: more
-// reuse of a staged tile pair versus finer load balance) and the CTAs per SM of the
-// persistent grid.  Each candidate runs the kernel on a leading slice of the work items
-// (the first 1/16th, at least 148 x 8 items) timed with CUDA events; the fastest is kept
-// per (device, mesh sizes, number of wavenumbers) for the life of the process.
+// Autotuner.  The free parameters are the tile shape of a work item (1 x 1 or 2 x 2 pairs
+// of 32-cell tiles staged together: reuse of staged tiles versus shared memory per CTA),
+// the wavenumbers per work item (k-chunk: more reuse of a staged tile pair versus finer
+// load balance) and the CTAs per SM of the persistent grid (which also sets the register
+// cap of the kernel: 4 or fewer CTAs allow 128 registers, 5 or 6 allow 80).  Each
+// candidate runs the kernel on a leading slice of the work items (the first 1/16th, at
+// least 148 x 8 items) timed with CUDA events; the fastest is kept per (device, mesh
+// sizes, number of wavenumbers) for the life of the process.  The quadrature order is not
+// a parameter: the 6-point rule is part of the problem (another order gives another
+// matrix).
 #include <algorithm>
 #include <cstring>
 #include <map>
@@ -20,12 +25,6 @@
 #include "core.h"
 
 namespace bempp_b200 {
-
-struct SweepTuning {
-  int kchunk = 8;
-  int blocks_per_sm = 4;
-  double probe_ms = 0.0;
-};
 
 namespace {
 
@@ -49,6 +48,7 @@ std::mutex g_sweep_mu;
 std::unique_ptr<SweepPlan> g_plan;  // the most recent plan (replayed while inputs repeat)
 std::map<std::tuple<int, std::vector<int64_t>, int>, SweepTuning> g_tuned;
 SweepTuning g_last;
+SweepTuning g_forced{0, 4, 1, 0.0};  // kchunk > 0: parameters fixed by the caller (no autotuning)
 
 int sm_count(int device) {
   int sms = 0;
@@ -56,14 +56,15 @@ int sm_count(int device) {
   return sms;
 }
 
-long long count_items(SweepArgs& a, int kchunk) {
+long long count_items(SweepArgs& a, int kchunk, int tile_shape) {
   a.kchunk = kchunk;
+  a.tile_shape = tile_shape;
   const int nchunks = (a.nk + kchunk - 1) / kchunk;
   long long total = 0;
   for (int m = 0; m < a.nmesh; ++m) {
     a.mesh[m].item_begin = total;
-    // tile pairs (test tile >= trial tile): the kernel mirrors the single layer
-    const long long nt = a.mesh[m].ntiles;
+    // super-tile pairs (test >= trial): the kernel mirrors the single layer
+    const long long nt = (a.mesh[m].ntiles + tile_shape - 1) / tile_shape;
     total += nt * (nt + 1) / 2 * nchunks;
   }
   a.nitems = total;
@@ -133,10 +134,13 @@ void helmholtz_sl_sweep_device(GridT* const* grids, size_t ngrids, const double*
     a.counter = plan->d_counter.as<unsigned long long>();
     const int sms = sm_count(device);
 
-    // autotune once per (device, mesh sizes, nk)
+    // autotune once per (device, mesh sizes, nk), unless the caller fixed the parameters
     const auto key = std::make_tuple(device, sizes, static_cast<int>(nk));
     auto it = g_tuned.find(key);
-    if (it == g_tuned.end()) {
+    if (g_forced.kchunk > 0) {
+      g_tuned[key] = g_forced;
+      it = g_tuned.find(key);
+    } else if (it == g_tuned.end()) {
       cudaStream_t ts;
       BEMPP_CUDA(cudaStreamCreateWithFlags(&ts, cudaStreamNonBlocking));
       cudaEvent_t e0, e1;
@@ -144,25 +148,33 @@ void helmholtz_sl_sweep_device(GridT* const* grids, size_t ngrids, const double*
       BEMPP_CUDA(cudaEventCreate(&e1));
       SweepTuning best;
       best.probe_ms = 1e30;
-      for (int kchunk : {1, 2, 4, 8, 16, 32}) {
-        if (kchunk > static_cast<int>(nk) && kchunk != 1) continue;
-        for (int bps : {2, 3, 4}) {
-          SweepArgs probe = a;
-          const long long full = count_items(probe, kchunk);
-          // a leading slice: same per-item mix as the largest mesh, ~1/16 of the work
-          probe.nitems = std::min<long long>(full, std::max<long long>(full / 16, 8LL * sms));
-          BEMPP_CUDA(cudaMemsetAsync(probe.counter, 0, sizeof(unsigned long long), ts));
-          BEMPP_CUDA(cudaEventRecord(e0, ts));
-          BEMPP_CUDA(launch_sweep_sl(probe, rule, rules, bps * sms, ts));
-          BEMPP_CUDA(cudaEventRecord(e1, ts));
-          BEMPP_CUDA(cudaEventSynchronize(e1));
-          float ms = 0.f;
-          BEMPP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-          const double per_item = ms / static_cast<double>(probe.nitems) * kchunk;
-          if (per_item < best.probe_ms) {
-            best.probe_ms = per_item;
-            best.kchunk = kchunk;
-            best.blocks_per_sm = bps;
+      for (int shape : {1, 2}) {
+        // CTAs per SM that fit the shape's shared memory (227 KB per SM)
+        const int fit = static_cast<int>((227u << 10) / (sweep_smem_bytes(shape) + 1024));
+        for (int kchunk : {1, 2, 4, 8, 16, 32}) {
+          if (kchunk > static_cast<int>(nk) && kchunk != 1) continue;
+          for (int bps : {2, 3, 4, 5, 6}) {
+            if (bps > fit) continue;
+            SweepArgs probe = a;
+            const long long full = count_items(probe, kchunk, shape);
+            // a leading slice: same per-item mix as the largest mesh, ~1/16 of the work
+            probe.nitems = std::min<long long>(full, std::max<long long>(full / 16, 8LL * sms));
+            BEMPP_CUDA(cudaMemsetAsync(probe.counter, 0, sizeof(unsigned long long), ts));
+            BEMPP_CUDA(cudaEventRecord(e0, ts));
+            BEMPP_CUDA(launch_sweep_sl(probe, rule, rules, bps, sms, ts));
+            BEMPP_CUDA(cudaEventRecord(e1, ts));
+            BEMPP_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            BEMPP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            // milliseconds per (tile pair, wavenumber)
+            const double per_unit = ms / static_cast<double>(probe.nitems) / kchunk /
+                                    (shape * shape);
+            if (per_unit < best.probe_ms) {
+              best.probe_ms = per_unit;
+              best.kchunk = kchunk;
+              best.blocks_per_sm = bps;
+              best.tile_shape = shape;
+            }
           }
         }
       }
@@ -172,14 +184,14 @@ void helmholtz_sl_sweep_device(GridT* const* grids, size_t ngrids, const double*
       it = g_tuned.emplace(key, best).first;
     }
     plan->tuning = it->second;
-    count_items(a, plan->tuning.kchunk);
+    count_items(a, plan->tuning.kchunk, plan->tuning.tile_shape);
 
     // capture: counter reset + persistent launch
     cudaStream_t cs;
     BEMPP_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     BEMPP_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     cudaError_t e1 = cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), cs);
-    cudaError_t e2 = launch_sweep_sl(a, rule, rules, plan->tuning.blocks_per_sm * sms, cs);
+    cudaError_t e2 = launch_sweep_sl(a, rule, rules, plan->tuning.blocks_per_sm, sms, cs);
     cudaError_t e3 = cudaStreamEndCapture(cs, &plan->graph);
     cudaStreamDestroy(cs);
     BEMPP_CUDA(e1);
@@ -190,6 +202,23 @@ void helmholtz_sl_sweep_device(GridT* const* grids, size_t ngrids, const double*
   }
   g_last = g_plan->tuning;
   BEMPP_CUDA(cudaGraphLaunch(g_plan->exec, stream));
+}
+
+void set_sweep_tuning(int kchunk, int blocks_per_sm, int tile_shape) {
+  std::lock_guard<std::mutex> lock(g_sweep_mu);
+  g_plan.reset();  // the next sweep builds (and captures) a new plan
+  if (kchunk <= 0) {
+    g_forced = SweepTuning{};
+    g_forced.kchunk = 0;
+    g_tuned.clear();
+    return;
+  }
+  if (blocks_per_sm < 1 || blocks_per_sm > 6 || (tile_shape != 1 && tile_shape != 2))
+    throw Error(kInvalidArgument, "blocks per SM must be 1..6 and the tile shape 1 or 2");
+  g_forced.kchunk = kchunk;
+  g_forced.blocks_per_sm = blocks_per_sm;
+  g_forced.tile_shape = tile_shape;
+  g_forced.probe_ms = 0.0;
 }
 
 SweepTuning last_sweep_tuning() {

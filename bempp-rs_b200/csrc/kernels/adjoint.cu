@@ -183,6 +183,20 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
     }
     if (active && !far) {
+      // e^{ikr} referenced to the pair (e^{ik r0} e^{ik (r - r0)}, r0 = |c_x - c_y|) when
+      // k (rad_x + rad_y) <= 0.8 bounds every phase k (r - r0): c is rotated by e^{ik r0}
+      // for the gradient terms and the sums S0, Sk are rotated back after the loop
+      const bool ref = k * (T.G(fRad, it) + S.G(fRad, js)) <= 0.8;
+      double kr0 = 0.0, pc = 1.0, ps = 0.0, cq_re = c_re, cq_im = c_im;
+      if (ref) {
+        const double dcx = T.G(fCx, it) - S.G(fCx, js), dcy = T.G(fCy, it) - S.G(fCy, js),
+                     dcz = T.G(fCz, it) - S.G(fCz, js);
+        const double r0sq = dcx * dcx + dcy * dcy + dcz * dcz;
+        kr0 = k * (r0sq * rsqrt_refined(r0sq));
+        sincos_cw(kr0, ps, pc);
+        cq_re = c_re * pc - c_im * ps;
+        cq_im = c_re * ps + c_im * pc;
+      }
 #pragma unroll 1
       for (int p = 0; p < Q; ++p) {
         const double x0 = T.P(p, 0, it), x1 = T.P(p, 1, it), x2 = T.P(p, 2, it);
@@ -195,7 +209,10 @@ __global__ void __launch_bounds__(kThreads, 3)
           const double rinv = rsqrt_refined(r2);
           const double r = r2 * rinv, kr = k * r;
           double sn, csn;
-          sincos(kr, &sn, &csn);
+          if (ref)
+            sincos_small(fma(k, r, -kr0), sn, csn);
+          else
+            sincos(kr, &sn, &csn);
           const double wq = rule.w[q];
           g_re = fma(wq * rinv, csn, g_re);
           g_im = fma(wq * rinv, sn, g_im);
@@ -203,7 +220,7 @@ __global__ void __launch_bounds__(kThreads, 3)
           e_im = fma(wq, sn, e_im);
           // Re(c e^{ikr} (ikr - 1)) / r^3
           const double f_re = -csn - kr * sn, f_im = kr * csn - sn;
-          const double gs = wq * (c_re * f_re - c_im * f_im) * rinv * rinv * rinv;
+          const double gs = wq * (cq_re * f_re - cq_im * f_im) * rinv * rinv * rinv;
           vp[0] = fma(gs, dx, vp[0]);
           vp[1] = fma(gs, dy, vp[1]);
           vp[2] = fma(gs, dz, vp[2]);
@@ -224,6 +241,14 @@ __global__ void __launch_bounds__(kThreads, 3)
           vt[a][1] = fma(f, vp[1], vt[a][1]);
           vt[a][2] = fma(f, vp[2], vt[a][2]);
         }
+      }
+      if (ref) {
+        const double s0r = S0_re * pc - S0_im * ps, s0i = S0_re * ps + S0_im * pc;
+        const double skr = Sk_re * pc - Sk_im * ps, ski = Sk_re * ps + Sk_im * pc;
+        S0_re = s0r;
+        S0_im = s0i;
+        Sk_re = skr;
+        Sk_im = ski;
       }
     }
     const double jdet_j = S.G(fJdet, js);
@@ -333,6 +358,10 @@ __global__ void __launch_bounds__(256)
   const double2 li = lam[tc], mj = mu[sc];
   const double c_re = li.x * mj.x + li.y * mj.y, c_im = li.x * mj.y - li.y * mj.x;
   const int off = rules.offset[cfg], npts = rules.offset[cfg + 1] - off;
+  // |k r| <= k (diam_x + diam_y) for a pair sharing a vertex: no phase reduction needed
+  // when that is below pi/4
+  const bool small_phase = k * (bempp_b200::g(cs.geom, kDiam, cs.stride, tc) +
+                                bempp_b200::g(cs.geom, kDiam, cs.stride, sc)) <= 0.78;
   double S0_re = 0.0, S0_im = 0.0, Sk_re = 0.0, Sk_im = 0.0;
   double gx[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, gy[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
   for (int ii = lane; ii < npts; ii += 32) {
@@ -344,10 +373,13 @@ __global__ void __launch_bounds__(256)
     for (int c = 0; c < 3; ++c)
       d[c] = (x.v0[c] + xi0 * x.t0[c] + xi1 * x.t1[c]) - (y.v0[c] + et0 * y.t0[c] + et1 * y.t1[c]);
     const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-    const double rinv = rsqrt(r2);
+    const double rinv = rsqrt_refined(r2);
     const double r = r2 * rinv, kr = k * r;
     double sn, csn;
-    sincos(kr, &sn, &csn);
+    if (small_phase)
+      sincos_taylor(kr, sn, csn);
+    else
+      sincos_cw(kr, sn, csn);
     S0_re = fma(w * rinv, csn, S0_re);
     S0_im = fma(w * rinv, sn, S0_im);
     Sk_re = fma(w, csn, Sk_re);

@@ -170,12 +170,15 @@ struct SweepArgs {
   const double* ks;       // device array of nk wavenumbers
   int nk;
   int kchunk;             // wavenumbers per work item
+  int tile_shape = 1;     // a work item covers tile_shape x tile_shape pairs of 32-cell tiles
   long long nitems;
   unsigned long long* counter;  // work counter, zeroed before each launch
 };
-size_t sweep_smem_bytes();
+size_t sweep_smem_bytes(int tile_shape);
+// Persistent launch of blocks_per_sm (at most 6) x sms CTAs.
 cudaError_t launch_sweep_sl(const SweepArgs& args, const RegularRule& rule,
-                            const SingularRules& rules, int blocks, cudaStream_t stream);
+                            const SingularRules& rules, int blocks_per_sm, int sms,
+                            cudaStream_t stream);
 
 // CUDA-core FMA throughput probe (diag.cu).
 cudaError_t measure_fma_peak(int fp64, int iters, int reps, double* tflops);

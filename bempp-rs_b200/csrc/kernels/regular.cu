@@ -957,10 +957,11 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT>())
 
 // FP64 near pairs of a mixed-precision assembly: one thread per pair of the near list
 // (test cell, trial cell), each staging its two cells into its own column of a per-warp
-// pair of shared-memory tiles and integrating them with block_fp64 (own sincos).
+// pair of shared-memory tiles and integrating them with block_fp64 (phases referenced to
+// the pair, or the in-tree reduced sincos: FPH).
 // Only pairs whose trial cell lies in [trial_lo, trial_hi) (a chunk) are done.  DP0 x DP0
 // entries are stored; other spaces add into the output with atomics.
-template <int QT, int KER, int OP, int NBT, int NBS, bool DIRECT>
+template <int QT, int KER, int OP, int NBT, int NBS, bool DIRECT, int FPH>
 __global__ void __launch_bounds__(kThreads)
     near_pairs_fp64(CellSet test, CellSet trial, RegularRule rule, double k, NearArgs near,
                     double* __restrict__ out, int64_t ld, int trial_lo, int trial_hi) {
@@ -979,7 +980,7 @@ __global__ void __launch_bounds__(kThreads)
   stage_cell(T, lane, test, pr.x, Q);  // this lane's column only: no synchronisation
   stage_cell(S, lane, trial, pr.y, Q);
   double ore[NBT][NBS], oim[NBT][NBS];
-  block_fp64<QT, KER, OP, NBT, NBS, false, kF64Reduced>(T, lane, S, lane, rule, k, ore, oim);
+  block_fp64<QT, KER, OP, NBT, NBS, false, FPH>(T, lane, S, lane, rule, k, ore, oim);
   if (DIRECT) {
     const int64_t o = static_cast<int64_t>(pr.y) * ld + pr.x;
     if (kC)
@@ -1083,13 +1084,21 @@ __device__ void duffy_sl_dp0_warp(const Tile& T, int it, const Tile& S, int js, 
   im = si * sc;
 }
 
-__global__ void __launch_bounds__(kThreads)
+// TS: tile shape of a work item, TS x TS tiles of 32 cells on each side (a super-tile
+// pair: 1 x 1 or 2 x 2 tile pairs staged together); MINB: CTAs per SM the register
+// allocation must allow (4: up to 128 registers, 6: up to 80).
+template <int TS, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
     sweep_sl_dp0(SweepArgs a, RegularRule rule, SingularRules rules) {
   const int Q = 6;
   extern __shared__ __align__(16) unsigned char smem[];
-  unsigned char* cursor = smem;
-  const Tile T = carve_tile(cursor, Q, true, 1);
-  const Tile S = carve_tile(cursor, Q, true, 1);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem);  // completion of the tile copies
+  unsigned char* cursor = smem + 16;
+  Tile Tt[TS], St[TS];
+#pragma unroll
+  for (int i = 0; i < TS; ++i) Tt[i] = carve_tile(cursor, Q, true, 1);
+#pragma unroll
+  for (int i = 0; i < TS; ++i) St[i] = carve_tile(cursor, Q, true, 1);
   unsigned short* nearq = reinterpret_cast<unsigned short*>(cursor);
   unsigned short* adjq = nearq + kTile * kTile;
   unsigned char* adjc = reinterpret_cast<unsigned char*>(adjq + kTile * kTile);
@@ -1098,12 +1107,10 @@ __global__ void __launch_bounds__(kThreads)
   float2* mir = reinterpret_cast<float2*>(s_item + 1);  // [js * (kTile + 1) + it]
   unsigned* skip = reinterpret_cast<unsigned*>(mir + kTile * (kTile + 1));  // [it]: bit js
   const int it = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) mbar_init(mbar, 1);
+  unsigned phase = 0;  // parity of the mbarrier phase of the current item's copies
   for (;;) {
-    if (threadIdx.x == 0) {
-      *s_item = static_cast<long long>(atomicAdd(a.counter, 1ull));
-      counts[0] = counts[1] = 0;
-    }
-    if (threadIdx.x < kTile) skip[threadIdx.x] = 0u;
+    if (threadIdx.x == 0) *s_item = static_cast<long long>(atomicAdd(a.counter, 1ull));
     __syncthreads();
     const long long item = *s_item;
     if (item >= a.nitems) break;
@@ -1112,91 +1119,130 @@ __global__ void __launch_bounds__(kThreads)
     const SweepMesh& M = a.mesh[m];
     const long long local = item - M.item_begin;
     // wavenumber chunk outermost: the items resident at one time write one output
-    // matrix (one chunk of them), in the banded tile-pair order
-    const long long npairs = lower_tile_pair_count(M.ntiles, 0, M.ntiles);
+    // matrix (one chunk of them), in the banded order of the super-tile pairs
+    const int nsup = (M.ntiles + TS - 1) / TS;
+    const long long npairs = lower_tile_pair_count(nsup, 0, nsup);
     const int kc = static_cast<int>(local / npairs);
-    int tt, st;
-    lower_tile_pair(local % npairs, M.ntiles, 0, M.ntiles, tt, st);
-    const bool mirror = tt > st;
+    int TT, ST;
+    lower_tile_pair(local % npairs, nsup, 0, nsup, TT, ST);
     const int nc = M.cells.ncells;
-    const int ti0 = tt * kTile, sj0 = st * kTile;
-    const int nti = min(kTile, nc - ti0), nsj = min(kTile, nc - sj0);
-    load_tile(T, M.cells, ti0, nti, Q, true, nullptr, 1);
-    load_tile(S, M.cells, sj0, nsj, Q, true, nullptr, 1);
-    __syncthreads();
-    // classify the tile pair once: vertex-sharing and near pairs are queued, and marked in
-    // the test cell's skip word for the far-pair loop of every wavenumber
-    if (it < nti) {
-      const int av[3] = {T.vid[it], T.vid[kTile + it], T.vid[2 * kTile + it]};
-      unsigned bits = 0u;
-      for (int js = warp; js < nsj; js += kWarps) {
-        const int bv[3] = {S.vid[js], S.vid[kTile + js], S.vid[2 * kTile + js]};
-        if (share_vertex(av[0], av[1], av[2], bv[0], bv[1], bv[2])) {
-          const int slot = atomicAdd(counts + 1, 1);
-          adjq[slot] = static_cast<unsigned short>(it | (js << 8));
-          adjc[slot] = static_cast<unsigned char>(adjacency_config(av, bv, ti0 + it == sj0 + js));
-          bits |= 1u << js;
-        } else if (near_pair(T, it, S, js)) {
-          const int slot = atomicAdd(counts, 1);
-          nearq[slot] = static_cast<unsigned short>(it | (js << 8));
-          bits |= 1u << js;
-        }
+    // every tile of the two super-tiles by bulk (TMA) copies on the mbarrier: rows of 32
+    // cells of the padded grid arrays; the previous item's reads of the tiles ended at
+    // the barriers that closed it
+    if (threadIdx.x == 0) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      unsigned bytes = 0;
+      for (int i = 0; i < TS; ++i) {
+        if (TS * TT + i < M.ntiles) bytes += bulk_tile_bytes(Q, true, true);
+        if (TS * ST + i < M.ntiles) bytes += bulk_tile_bytes(Q, true, true);
       }
-      if (bits) atomicOr(skip + it, bits);
+      mbar_expect_tx(mbar, bytes);
+      for (int i = 0; i < TS; ++i) {
+        if (TS * TT + i < M.ntiles) stage_tile_bulk(Tt[i], M.cells, (TS * TT + i) * kTile, Q, true, mbar, true);
+        if (TS * ST + i < M.ntiles) stage_tile_bulk(St[i], M.cells, (TS * ST + i) * kTile, Q, true, mbar, true);
+      }
     }
-    __syncthreads();
-    const int nnear = counts[0], nadj = counts[1];
-    const unsigned skip_it = it < nti ? skip[it] : ~0u;
-    const int k0 = kc * a.kchunk, k1 = min(a.nk, k0 + a.kchunk);
-    for (int kk = k0; kk < k1; ++kk) {
-      const double k = a.ks[kk];
-      float2* out = M.out + static_cast<long long>(kk) * nc * nc;
+    const bool staged = mbar_wait_bounded(mbar, phase);
+    phase ^= 1u;
+    if (__syncthreads_or(!staged)) {
+      // the copies did not complete in time (never expected): record it, give them a last
+      // bounded wait and stop this CTA (the item's entries stay unwritten; the host's
+      // completion check reports it)
+      if (threadIdx.x == 0) atomicAdd(&g_stage_timeouts, 1u);
+      mbar_wait_bounded(mbar, phase ^ 1u);
+      return;
+    }
+#pragma unroll 1
+    for (int sub = 0; sub < TS * TS; ++sub) {
+      const int tt = TS * TT + sub / TS, st = TS * ST + sub % TS;
+      if (tt >= M.ntiles || st >= M.ntiles || tt < st) continue;  // block-uniform
+      const Tile& T = Tt[sub / TS];
+      const Tile& S = St[sub % TS];
+      const bool mirror = tt > st;
+      const int ti0 = tt * kTile, sj0 = st * kTile;
+      const int nti = min(kTile, nc - ti0), nsj = min(kTile, nc - sj0);
+      if (threadIdx.x == 0) counts[0] = counts[1] = 0;
+      if (threadIdx.x < kTile) skip[threadIdx.x] = 0u;
+      __syncthreads();
+      // classify the tile pair once: vertex-sharing and near pairs are queued, and marked
+      // in the test cell's skip word for the far-pair loop of every wavenumber
       if (it < nti) {
+        const int av[3] = {T.vid[it], T.vid[kTile + it], T.vid[2 * kTile + it]};
+        unsigned bits = 0u;
         for (int js = warp; js < nsj; js += kWarps) {
-          if ((skip_it >> js) & 1u) continue;
+          const int bv[3] = {S.vid[js], S.vid[kTile + js], S.vid[2 * kTile + js]};
+          if (share_vertex(av[0], av[1], av[2], bv[0], bv[1], bv[2])) {
+            const int slot = atomicAdd(counts + 1, 1);
+            adjq[slot] = static_cast<unsigned short>(it | (js << 8));
+            adjc[slot] = static_cast<unsigned char>(adjacency_config(av, bv, ti0 + it == sj0 + js));
+            bits |= 1u << js;
+          } else if (near_pair(T, it, S, js)) {
+            const int slot = atomicAdd(counts, 1);
+            nearq[slot] = static_cast<unsigned short>(it | (js << 8));
+            bits |= 1u << js;
+          }
+        }
+        if (bits) atomicOr(skip + it, bits);
+      }
+      __syncthreads();
+      const int nnear = counts[0], nadj = counts[1];
+      const unsigned skip_it = it < nti ? skip[it] : ~0u;
+      const int k0 = kc * a.kchunk, k1 = min(a.nk, k0 + a.kchunk);
+      for (int kk = k0; kk < k1; ++kk) {
+        const double k = a.ks[kk];
+        float2* out = M.out + static_cast<long long>(kk) * nc * nc;
+        if (it < nti) {
+          for (int js = warp; js < nsj; js += kWarps) {
+            if ((skip_it >> js) & 1u) continue;
+            double ore[1][1], oim[1][1];
+            block_fp32<6, kHelmholtz, kSL, 1, 1, kPhaseRuntime>(T, it, S, js, rule, k, ore, oim);
+            const float2 v = make_float2(static_cast<float>(ore[0][0]), static_cast<float>(oim[0][0]));
+            out[static_cast<long long>(sj0 + js) * nc + ti0 + it] = v;
+            if (mirror) mir[js * (kTile + 1) + it] = v;
+          }
+        }
+        for (int e = threadIdx.x; e < nnear; e += kThreads) {
+          const int pi = nearq[e] & 0xff, pj = nearq[e] >> 8;
           double ore[1][1], oim[1][1];
-          block_fp32<6, kHelmholtz, kSL, 1, 1, kPhaseRuntime>(T, it, S, js, rule, k, ore, oim);
+          // FP64 near pair: phase referenced to the pair when k (rad_x + rad_y) bounds it,
+          // else the in-tree reduced sincos
+          if (k * (T.G(fRad, pi) + S.G(fRad, pj)) <= static_cast<double>(kSmallPhaseMax))
+            block_fp64<6, kHelmholtz, kSL, 1, 1, false, kF64Referenced>(T, pi, S, pj, rule, k, ore, oim);
+          else
+            block_fp64<6, kHelmholtz, kSL, 1, 1, false, kF64Reduced>(T, pi, S, pj, rule, k, ore, oim);
           const float2 v = make_float2(static_cast<float>(ore[0][0]), static_cast<float>(oim[0][0]));
-          out[static_cast<long long>(sj0 + js) * nc + ti0 + it] = v;
-          if (mirror) mir[js * (kTile + 1) + it] = v;
+          out[static_cast<long long>(sj0 + pj) * nc + ti0 + pi] = v;
+          if (mirror) mir[pj * (kTile + 1) + pi] = v;
         }
-      }
-      for (int e = threadIdx.x; e < nnear; e += kThreads) {
-        const int pi = nearq[e] & 0xff, pj = nearq[e] >> 8;
-        double ore[1][1], oim[1][1];
-        block_fp64<6, kHelmholtz, kSL, 1, 1, false>(T, pi, S, pj, rule, k, ore, oim);
-        const float2 v = make_float2(static_cast<float>(ore[0][0]), static_cast<float>(oim[0][0]));
-        out[static_cast<long long>(sj0 + pj) * nc + ti0 + pi] = v;
-        if (mirror) mir[pj * (kTile + 1) + pi] = v;
-      }
-      for (int e = warp; e < nadj; e += kWarps) {
-        const int pi = adjq[e] & 0xff, pj = adjq[e] >> 8;
-        double re, im;
-        duffy_sl_dp0_warp(T, pi, S, pj, adjc[e], rules, k, re, im);
-        if (it == 0)
-          out[static_cast<long long>(sj0 + pj) * nc + ti0 + pi] =
-              make_float2(static_cast<float>(re), static_cast<float>(im));
-        if (mirror) {
-          // the transposed pair: trial cell pj as the test cell, its own configuration
-          const int av[3] = {S.vid[pj], S.vid[kTile + pj], S.vid[2 * kTile + pj]};
-          const int bv[3] = {T.vid[pi], T.vid[kTile + pi], T.vid[2 * kTile + pi]};
-          duffy_sl_dp0_warp(S, pj, T, pi, adjacency_config(av, bv, false), rules, k, re, im);
+        for (int e = warp; e < nadj; e += kWarps) {
+          const int pi = adjq[e] & 0xff, pj = adjq[e] >> 8;
+          double re, im;
+          duffy_sl_dp0_warp(T, pi, S, pj, adjc[e], rules, k, re, im);
           if (it == 0)
-            mir[pj * (kTile + 1) + pi] = make_float2(static_cast<float>(re), static_cast<float>(im));
+            out[static_cast<long long>(sj0 + pj) * nc + ti0 + pi] =
+                make_float2(static_cast<float>(re), static_cast<float>(im));
+          if (mirror) {
+            // the transposed pair: trial cell pj as the test cell, its own configuration
+            const int av[3] = {S.vid[pj], S.vid[kTile + pj], S.vid[2 * kTile + pj]};
+            const int bv[3] = {T.vid[pi], T.vid[kTile + pi], T.vid[2 * kTile + pi]};
+            duffy_sl_dp0_warp(S, pj, T, pi, adjacency_config(av, bv, false), rules, k, re, im);
+            if (it == 0)
+              mir[pj * (kTile + 1) + pi] = make_float2(static_cast<float>(re), static_cast<float>(im));
+          }
+        }
+        if (mirror) {
+          // the transposed block, entry (row sj0 + j, column ti0 + i), j fastest: coalesced
+          __syncthreads();
+          for (int idx = threadIdx.x; idx < kTile * kTile; idx += kThreads) {
+            const int i = idx / kTile, j = idx % kTile;
+            if (i < nti && j < nsj)
+              out[static_cast<long long>(ti0 + i) * nc + sj0 + j] = mir[j * (kTile + 1) + i];
+          }
+          __syncthreads();  // mir is reused by the next wavenumber
         }
       }
-      if (mirror) {
-        // the transposed block, entry (row sj0 + j, column ti0 + i), j fastest: coalesced
-        __syncthreads();
-        for (int idx = threadIdx.x; idx < kTile * kTile; idx += kThreads) {
-          const int i = idx / kTile, j = idx % kTile;
-          if (i < nti && j < nsj)
-            out[static_cast<long long>(ti0 + i) * nc + sj0 + j] = mir[j * (kTile + 1) + i];
-        }
-        __syncthreads();  // mir is reused by the next wavenumber
-      }
+      __syncthreads();  // the queues and skip words are reused by the next tile pair
     }
-    __syncthreads();  // the tiles and queues are reused by the next item
   }
 }
 
@@ -1252,7 +1298,9 @@ cudaError_t launch_near_pairs(const CellSet& test, const CellSet& trial, const R
   const size_t per_warp = 2 * (sizeof(double) * tile_doubles(rule.npts) + sizeof(int) * tile_ints(1) + 16);
   const int warps = static_cast<int>(std::max<size_t>(1, std::min<size_t>(kWarps, (200u << 10) / per_warp)));
   const size_t smem = warps * per_warp + 16;
-  auto fn = near_pairs_fp64<QT, KER, OP, NBT, NBS, DIRECT>;
+  // phases referenced to the pair when the launch's bound k (rad_x + rad_y) <= 0.8 holds
+  auto fn = a.small_phase ? near_pairs_fp64<QT, KER, OP, NBT, NBS, DIRECT, kF64Referenced>
+                          : near_pairs_fp64<QT, KER, OP, NBT, NBS, DIRECT, kF64Reduced>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
@@ -1299,8 +1347,10 @@ cudaError_t launch_one(const CellSet& test, const SpaceTiles& tt, const CellSet&
     }
     if (a.near.trial_tiles != trial_tiles) return cudaErrorInvalidValue;
     cudaError_t e;
+    // the launch-wide bound failed: each warp still takes the unreduced polynomial phase
+    // when its own pairs allow it (most pairs of a mesh whose largest cells set the bound)
     if (KER == kHelmholtz && !a.small_phase)
-      e = launch_mode<QT, KER, OP, NBT, NBS, true, DIRECT, kPhaseGeneral, kNearMasked>(
+      e = launch_mode<QT, KER, OP, NBT, NBS, true, DIRECT, kPhaseRuntime, kNearMasked>(
           test, tt, trial, st, rule, a, ty0, ty1, stream);
     else
       e = launch_mode<QT, KER, OP, NBT, NBS, true, DIRECT, kPhaseSmall, kNearMasked>(
@@ -1378,26 +1428,43 @@ cudaError_t take_stage_timeouts(unsigned* count) {
   return cudaMemcpyToSymbol(g_stage_timeouts, &zero, sizeof(unsigned));
 }
 
-size_t sweep_smem_bytes() {
+size_t sweep_smem_bytes(int ts) {
   size_t b = 0;
-  for (int t = 0; t < 2; ++t) {
+  for (int t = 0; t < 2 * ts; ++t) {
     b += sizeof(double) * tile_doubles(6) + sizeof(float) * tile_floats(6, true) +
          sizeof(int) * tile_ints(1);
     b = (b + 15) & ~size_t(15);
   }
-  return b + 2 * sizeof(unsigned short) * kTile * kTile + kTile * kTile + 2 * sizeof(int) +
+  return 16 + b + 2 * sizeof(unsigned short) * kTile * kTile + kTile * kTile + 2 * sizeof(int) +
          sizeof(long long) + sizeof(float2) * kTile * (kTile + 1) + sizeof(unsigned) * kTile + 32;
 }
 
-cudaError_t launch_sweep_sl(const SweepArgs& args, const RegularRule& rule,
-                            const SingularRules& rules, int blocks, cudaStream_t stream) {
-  if (rule.npts != 6) return cudaErrorInvalidValue;
-  const size_t smem = sweep_smem_bytes();
-  cudaError_t e = cudaFuncSetAttribute(sweep_sl_dp0, cudaFuncAttributeMaxDynamicSharedMemorySize,
+namespace {
+template <int TS, int MINB>
+cudaError_t launch_sweep_shape(const SweepArgs& args, const RegularRule& rule,
+                               const SingularRules& rules, int blocks, cudaStream_t stream) {
+  const size_t smem = sweep_smem_bytes(TS);
+  auto fn = sweep_sl_dp0<TS, MINB>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  sweep_sl_dp0<<<blocks, kThreads, smem, stream>>>(args, rule, rules);
+  fn<<<blocks, kThreads, smem, stream>>>(args, rule, rules);
   return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_sweep_sl(const SweepArgs& args, const RegularRule& rule,
+                            const SingularRules& rules, int blocks_per_sm, int sms,
+                            cudaStream_t stream) {
+  if (rule.npts != 6) return cudaErrorInvalidValue;
+  if (args.tile_shape != 1 && args.tile_shape != 2) return cudaErrorInvalidValue;
+  const int blocks = blocks_per_sm * sms;
+  // the register cap follows the CTAs per SM asked for (at most 6)
+  if (args.tile_shape == 1)
+    return blocks_per_sm > 4 ? launch_sweep_shape<1, 6>(args, rule, rules, blocks, stream)
+                             : launch_sweep_shape<1, 4>(args, rule, rules, blocks, stream);
+  return blocks_per_sm > 4 ? launch_sweep_shape<2, 6>(args, rule, rules, blocks, stream)
+                           : launch_sweep_shape<2, 4>(args, rule, rules, blocks, stream);
 }
 
 cudaError_t launch_regular_dp0(const CellSet& test, const CellSet& trial,

@@ -317,7 +317,7 @@ def helmholtz_sl_fp64_vs_mixed(args):
         wl = Workload(w, prec)
         if sample is None and not args.skip_cpu:  # CPU baseline leg: oracle rows (checker)
             sample = oracle_row_sample("helmholtz", w["ops"], w["k"], w["space"], wl.points,
-                                       wl.cells, args.cpu_sample_cells, 1)
+                                       wl.cells, args.cpu_sample_cells, 160, 1)
             res["cpu_baseline"] = cpu_baseline(w, wl.points, wl.cells, wl.n, args, sample)
         ms, _ = wl.timed(max(3, args.steps), 2)
         ph = wl.phase_ms()["single_layer"]
@@ -370,7 +370,7 @@ def helmholtz_p1_ops(args):
     if not args.skip_cpu:  # CPU baseline leg: oracle rows of each operator (checker)
         wl0 = wls["fp64"]
         sample = oracle_row_sample("helmholtz", w["ops"], w["k"], w["space"], wl0.points,
-                                   wl0.cells, 27, 2)
+                                   wl0.cells, 256, 27, 2)
         out["cpu_baseline"] = cpu_baseline(w, wl0.points, wl0.cells, wl0.n, args, sample)
     for prec, wl in wls.items():
         wl.timed(1, 2)
@@ -510,7 +510,7 @@ def sweep_timing(args):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
     entries = sum(len(ks) * len(g.cells) ** 2 for g in grids)
-    kc, bps, probe = last_tuning()
+    kc, bps, probe, shape = last_tuning()
     check = None
     if not args.skip_cpu:
         # CPU baseline leg as the checker: oracle rows (16 seeded rows per mesh) at the
@@ -521,7 +521,7 @@ def sweep_timing(args):
             cells = g.cells.astype(np.int64)
             for j in (0, len(ks) // 2, len(ks) - 1):
                 smp = oracle_row_sample("helmholtz", ["single_layer"], float(ks[j]), "dp0", pts,
-                                        cells, 16, j)
+                                        cells, 128, 16, j)
                 errs[f"{len(cells)}_k{ks[j]:.3f}"] = rows_error(out[j], smp, "single_layer")
         check = {"rel_frobenius_error_vs_oracle_rows": errs, "max": max(errs.values()),
                  "rows_per_matrix": 16}
@@ -530,7 +530,8 @@ def sweep_timing(args):
     return {"workload": "helmholtz_sl_dp0_sweep_32k_ico3_4_5_c64", "entries": entries,
             "ms_per_sweep": ms, "entries_per_s": entries / (ms * 1e-3),
             "first_call_s": first_s, "tuning": {"k_per_item": kc, "ctas_per_sm": bps,
-                                                "probe_ms_per_item": probe},
+                                                "tile_shape": f"{shape}x{shape} tiles of 32 cells",
+                                                "probe_ms_per_tile_pair_and_k": probe},
             "launches_per_sweep": 1, "parity": check}
 
 
@@ -580,9 +581,8 @@ def run_ours(args):
     # GPU's rows of the same DOFs
     sample = parity = None
     if rank == 0 and not args.skip_cpu:
-        nrows = args.cpu_sample_cells // 6 if w["space"] == "p1" else args.cpu_sample_cells
         sample = oracle_row_sample(w["kernel"], w["ops"], w["k"], w["space"], wl.points,
-                                   wl.cells, nrows, 0)
+                                   wl.cells, args.cpu_sample_cells, 160, 0)
         parity = {"rel_frobenius_error_vs_oracle_rows": {
                       op: rows_error(out, sample, op) for op, out in zip(w["ops"], wl.outs)},
                   "rows": len(sample["rows"]),
@@ -730,20 +730,32 @@ def _space_degree(space):
     return (1, True) if space == "p1" else (0, False)
 
 
-def oracle_row_sample(kernel, ops, k, space, points, cells, nrows, seed):
-    """Complete rows of ``nrows`` seeded test DOFs of each operator, from the oracle on all
-    host threads: {"rows", "oracle_rows": {op: rows x n}, "seconds": {op: s},
-    "regular_seconds", "singular_seconds", "test_cells", "threads"}.  The regular part is
-    assembled for the cells holding those DOFs (which completes their rows), the singular
-    part for the whole grid; their sum gives the rows, and the regular time scales with
-    the number of test cells while the singular time is that of the whole step."""
+def oracle_row_sample(kernel, ops, k, space, points, cells, window, nrows, seed):
+    """Complete rows of at most ``nrows`` seeded test DOFs of each operator, from the
+    oracle on all host threads: {"rows", "oracle_rows": {op: rows x n}, "seconds": {op: s},
+    "regular_seconds", "singular_seconds", "test_cells", "threads"}.  The test cells are a
+    seeded run of ``window`` consecutive cells starting at a multiple of the oracle's
+    128-cell block (so its blocks are full); the rows are DOFs all of whose cells lie in
+    that run (so its regular part completes them), and the singular part of the whole grid
+    is added.  The regular time scales with the number of test cells; the singular time is
+    that of the whole step."""
     from oracle import oracle
 
     deg, cont = _space_degree(space)
     threads = os.cpu_count() or 1
     dofs, n = oracle.cell_dofs(points, cells, deg, cont)
-    rows = np.sort(np.random.default_rng(seed).choice(n, size=min(nrows, n), replace=False))
-    sub = np.flatnonzero(np.isin(dofs, rows).any(axis=1))
+    ncells = len(cells)
+    rng = np.random.default_rng(seed)
+    window = min(window, ncells)
+    c0 = int(rng.integers(0, max(1, (ncells - window) // 128 + 1))) * 128
+    sub = np.arange(c0, min(ncells, c0 + window))
+    inside = np.zeros(ncells, dtype=bool)
+    inside[sub] = True
+    # DOFs touched only by cells of the run
+    touched_outside = np.zeros(n, dtype=bool)
+    touched_outside[np.unique(dofs[~inside])] = True
+    eligible = np.setdiff1d(np.unique(dofs[sub]), np.flatnonzero(touched_outside))
+    rows = np.sort(rng.choice(eligible, size=min(nrows, len(eligible)), replace=False))
     out = {"rows": rows, "oracle_rows": {}, "seconds": {}, "regular_seconds": {},
            "singular_seconds": {}, "test_cells": int(len(sub)), "threads": threads, "n": n}
     kw = dict(k=k, test_degree=deg, test_continuous=cont, trial_degree=deg,
@@ -785,14 +797,12 @@ def cpu_baseline(w, points, cells, n, args, sample=None):
     """CPU baseline of the headline workload on a bounded sample (about 10-30 s of CPU
     work): complete rows of a seeded DOF subset of every operator, scaled."""
     if sample is None:
-        nrows = args.cpu_sample_cells // 6 if w["space"] == "p1" else args.cpu_sample_cells
         sample = oracle_row_sample(w["kernel"], w["ops"], w["k"], w["space"], points, cells,
-                                   nrows, 0)
+                                   args.cpu_sample_cells, 160, 0)
     return {"value": cpu_rate(sample, len(cells), len(w["ops"]), n), "unit": "entries/s",
             "cores": sample["threads"], "kind": "port",
-            "sample": f"complete rows of {len(sample['rows'])} seeded test DOFs of each of "
-                      f"{len(w['ops'])} operator(s): the regular part for the "
-                      f"{sample['test_cells']} of {len(cells)} test cells holding them (x all "
+            "sample": f"regular part of {len(w['ops'])} operator(s) for a seeded run of "
+                      f"{sample['test_cells']} of {len(cells)} consecutive test cells (x all "
                       f"trial cells), time scaled by {len(cells) / sample['test_cells']:.1f}, "
                       "plus the whole singular part; CPU FP64 restatement of the bempp-rs "
                       "algorithm (OpenMP over 128x128 blocks, -O3 -march=native)",
@@ -814,10 +824,8 @@ def run_reference(args):
     deg, cont = _space_degree(w["space"])
     threads = os.cpu_count() or 1
     n = oracle.space_size(points, cells, deg, cont)
-    nrows = args.cpu_sample_cells // 6 if w["space"] == "p1" else args.cpu_sample_cells
     for i in range(args.warmup):  # untimed: small samples (library load, page-in, caches)
-        oracle_row_sample(w["kernel"], w["ops"], w["k"], w["space"], points, cells,
-                          max(1, nrows // 16), i)
+        oracle_row_sample(w["kernel"], w["ops"], w["k"], w["space"], points, cells, 128, 8, i)
     t = time.perf_counter()
     for op in w["ops"]:
         oracle.assemble(points, cells, w["kernel"], op, k=w["k"], test_degree=deg,
@@ -828,13 +836,14 @@ def run_reference(args):
     value = eps / full_s
     est = []
     for i in range(min(args.steps, 2)):
-        smp = oracle_row_sample(w["kernel"], w["ops"], w["k"], w["space"], points, cells, nrows,
-                                100 + i)
+        smp = oracle_row_sample(w["kernel"], w["ops"], w["k"], w["space"], points, cells,
+                                args.cpu_sample_cells, 8, 100 + i)
         est.append(cpu_rate(smp, len(cells), len(w["ops"]), n))
     est_med = statistics.median(est) if est else None
     sample_desc = (f"one complete step timed: all {len(w['ops'])} operator(s), {n} x {n} each, "
                    f"{full_s:.1f} s on {threads} threads; cross-check: {len(est)} sampled steps "
-                   f"(complete rows of {nrows} seeded test DOFs per operator, scaled) estimate "
+                   f"(regular part of {args.cpu_sample_cells} consecutive test cells scaled, plus the "
+                   f"singular part) estimate "
                    f"{est_med:.4g} entries/s, {est_med / value:.3f} x the measured full step"
                    if est_med else f"one complete step timed ({full_s:.1f} s)")
     line = {
@@ -869,7 +878,7 @@ def main():
     ap.add_argument("--k", type=float, default=None, help="wavenumber override (Helmholtz)")
     ap.add_argument("--once", action="store_true")
     ap.add_argument("--cpu-sample-cells", type=int, default=640,
-                    help="test DOFs (DP0) or 6 x test DOFs (P1) of the CPU row samples")
+                    help="consecutive test cells of the CPU baseline samples")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-comparisons", action="store_true",

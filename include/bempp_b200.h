@@ -341,9 +341,16 @@ BemppStatus bempp_helmholtz_single_layer_dp0_sweep_device(GridT *const *grids, s
                                                           const double *wavenumbers, size_t nk,
                                                           const BoundaryAssemblerOptionsT *options,
                                                           void *const *outputs, void *stream);
-/* Addition: parameters the autotuner chose for the last sweep (probe_ms: its measured
- * milliseconds per wavenumber-item on the probe slice). */
-BemppStatus bempp_sweep_last_tuning(int32_t *kchunk, int32_t *blocks_per_sm, double *probe_ms);
+/* Addition: fixes the sweep's launch parameters for the following sweeps instead of
+ * autotuning (kchunk wavenumbers per work item, blocks_per_sm 1..6 CTAs per SM,
+ * tile_shape 1 or 2); kchunk <= 0 returns to autotuning and forgets earlier results. */
+BemppStatus bempp_sweep_set_tuning(int32_t kchunk, int32_t blocks_per_sm, int32_t tile_shape);
+/* Addition: parameters the autotuner chose for the last sweep: wavenumbers per work item,
+ * CTAs per SM, tile shape (a work item covers tile_shape x tile_shape pairs of 32-cell
+ * tiles) and probe_ms, its measured milliseconds per (tile pair, wavenumber) on the probe
+ * slice.  Any pointer may be NULL. */
+BemppStatus bempp_sweep_last_tuning(int32_t *kchunk, int32_t *blocks_per_sm, int32_t *tile_shape,
+                                    double *probe_ms);
 
 /* Addition, with no counterpart in the reference: dense regular-quadrature assembly of a
  * DP0 x DP0 Laplace (kernel 0) or Helmholtz (kernel 1) single-layer, double-layer or

@@ -56,5 +56,31 @@ def test_sweep_matches_single_assemblies():
             assert err <= 1e-6, (len(g.cells), k, err)
             # entrywise as well: the mirrored blocks' vertex-sharing entries (own Duffy rule)
             assert d.abs().max().item() <= 1e-6 * ref.abs().max().item(), (len(g.cells), k)
-    kc, bps, ms = last_tuning()
-    assert kc >= 1 and bps >= 1 and ms > 0
+    kc, bps, ms, shape = last_tuning()
+    assert kc >= 1 and bps >= 1 and ms > 0 and shape in (1, 2)
+
+
+@pytest.mark.parametrize("kchunk,bps,shape", [(2, 6, 1), (4, 3, 2), (1, 2, 2)])
+def test_every_tuner_candidate_shape_is_correct(kchunk, bps, shape):
+    """The launch variants the autotuner chooses among (tile shape 1 x 1 or 2 x 2 tile
+    pairs per work item, the 80- and 128-register builds): each fixed by hand must give
+    the same matrices as the single assemblies."""
+    import torch
+
+    from bempp.sweep import helmholtz_single_layer_sweep, last_tuning, set_tuning
+
+    grids = [stretched(2, 1280), stretched(3, 5120)]
+    ks = np.array([2.0, 11.0, 19.5])
+    set_tuning(kchunk, bps, shape)
+    try:
+        outs = helmholtz_single_layer_sweep(grids, ks)
+        torch.cuda.synchronize()
+        assert last_tuning()[0] == kchunk and last_tuning()[3] == shape
+    finally:
+        set_tuning(0)
+    for g, o in zip(grids, outs):
+        for j, k in enumerate(ks):
+            ref = single(g, k)
+            d = o[j].to(torch.complex128) - ref
+            assert (torch.linalg.norm(d) / torch.linalg.norm(ref)).item() <= 1e-6
+            assert d.abs().max().item() <= 1e-6 * ref.abs().max().item()
