@@ -689,8 +689,8 @@ GridT* bempp_grid_from_points_cells(const void* points, size_t npoints, DType dt
 void grid_t_free_bempp(GridT* ptr) { delete ptr; }
 
 ElementFamilyT* create_lagrange_family_bempp(size_t degree, Continuity continuity, DType dtype) {
-  if (degree > 1) {
-    set_last_error("only Lagrange degree 0 and 1 are supported");
+  if (degree > 2) {
+    set_last_error("only Lagrange degree 0, 1 and 2 are supported");
     return nullptr;
   }
   if (continuity > Continuity_Discontinuous || dtype > DType_C64) {

@@ -186,6 +186,7 @@ SpaceTiles space_tiles(const SpaceT& s) {
   t.cell_ldof = s.d_cell_ldof.as<uint8_t>();
   t.inc_off = s.d_tile_inc_off.as<uint8_t>();
   t.inc_ent = s.d_tile_inc_ent.as<uint8_t>();
+  t.cell_dofs = s.d_dofs.as<int>();
   return t;
 }
 
@@ -477,7 +478,7 @@ void assemble_potential_device(BoundaryAssemblerT& a, SpaceT& space, const doubl
     a.convert.alloc(sizeof(double) * reals);
     out = a.convert.ptr;
   }
-  if (space.nbasis == 3) {  // P1 DOF columns are sums over the cells of the DOF
+  if (space.nbasis > 1) {  // P1 / P2 DOF columns are sums over the cells of the DOF
     BEMPP_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * reals, stream));
     ++a.launches;
   }

@@ -65,8 +65,8 @@ void GridT::build_topology() {
 namespace bempp_b200 {
 
 SpaceT* make_space(GridT* grid, const ElementFamilyT& fam) {
-  if (fam.degree > 1)
-    throw Error(kUnsupported, "only Lagrange degree 0 and 1 spaces are supported");
+  if (fam.degree > 2)
+    throw Error(kUnsupported, "only Lagrange degree 0, 1 and 2 spaces are supported");
   std::lock_guard<std::mutex> lock(grid->mu);
   grid->build_topology();
   auto* s = new SpaceT();
@@ -87,7 +87,7 @@ SpaceT* make_space(GridT* grid, const ElementFamilyT& fam) {
       s->entity_dofs[2][c] = {c};
     }
     s->ndofs = nc;
-  } else if (s->continuous) {
+  } else if (fam.degree == 1 && s->continuous) {
     s->nbasis = 3;
     s->cell_dofs.resize(3 * nc);
     int64_t size = 0;
@@ -98,15 +98,37 @@ SpaceT* make_space(GridT* grid, const ElementFamilyT& fam) {
         s->cell_dofs[3 * c + i] = ed[0];
       }
     s->ndofs = size;
-  } else {
-    // DP1: all three DOFs belong to the cell interior
-    s->nbasis = 3;
-    s->cell_dofs.resize(3 * nc);
+  } else if (fam.degree == 2 && s->continuous) {
+    // P2: per cell its vertices, then its edges (local edge i opposite vertex i), the
+    // first visit of an entity allocating its DOF (src/function.rs:409-440)
+    s->nbasis = 6;
+    s->cell_dofs.resize(6 * nc);
+    int64_t size = 0;
     for (int64_t c = 0; c < nc; ++c) {
-      for (int i = 0; i < 3; ++i) s->cell_dofs[3 * c + i] = 3 * c + i;
-      s->entity_dofs[2][c] = {3 * c, 3 * c + 1, 3 * c + 2};
+      for (int i = 0; i < 3; ++i) {
+        auto& ed = s->entity_dofs[0][grid->vtx()[3 * c + i]];
+        if (ed.empty()) ed.push_back(size++);
+        s->cell_dofs[6 * c + i] = ed[0];
+      }
+      for (int i = 0; i < 3; ++i) {
+        auto& ed = s->entity_dofs[1][grid->cell_edges[c][i]];
+        if (ed.empty()) ed.push_back(size++);
+        s->cell_dofs[6 * c + 3 + i] = ed[0];
+      }
     }
-    s->ndofs = 3 * nc;
+    s->ndofs = size;
+  } else {
+    // DP1 / DP2: every DOF belongs to the cell interior
+    const int nb = fam.degree == 1 ? 3 : 6;
+    s->nbasis = nb;
+    s->cell_dofs.resize(nb * nc);
+    for (int64_t c = 0; c < nc; ++c) {
+      for (int i = 0; i < nb; ++i) {
+        s->cell_dofs[nb * c + i] = nb * c + i;
+        s->entity_dofs[2][c].push_back(nb * c + i);
+      }
+    }
+    s->ndofs = nb * nc;
   }
   return s;
 }
@@ -246,8 +268,11 @@ void build_tiles(const SpaceT& s, int tile, std::vector<int>& off, std::vector<i
   dofs.clear();
   ldof.assign(nc * nb, 0);
   max_dofs = 0;
-  inc_off.assign(static_cast<size_t>(ntiles) * (3 * tile + 1), 0);
-  inc_ent.assign(static_cast<size_t>(ntiles) * 3 * tile, 0);
+  // the DOF incidence serves the P1 / DP1 gather of the tiled kernels only (degree-2
+  // spaces use the generic pair kernel)
+  const bool incidence = nb <= 3;
+  inc_off.assign(incidence ? static_cast<size_t>(ntiles) * (3 * tile + 1) : 0, 0);
+  inc_ent.assign(incidence ? static_cast<size_t>(ntiles) * 3 * tile : 0, 0);
   std::vector<int> local, count;
   for (int t = 0; t < ntiles; ++t) {
     const int64_t c0 = static_cast<int64_t>(t) * tile, c1 = std::min<int64_t>(c0 + tile, nc);
@@ -265,6 +290,7 @@ void build_tiles(const SpaceT& s, int tile, std::vector<int>& off, std::vector<i
     dofs.insert(dofs.end(), local.begin(), local.end());
     off[t + 1] = static_cast<int>(dofs.size());
     max_dofs = std::max<int>(max_dofs, static_cast<int>(local.size()));
+    if (!incidence) continue;
     // incidence (counting sort of the tile's (cell, basis) entries by local DOF)
     const int nd = static_cast<int>(local.size());
     uint8_t* io = &inc_off[static_cast<size_t>(t) * (3 * tile + 1)];

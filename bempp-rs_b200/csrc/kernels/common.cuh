@@ -176,6 +176,44 @@ __device__ __forceinline__ double rinv3_refined(double a) {
   return fma(y3 * e, fma(e, 1.875, 1.5), y3);
 }
 
+// Lagrange basis of NB functions (1: degree 0, 3: degree 1, 6: degree 2 in ndelement's
+// order: vertices 0, 1, 2, then the midpoints of edges [1,2], [0,2], [0,1]) at (x, y):
+// values and derivatives along the two reference axes.
+template <int NB>
+__device__ __forceinline__ void lagrange_basis(double x, double y, double v[NB], double d0[NB],
+                                      double d1[NB]) {
+  if (NB == 1) {
+    v[0] = 1.0;
+    d0[0] = d1[0] = 0.0;
+  } else {
+    const double l[3] = {1.0 - x - y, x, y};
+    const double g0[3] = {-1.0, 1.0, 0.0}, g1[3] = {-1.0, 0.0, 1.0};
+    if (NB == 3) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        v[i] = l[i];
+        d0[i] = g0[i];
+        d1[i] = g1[i];
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        v[i] = l[i] * (2.0 * l[i] - 1.0);
+        d0[i] = (4.0 * l[i] - 1.0) * g0[i];
+        d1[i] = (4.0 * l[i] - 1.0) * g1[i];
+      }
+      const int ea[3] = {1, 0, 0}, eb[3] = {2, 2, 1};
+#pragma unroll
+      for (int e = 0; e < 3; ++e) {
+        const int a = ea[e], b = eb[e];
+        v[3 + e] = 4.0 * l[a] * l[b];
+        d0[3 + e] = 4.0 * (l[a] * g0[b] + l[b] * g0[a]);
+        d1[3 + e] = 4.0 * (l[a] * g1[b] + l[b] * g1[a]);
+      }
+    }
+  }
+}
+
 // P1 basis on the reference triangle: phi0 = 1 - x - y, phi1 = x, phi2 = y.
 __device__ __forceinline__ void p1_basis(double x, double y, double* phi) {
   phi[0] = 1.0 - x - y;

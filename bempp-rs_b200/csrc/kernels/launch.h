@@ -71,7 +71,7 @@ cudaError_t launch_regular_dp0(const CellSet& test, const CellSet& trial,
 
 // DOF layout of a space for the tile-scatter kernel.
 struct SpaceTiles {
-  int nbasis;               // 1 (DP0) or 3 (P1 / DP1)
+  int nbasis;               // 1 (DP0), 3 (P1 / DP1) or 6 (P2 / DP2)
   int tile_cells;           // cells per tile
   int ntiles;
   int max_tile_dofs;
@@ -82,6 +82,7 @@ struct SpaceTiles {
   // entries b * tile_cells + c, grouped by local DOF
   const uint8_t* inc_off = nullptr;
   const uint8_t* inc_ent = nullptr;
+  const int* cell_dofs = nullptr;  // ncells * nbasis global DOF numbers
 };
 
 // Any pair of spaces: per-tile shared-memory accumulation, then atomic adds into a
@@ -124,6 +125,30 @@ cudaError_t launch_singular(const CellSet& test, const int* test_dofs, int nbt,
                             const CellSet& trial, const int* trial_dofs, int nbs,
                             const SingularRules& rules, const SingularPairs& pairs,
                             const SingularArgs& a, cudaStream_t stream);
+
+// Cell-pair quadrature for any pairing of Lagrange degrees 0..2 (generic.cu), FP64, one
+// warp per pair: the regular part over every (test cell, trial cell in [trial_lo,
+// trial_hi)) pair (vertex-sharing pairs skipped on one grid) with the tensor rule, or the
+// singular list with its Duffy rules.  Adds into the zero-initialised dense output (or
+// stores per-pair blocks, singular only).
+struct GenericPairArgs {
+  int kernel, op;
+  double k;
+  int nbt, nbs;
+  CellSet test, trial;
+  const int* test_dofs;
+  const int* trial_dofs;
+  RegularRule rule;
+  SingularRules rules;
+  SingularPairs pairs;
+  bool singular;
+  int same_grid;
+  void* out;
+  int64_t ld;
+  int trial_lo = 0, trial_hi = 0x7fffffff;
+  double* pair_values = nullptr;
+};
+cudaError_t launch_generic_pairs(const GenericPairArgs& g, cudaStream_t stream);
 
 // Allocation-free regular DP0 assembly between two distinct meshes (noalloc.cu); the
 // scratch lives in a static device array of noalloc_max_cells() cells per mesh and

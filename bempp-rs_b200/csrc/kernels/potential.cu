@@ -65,9 +65,11 @@ __global__ void __launch_bounds__(kThreads)
           kim = f * fma(-kr, cs, sn);
         }
       }
+      double bv[NB], bd0[NB], bd1[NB];  // degree 2: the basis at the point (bd* unused)
+      if (NB == 6) lagrange_basis<NB>(rule.xi[2 * q], rule.xi[2 * q + 1], bv, bd0, bd1);
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
-        const double wb = NB == 1 ? rule.w[q] : rule.wphi[b][q];
+        const double wb = NB == 1 ? rule.w[q] : NB == 3 ? rule.wphi[b][q] : rule.w[q] * bv[b];
         u_re[b] = fma(kre, wb, u_re[b]);
         if (kC) u_im[b] = fma(kim, wb, u_im[b]);
       }
@@ -109,6 +111,7 @@ cudaError_t launch_op(const double* points, int npoints, const CellSet& trial, c
                       cudaStream_t stream) {
   if (nbasis == 1) return launch_nb<KER, OP, 1>(points, npoints, trial, dofs, rule, k, out, ld, stream);
   if (nbasis == 3) return launch_nb<KER, OP, 3>(points, npoints, trial, dofs, rule, k, out, ld, stream);
+  if (nbasis == 6) return launch_nb<KER, OP, 6>(points, npoints, trial, dofs, rule, k, out, ld, stream);
   return cudaErrorInvalidValue;
 }
 

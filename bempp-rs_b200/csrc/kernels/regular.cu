@@ -1480,6 +1480,33 @@ cudaError_t launch_regular_scatter(const CellSet& test, const SpaceTiles& tt,
                                    const CellSet& trial, const SpaceTiles& st,
                                    const RegularRule& rule, const RegularArgs& a,
                                    cudaStream_t stream) {
+  if (tt.nbasis > 3 || st.nbasis > 3) {
+    // degree-2 spaces: the generic warp-per-pair kernel (FP64) over this launch's trial
+    // cells
+    GenericPairArgs g;
+    g.kernel = a.kernel;
+    g.op = a.op;
+    g.k = a.k;
+    g.nbt = tt.nbasis;
+    g.nbs = st.nbasis;
+    g.test = test;
+    g.trial = trial;
+    g.test_dofs = tt.cell_dofs;
+    g.trial_dofs = st.cell_dofs;
+    g.rule = rule;
+    g.rules = SingularRules{};
+    g.pairs = SingularPairs{};
+    g.singular = false;
+    g.same_grid = a.same_grid;
+    g.out = a.out;
+    g.ld = a.ld;
+    const int tiles = (trial.ncells + kTile - 1) / kTile;
+    const int ny = a.trial_tiles > 0 ? std::min(a.trial_tiles, tiles - a.trial_tile0)
+                                     : tiles - a.trial_tile0;
+    g.trial_lo = a.trial_tile0 * kTile;
+    g.trial_hi = std::min(trial.ncells, (a.trial_tile0 + std::max(ny, 0)) * kTile);
+    return launch_generic_pairs(g, stream);
+  }
   if (tt.tile_cells != kTile || st.tile_cells != kTile) return cudaErrorInvalidValue;
   return dispatch(test, tt, trial, st, rule, a, stream, false);
 }

@@ -281,6 +281,29 @@ cudaError_t launch_singular(const CellSet& test, const int* test_dofs, int nbt,
                             const SingularRules& rules, const SingularPairs& pairs,
                             const SingularArgs& a, cudaStream_t stream) {
   if (pairs.npairs <= 0) return cudaSuccess;
+  if (nbt > 3 || nbs > 3) {  // degree-2 spaces: the generic warp-per-pair kernel
+    GenericPairArgs g;
+    g.kernel = a.kernel;
+    g.op = a.op;
+    g.k = a.k;
+    g.nbt = nbt;
+    g.nbs = nbs;
+    g.test = test;
+    g.trial = trial;
+    g.test_dofs = test_dofs;
+    g.trial_dofs = trial_dofs;
+    g.rule = RegularRule{};
+    g.rules = rules;
+    g.pairs = pairs;
+    g.singular = true;
+    g.same_grid = 1;
+    g.out = a.out;
+    g.ld = a.ld;
+    g.trial_lo = a.trial_lo;
+    g.trial_hi = a.trial_hi;
+    g.pair_values = a.pair_values;
+    return launch_generic_pairs(g, stream);
+  }
   return a.kernel == kLaplace
              ? launch_op<kLaplace>(test, test_dofs, nbt, trial, trial_dofs, nbs, rules, pairs, a, stream)
              : launch_op<kHelmholtz>(test, test_dofs, nbt, trial, trial_dofs, nbs, rules, pairs, a, stream);

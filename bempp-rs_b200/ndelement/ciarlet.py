@@ -21,7 +21,8 @@ class Continuity(IntEnum):
 
 
 class CiarletElement:
-    """Lagrange element on a triangle: degree 0 (one DOF) or degree 1 (three DOFs)."""
+    """Lagrange element on a triangle: degree 0 (one DOF), 1 (three) or 2 (six: the
+    vertices, then the midpoints of edges [1,2], [0,2], [0,1])."""
 
     def __init__(self, cell: ReferenceCellType, degree: int, continuity: Continuity):
         self.cell_type = cell
@@ -30,7 +31,7 @@ class CiarletElement:
 
     @property
     def dim(self) -> int:
-        return 1 if self.degree == 0 else 3
+        return {0: 1, 1: 3, 2: 6}[self.degree]
 
 
 class ElementFamily:

@@ -302,7 +302,10 @@ GridT *bempp_grid_from_points_cells(const void *points, size_t npoints, DType dt
                                     const size_t *cells, size_t ncells);
 /* src/bindings/ndgrid.rs:6-16 (null-safe) */
 void grid_t_free_bempp(GridT *ptr);
-/* src/bindings/ndelement.rs:18-25: Lagrange degree 0 or 1 on triangles */
+/* src/bindings/ndelement.rs:18-25: Lagrange degree 0, 1 or 2 on triangles (degree 2:
+ * DOFs at the vertices, then at the midpoints of edges [1,2], [0,2], [0,1], nodal basis;
+ * spaces of degree 2 are assembled in FP64 by a warp-per-cell-pair kernel whatever the
+ * precision option) */
 ElementFamilyT *create_lagrange_family_bempp(size_t degree, Continuity continuity,
                                              DType dtype);
 /* src/bindings/ndelement.rs:27-43: not supported (returns NULL, records an error) */

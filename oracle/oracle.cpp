@@ -21,7 +21,9 @@
 //     (Springer 2011), section 5.2, regularising transformations for identical,
 //     edge-adjacent and vertex-adjacent triangles with n-point Gauss-Legendre per axis;
 //   ndelement (git main, no rev) `simplex_rule`: fully symmetric triangle rules by point
-//     count (generated table, see gen_simplex_rules.py), P1/DP0 Lagrange tabulation.
+//     count (generated table, see gen_simplex_rules.py); Lagrange tabulation of degree 0, 1
+//     and 2 with ndelement's DOF order on the reference triangle (vertices 0, 1, 2, then
+//     the midpoints of edges 0 = [1,2], 1 = [0,2], 2 = [0,1]; nodal basis).
 // Parity with bempp-rs itself is pinned by the bempp-cl golden matrices of
 // tests/compare_to_bempp_cl.rs (absolute 1e-3 / 1e-4); the exact Duffy point sets of
 // bempp-quadrature cannot be checked here (unpinned at the 1e-12 level).
@@ -34,6 +36,7 @@
 #include <complex>
 #include <cstdint>
 #include <cstring>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -67,7 +70,16 @@ struct Mesh {
       for (int i = 0; i < 3; ++i) vertex_cells[cells[3 * c + i]].push_back(c);
   }
   int64_t v(int64_t c, int i) const { return cells[3 * c + i]; }
+  // local edge i of cell c joins its vertices other than i (ndelement's reference
+  // triangle: edges [1,2], [0,2], [0,1])
+  std::pair<int64_t, int64_t> edge(int64_t c, int i) const {
+    const int64_t a = v(c, (i + 1) % 3), b = v(c, (i + 2) % 3);
+    return {std::min(a, b), std::max(a, b)};
+  }
 };
+
+constexpr int kMaxBasis = 6;
+inline int nbasis_of(int degree) { return degree == 0 ? 1 : degree == 1 ? 3 : 6; }
 
 struct Space {
   int degree = 0;
@@ -105,8 +117,33 @@ Space make_space(const Mesh& m, int degree, bool continuous) {
       for (int64_t c = 0; c < 3 * m.ncells; ++c) s.cell_dofs[c] = c;
       s.ndofs = 3 * m.ncells;
     }
+  } else if (degree == 2) {
+    s.nbasis = 6;
+    s.cell_dofs.resize(6 * m.ncells);
+    if (continuous) {
+      // per cell: its vertices, then its edges, each in local order
+      std::vector<int64_t> vdof(m.npts, -1);
+      std::map<std::pair<int64_t, int64_t>, int64_t> edof;
+      int64_t size = 0;
+      for (int64_t c = 0; c < m.ncells; ++c) {
+        for (int i = 0; i < 3; ++i) {
+          int64_t v = m.v(c, i);
+          if (vdof[v] < 0) vdof[v] = size++;
+          s.cell_dofs[6 * c + i] = vdof[v];
+        }
+        for (int i = 0; i < 3; ++i) {
+          auto it = edof.find(m.edge(c, i));
+          if (it == edof.end()) it = edof.emplace(m.edge(c, i), size++).first;
+          s.cell_dofs[6 * c + 3 + i] = it->second;
+        }
+      }
+      s.ndofs = size;
+    } else {
+      for (int64_t c = 0; c < 6 * m.ncells; ++c) s.cell_dofs[c] = c;
+      s.ndofs = 6 * m.ncells;
+    }
   } else {
-    throw std::runtime_error("oracle: only degree 0 and 1 Lagrange spaces");
+    throw std::runtime_error("oracle: only degree 0, 1 and 2 Lagrange spaces");
   }
   return s;
 }
@@ -329,18 +366,36 @@ struct CellGeom {
 
 enum Op { kSingleLayer = 0, kDoubleLayer = 1, kAdjointDoubleLayer = 2, kHypersingular = 3 };
 
-// basis tables: value, d/dxi0, d/dxi1 for basis b at reference point xi
-inline void tabulate(int degree, const double* xi, double val[3], double d0[3], double d1[3]) {
+// basis tables: value, d/dxi0, d/dxi1 for basis b at reference point xi.  Degree 2: the
+// nodal basis of the vertices and edge midpoints, with l0 = 1 - x - y, l1 = x, l2 = y:
+// l_i (2 l_i - 1) at vertex i, then 4 l1 l2, 4 l0 l2, 4 l0 l1 at edges 0, 1, 2.
+inline void tabulate(int degree, const double* xi, double val[kMaxBasis],
+                     double d0[kMaxBasis], double d1[kMaxBasis]) {
   if (degree == 0) {
     val[0] = 1.0;
     d0[0] = 0.0;
     d1[0] = 0.0;
-  } else {
+  } else if (degree == 1) {
     val[0] = 1.0 - xi[0] - xi[1];
     val[1] = xi[0];
     val[2] = xi[1];
     d0[0] = -1.0; d0[1] = 1.0; d0[2] = 0.0;
     d1[0] = -1.0; d1[1] = 0.0; d1[2] = 1.0;
+  } else {
+    const double l[3] = {1.0 - xi[0] - xi[1], xi[0], xi[1]};
+    const double g0[3] = {-1.0, 1.0, 0.0}, g1[3] = {-1.0, 0.0, 1.0};  // grad l_i
+    for (int i = 0; i < 3; ++i) {
+      val[i] = l[i] * (2.0 * l[i] - 1.0);
+      d0[i] = (4.0 * l[i] - 1.0) * g0[i];
+      d1[i] = (4.0 * l[i] - 1.0) * g1[i];
+    }
+    const int ea[3] = {1, 0, 0}, eb[3] = {2, 2, 1};
+    for (int e = 0; e < 3; ++e) {
+      const int a = ea[e], b = eb[e];
+      val[3 + e] = 4.0 * l[a] * l[b];
+      d0[3 + e] = 4.0 * (l[a] * g0[b] + l[b] * g0[a]);
+      d1[3 + e] = 4.0 * (l[a] * g1[b] + l[b] * g1[a]);
+    }
   }
 }
 
@@ -445,10 +500,11 @@ void assemble(const Mesh& m, const Space& test, const Space& trial, const Assemb
     const int Q = static_cast<int>(rule.wts.size());
     // tables: the reference tabulates the trial table at the test points
     // (src/boundary_assemblers.rs:464); identical rules on both sides make it the same.
-    std::vector<double> tv(Q * 3), td0(Q * 3), td1(Q * 3), sv(Q * 3), sd0(Q * 3), sd1(Q * 3);
+    constexpr int B = kMaxBasis;
+    std::vector<double> tv(Q * B), td0(Q * B), td1(Q * B), sv(Q * B), sd0(Q * B), sd1(Q * B);
     for (int p = 0; p < Q; ++p) {
-      tabulate(test.degree, &rule.pts[2 * p], &tv[3 * p], &td0[3 * p], &td1[3 * p]);
-      tabulate(trial.degree, &rule.pts[2 * p], &sv[3 * p], &sd0[3 * p], &sd1[3 * p]);
+      tabulate(test.degree, &rule.pts[2 * p], &tv[B * p], &td0[B * p], &td1[B * p]);
+      tabulate(trial.degree, &rule.pts[2 * p], &sv[B * p], &sd0[B * p], &sd1[B * p]);
     }
     auto tcol = colouring(m, test);
     auto scol = colouring(m, trial);
@@ -484,7 +540,7 @@ void assemble(const Mesh& m, const Space& test, const Space& trial, const Assemb
           }
           std::vector<KernelVals<T>> kmat(Q * Q);
           std::vector<double> spts(Q * 3);
-          T local[9];
+          T local[kMaxBasis * kMaxBasis];
           for (int64_t j = s0; j < s1; ++j) {
             int64_t sc_cell = sc[j];
             CellGeom sg;
@@ -505,8 +561,8 @@ void assemble(const Mesh& m, const Space& test, const Space& trial, const Assemb
                   for (int p = 0; p < Q; ++p) {
                     double tw = rule.wts[p] * tg.jdet;
                     for (int q = 0; q < Q; ++q) {
-                      e += integ.eval(kmat[p * Q + q], aa, b, &tv[3 * p], &td0[3 * p],
-                                      &td1[3 * p], &sv[3 * q], &sd0[3 * q], &sd1[3 * q], tg,
+                      e += integ.eval(kmat[p * Q + q], aa, b, &tv[B * p], &td0[B * p],
+                                      &td1[B * p], &sv[B * q], &sd0[B * q], &sd1[B * q], tg,
                                       sg, hel) *
                            (rule.wts[q] * sg.jdet) * tw;
                     }
@@ -556,10 +612,11 @@ void assemble(const Mesh& m, const Space& test, const Space& trial, const Assemb
     for (int64_t ci = 0; ci < static_cast<int64_t>(configs.size()); ++ci) {
       const TestTrialRule& r = rules[ci];
       const int n = r.n();
-      std::vector<double> tv(n * 3), td0(n * 3), td1(n * 3), sv(n * 3), sd0(n * 3), sd1(n * 3);
+      constexpr int B = kMaxBasis;
+      std::vector<double> tv(n * B), td0(n * B), td1(n * B), sv(n * B), sd0(n * B), sd1(n * B);
       for (int i = 0; i < n; ++i) {
-        tabulate(test.degree, &r.test_pts[2 * i], &tv[3 * i], &td0[3 * i], &td1[3 * i]);
-        tabulate(trial.degree, &r.trial_pts[2 * i], &sv[3 * i], &sd0[3 * i], &sd1[3 * i]);
+        tabulate(test.degree, &r.test_pts[2 * i], &tv[B * i], &td0[B * i], &td1[B * i]);
+        tabulate(trial.degree, &r.trial_pts[2 * i], &sv[B * i], &sd0[B * i], &sd1[B * i]);
       }
       std::vector<KernelVals<T>> kv(n);
       for (auto& pr : cell_pairs[ci]) {
@@ -577,8 +634,8 @@ void assemble(const Mesh& m, const Space& test, const Space& trial, const Assemb
           for (int aa = 0; aa < ntb; ++aa) {
             T e = T(0.0);
             for (int i = 0; i < n; ++i)
-              e += integ.eval(kv[i], aa, b, &tv[3 * i], &td0[3 * i], &td1[3 * i], &sv[3 * i],
-                              &sd0[3 * i], &sd1[3 * i], tg, sg, hel) *
+              e += integ.eval(kv[i], aa, b, &tv[B * i], &td0[B * i], &td1[B * i], &sv[B * i],
+                              &sd0[B * i], &sd1[B * i], tg, sg, hel) *
                    (r.wts[i] * tg.jdet * sg.jdet);
             per_config[ci].push_back({test.cell_dofs[pr.first * ntb + aa],
                                       trial.cell_dofs[pr.second * nsb + b], e});
@@ -628,7 +685,7 @@ int oracle_assemble_dense(int helmholtz, int op, double k, const double* points,
   }
 }
 
-// DOF map of a degree-0/1 Lagrange space (src/function.rs:365-445); returns ndofs and
+// DOF map of a degree-0/1/2 Lagrange space (src/function.rs:365-445); returns ndofs and
 // writes ncells * nbasis DOF numbers.
 int64_t oracle_cell_dofs(const int64_t* cells, int64_t ncells, int64_t npoints, int degree,
                          int continuous, int64_t* cell_dofs) {

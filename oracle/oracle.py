@@ -82,9 +82,13 @@ def _ptr(a, ctype):
     return a.ctypes.data_as(ctypes.POINTER(ctype))
 
 
+def nbasis(degree):
+    return {0: 1, 1: 3, 2: 6}[degree]
+
+
 def space_size(points, cells, degree, continuous):
     cells = np.ascontiguousarray(cells, dtype=np.int64)
-    out = np.empty(cells.shape[0] * (1 if degree == 0 else 3), dtype=np.int64)
+    out = np.empty(cells.shape[0] * nbasis(degree), dtype=np.int64)
     return int(lib().oracle_cell_dofs(_ptr(cells, ctypes.c_int64), cells.shape[0],
                                       len(points), degree, int(continuous),
                                       _ptr(out, ctypes.c_int64)))
@@ -92,7 +96,7 @@ def space_size(points, cells, degree, continuous):
 
 def cell_dofs(points, cells, degree, continuous):
     cells = np.ascontiguousarray(cells, dtype=np.int64)
-    nb = 1 if degree == 0 else 3
+    nb = nbasis(degree)
     out = np.empty(cells.shape[0] * nb, dtype=np.int64)
     n = lib().oracle_cell_dofs(_ptr(cells, ctypes.c_int64), cells.shape[0], len(points),
                                degree, int(continuous), _ptr(out, ctypes.c_int64))

@@ -48,10 +48,14 @@ def potential(x, points, cells, kernel, operator, *, k=0.0, degree=0, continuous
             kern = kern * np.exp(1j * k * r) * (1.0 - 1j * k * r)
     else:
         raise ValueError("potential operators: single_layer and double_layer")
+    l0, l1, l2 = 1.0 - xi[:, 0] - xi[:, 1], xi[:, 0], xi[:, 1]
     if degree == 0:
         basis = np.ones((len(w), 1))
-    else:
-        basis = np.stack([1.0 - xi[:, 0] - xi[:, 1], xi[:, 0], xi[:, 1]], axis=1)
+    elif degree == 1:
+        basis = np.stack([l0, l1, l2], axis=1)
+    else:  # nodal P2 basis: vertices, then midpoints of edges [1,2], [0,2], [0,1]
+        basis = np.stack([l0 * (2 * l0 - 1), l1 * (2 * l1 - 1), l2 * (2 * l2 - 1),
+                          4 * l1 * l2, 4 * l0 * l2, 4 * l0 * l1], axis=1)
     local = np.einsum("icq,q,qb,c->icb", kern, w, basis, jdet) / (4.0 * np.pi)
     out = np.zeros((x.shape[0], n), dtype=local.dtype)
     for b in range(dofs.shape[1]):

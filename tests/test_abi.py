@@ -450,3 +450,64 @@ def test_ndgrid_topology_is_validated():
                                                                                dtype=np.uintp))
     assert g == ffi.NULL
     assert "out of range" in _lib.last_error()
+
+
+# ------------------------------------------------------------ degree-2 spaces ---
+@pytest.mark.parametrize("level", range(3))
+def test_space_sizes_p2(level):
+    """python/test/test_function_space.py:31-41 and tests/test_space.rs (Lagrange 2): one
+    DOF per vertex and per edge; DP2 has six per cell."""
+    grid = regular_sphere(level)
+    p2 = function_space(grid, create_family(Family.Lagrange, 2))
+    assert p2.local_size == p2.global_size == (grid.entity_count(ReferenceCellType.Point) +
+                                               grid.entity_count(ReferenceCellType.Interval))
+    assert p2.is_serial
+    dp2 = function_space(grid, create_family(Family.Lagrange, 2, Continuity.Discontinuous))
+    assert dp2.global_size == 6 * grid.entity_count(ReferenceCellType.Triangle)
+
+
+@pytest.mark.parametrize("cont", [True, False])
+def test_p2_dof_numbering_matches_oracle(cont):
+    pts, cells = shapes.icosphere(2)
+    grid = Grid(pts, cells)
+    sp = function_space(grid, create_family(
+        Family.Lagrange, 2, Continuity.Standard if cont else Continuity.Discontinuous))
+    ref, n = oracle.cell_dofs(pts, cells, 2, cont)
+    assert sp.global_size == n
+    assert np.array_equal(np.array([sp.cell_dofs(c) for c in range(len(cells))]), ref)
+    if cont:
+        # the edge DOFs: get_local_dof_numbers(1, e) is the DOF of edge e, and the cell's
+        # local DOF 3 + i sits on its local edge i (opposite vertex i)
+        seen = set()
+        for c in range(len(cells)):
+            for i in range(3):
+                assert sp.get_local_dof_numbers(0, int(cells[c, i])) == [ref[c, i]]
+            seen.update(int(d) for d in ref[c, 3:])
+        edge_dofs = set()
+        e = 0
+        while True:
+            d = sp.get_local_dof_numbers(1, e)
+            if not d:
+                break
+            edge_dofs.update(d)
+            e += 1
+        assert edge_dofs == seen and e == len(seen)
+        col = sp.cell_colouring()[ReferenceCellType.Triangle]
+        ours = np.zeros(len(cells), dtype=np.int64)
+        for k, group in enumerate(col):
+            ours[group] = k
+        refc, nc = oracle.colouring(pts, cells, 2, True)
+        assert nc == len(col) and np.array_equal(ours, refc)
+
+
+def test_p2_ndgrid_edge_numbering_is_kept():
+    """Through ndgrid's arrays the edge DOFs hang on ndgrid's edges: the library keeps the
+    given cell -> edge numbering, so entity (1, e) is ndgrid's edge e."""
+    pts, cells = shapes.icosphere(1)
+    grid = Grid(pts, cells, cell_vertices=cells)
+    t = grid.topology_arrays()
+    sp = function_space(grid, create_family(Family.Lagrange, 2))
+    for c in range(len(cells)):
+        dofs = sp.cell_dofs(c)
+        for i in range(3):
+            assert sp.get_local_dof_numbers(1, int(t["cell_edges"][c, i])) == [dofs[3 + i]]

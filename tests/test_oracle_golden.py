@@ -81,3 +81,55 @@ def test_potential_oracle_matches_bempp_cl(golden_potentials, index):
     assert np.abs(p.real - ref.real).max() <= case["epsilon"]
     if np.iscomplexobj(ref):
         assert np.abs(p.imag - ref.imag).max() <= case["epsilon"]
+
+
+@pytest.mark.parametrize("kernel,op,k", [("laplace", "single_layer", 0.0),
+                                         ("laplace", "double_layer", 0.0),
+                                         ("laplace", "adjoint_double_layer", 0.0),
+                                         ("laplace", "hypersingular", 0.0),
+                                         ("helmholtz", "single_layer", 3.0),
+                                         ("helmholtz", "hypersingular", 3.0)])
+def test_oracle_p2_restricted_to_p1_is_the_p1_matrix(kernel, op, k):
+    """The degree-2 Lagrange space contains the degree-1 one: phi_v(P1) = phi_v(P2) +
+    (phi_e1 + phi_e2) / 2 over the two edges of the cell at v.  With that interpolation T,
+    T^T A(P2) T must equal A(P1), whose values and derivatives the bempp-cl goldens pin
+    (the hypersingular operator tests the P2 derivatives and the edge DOF order)."""
+    pts, cells = shapes.icosphere(1)
+    pts = shapes.radial_perturbation(pts, seed=3)
+    d2, n2 = oracle.cell_dofs(pts, cells, 2, True)
+    d1, n1 = oracle.cell_dofs(pts, cells, 1, True)
+    T = np.zeros((n2, n1))
+    for c in range(len(cells)):
+        for i in range(3):
+            T[d2[c, i], d1[c, i]] = 1.0
+        for e in range(3):  # local edge e joins local vertices e+1, e+2 (mod 3)
+            T[d2[c, 3 + e], d1[c, (e + 1) % 3]] = 0.5
+            T[d2[c, 3 + e], d1[c, (e + 2) % 3]] = 0.5
+    kw = dict(k=k, q_regular=6)
+    a2 = oracle.assemble(pts, cells, kernel, op, test_degree=2, test_continuous=True,
+                         trial_degree=2, trial_continuous=True, **kw)
+    a1 = oracle.assemble(pts, cells, kernel, op, test_degree=1, test_continuous=True,
+                         trial_degree=1, trial_continuous=True, **kw)
+    r = T.T @ a2 @ T
+    assert np.linalg.norm(r - a1) / np.linalg.norm(a1) <= 1e-13
+
+
+def test_oracle_p2_potential_restricted_to_p1():
+    from oracle import potential
+
+    pts, cells = shapes.icosphere(1)
+    d2, n2 = oracle.cell_dofs(pts, cells, 2, True)
+    d1, n1 = oracle.cell_dofs(pts, cells, 1, True)
+    T = np.zeros((n2, n1))
+    for c in range(len(cells)):
+        for i in range(3):
+            T[d2[c, i], d1[c, i]] = 1.0
+        for e in range(3):
+            T[d2[c, 3 + e], d1[c, (e + 1) % 3]] = 0.5
+            T[d2[c, 3 + e], d1[c, (e + 2) % 3]] = 0.5
+    x = np.array([[2.0, 0.1, 0.0], [0.0, -1.7, 0.4], [0.3, 0.2, 2.5]])
+    p2 = potential.potential(x, pts, cells, "helmholtz", "double_layer", k=2.0, degree=2,
+                             continuous=True, q_regular=6)
+    p1 = potential.potential(x, pts, cells, "helmholtz", "double_layer", k=2.0, degree=1,
+                             continuous=True, q_regular=6)
+    assert np.linalg.norm(p2 @ T - p1) / np.linalg.norm(p1) <= 1e-13
