@@ -453,8 +453,8 @@ void check_potential(const BoundaryAssemblerT& a, const SpaceT& space, int64_t n
   if (a.op != kSL && a.op != kDL)
     throw Error(kUnsupported, "potential operators: single and double layer only");
   if (npoints < 0 || npoints > 0x7fffffff) throw Error(kInvalidArgument, "point count");
-  if (space.nbasis != 1 && space.nbasis != 3)
-    throw Error(kUnsupported, "potential operators: DP0 and P1 spaces");
+  if (space.nbasis != 1 && space.nbasis != 3 && space.nbasis != 6)
+    throw Error(kUnsupported, "potential operators: Lagrange spaces of degree 0, 1 or 2");
 }
 }  // namespace
 
