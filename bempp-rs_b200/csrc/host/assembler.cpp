@@ -510,6 +510,8 @@ void assemble_potential_host(BoundaryAssemblerT& a, SpaceT& space, const double*
   BEMPP_CUDA(cudaStreamSynchronize(a.stream));
 }
 
+SingularPairList& sweep_pairs(GridT& g, int device) { return grid_pairs(g, device); }
+
 SingularRules sweep_rules(int device, int order) {
   const DeviceRules& dr = device_rules(device, order);
   return SingularRules{dr.offset.as<int>(), dr.test_xi.as<double>(), dr.trial_xi.as<double>(),

@@ -76,6 +76,7 @@ long long count_items(SweepArgs& a, int kchunk, int tile_shape) {
 // Defined in assembler.cpp.
 const GridGeometry& sweep_geometry(GridT& g, int device, const RegularRule& rule);
 SingularRules sweep_rules(int device, int order);
+SingularPairList& sweep_pairs(GridT& g, int device);
 
 void helmholtz_sl_sweep_device(GridT* const* grids, size_t ngrids, const double* ks, size_t nk,
                                const Options& opts, void* const* outs, cudaStream_t stream) {
@@ -126,9 +127,24 @@ void helmholtz_sl_sweep_device(GridT* const* grids, size_t ngrids, const double*
       m.cells.vids = geo.vids.as<int>();
       m.out = static_cast<float2*>(outs[i]);
       m.ntiles = static_cast<int>((grids[i]->ncells + 31) / 32);
+      // near field of the mesh with itself (the masks the far-pair kernel skips, the near
+      // pairs) and its vertex-sharing pairs
+      const NearField& nf = near_field(*grids[i], *grids[i]);
+      m.tile_mask = nf.tile_mask.as<int>();
+      m.masks = nf.masks.as<unsigned>();
+      m.near_pairs = nf.pairs.as<int2>();
+      m.nnear = nf.npairs;
+      SingularPairList& pl = sweep_pairs(*grids[i], device);
+      m.sing = SingularPairs{static_cast<int>(pl.test_cell.size()), pl.d_test.as<int>(),
+                             pl.d_trial.as<int>(), pl.d_config.as<int>()};
       sizes.push_back(grids[i]->ncells);
     }
     a.nmesh = static_cast<int>(ngrids);
+    a.near_begin[0] = a.sing_begin[0] = 0;
+    for (size_t r = 0; r < ngrids; ++r) {
+      a.near_begin[r + 1] = a.near_begin[r] + static_cast<long long>(a.mesh[r].nnear) * nk;
+      a.sing_begin[r + 1] = a.sing_begin[r] + static_cast<long long>(a.mesh[r].sing.npairs) * nk;
+    }
     a.ks = plan->d_ks.as<double>();
     a.nk = static_cast<int>(nk);
     a.counter = plan->d_counter.as<unsigned long long>();
@@ -186,14 +202,27 @@ void helmholtz_sl_sweep_device(GridT* const* grids, size_t ngrids, const double*
     plan->tuning = it->second;
     count_items(a, plan->tuning.kchunk, plan->tuning.tile_shape);
 
-    // capture: counter reset + persistent launch
-    cudaStream_t cs;
+    // capture: counter reset + the persistent far-pair launch on one branch, the FP64
+    // near and vertex-sharing launches on a forked branch (they write disjoint entries)
+    cudaStream_t cs, side;
+    cudaEvent_t fork, join;
     BEMPP_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    BEMPP_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    BEMPP_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    BEMPP_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
     BEMPP_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e1 = cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), cs);
-    cudaError_t e2 = launch_sweep_sl(a, rule, rules, plan->tuning.blocks_per_sm, sms, cs);
+    cudaError_t e1 = cudaEventRecord(fork, cs);
+    if (e1 == cudaSuccess) e1 = cudaStreamWaitEvent(side, fork, 0);
+    if (e1 == cudaSuccess) e1 = launch_sweep_near_singular(a, rule, rules, side);
+    if (e1 == cudaSuccess) e1 = cudaEventRecord(join, side);
+    cudaError_t e2 = e1 == cudaSuccess ? cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), cs) : e1;
+    if (e2 == cudaSuccess) e2 = launch_sweep_sl(a, rule, rules, plan->tuning.blocks_per_sm, sms, cs);
+    if (e2 == cudaSuccess && e1 == cudaSuccess) e2 = cudaStreamWaitEvent(cs, join, 0);
     cudaError_t e3 = cudaStreamEndCapture(cs, &plan->graph);
     cudaStreamDestroy(cs);
+    cudaStreamDestroy(side);
+    cudaEventDestroy(fork);
+    cudaEventDestroy(join);
     BEMPP_CUDA(e1);
     BEMPP_CUDA(e2);
     BEMPP_CUDA(e3);

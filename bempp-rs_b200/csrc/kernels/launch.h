@@ -188,6 +188,14 @@ struct SweepMesh {
   float2* out;            // nk column-major ncells x ncells matrices, wavenumber-major
   int ntiles;             // ceil(ncells / 32)
   long long item_begin;   // first work item of this mesh
+  // near field of the mesh with itself (NearArgs layout): per tile pair the index of its
+  // 32-word mask of near or vertex-sharing pairs (or -1); the near pairs that share no
+  // vertex, and the vertex-sharing pairs with their adjacency configuration
+  const int* tile_mask;
+  const unsigned* masks;
+  const int2* near_pairs;
+  int nnear;
+  SingularPairs sing;
 };
 struct SweepArgs {
   SweepMesh mesh[kMaxSweepMeshes];
@@ -198,12 +206,22 @@ struct SweepArgs {
   int tile_shape = 1;     // a work item covers tile_shape x tile_shape pairs of 32-cell tiles
   long long nitems;
   unsigned long long* counter;  // work counter, zeroed before each launch
+  // prefix sums over the meshes of (near pairs x nk) and (vertex-sharing pairs x nk)
+  long long near_begin[kMaxSweepMeshes + 1];
+  long long sing_begin[kMaxSweepMeshes + 1];
 };
 size_t sweep_smem_bytes(int tile_shape);
-// Persistent launch of blocks_per_sm (at most 6) x sms CTAs.
+// The far pairs of every item: persistent launch of blocks_per_sm (at most 6) x sms CTAs
+// (FP32, the pairs marked in the meshes' near-field masks left alone).
 cudaError_t launch_sweep_sl(const SweepArgs& args, const RegularRule& rule,
                             const SingularRules& rules, int blocks_per_sm, int sms,
                             cudaStream_t stream);
+// The near pairs (FP64, one thread per pair and wavenumber) and the vertex-sharing pairs
+// (their Duffy rules, FP64, one warp per pair and wavenumber) of every mesh and
+// wavenumber: they write the entries the far-pair launch leaves alone, so both may run
+// concurrently.
+cudaError_t launch_sweep_near_singular(const SweepArgs& args, const RegularRule& rule,
+                                       const SingularRules& rules, cudaStream_t stream);
 
 // CUDA-core FMA throughput probe (diag.cu).
 cudaError_t measure_fma_peak(int fp64, int iters, int reps, double* tflops);

@@ -50,6 +50,7 @@ namespace bempp_b200 {
 namespace {
 
 constexpr float kSmallPhaseMax = 0.8f;
+constexpr float kWidePhaseMax = 1.6f;
 
 // Blocks whose tile copies did not complete within the bounded wait (never expected).
 __device__ unsigned g_stage_timeouts = 0;
@@ -441,7 +442,8 @@ __device__ __forceinline__ void far_sums(const Tile& T, int it, const Tile& S, i
 // issue slots of the inner loop; both points arrive in two 128-bit shared-memory loads
 // (the paired layout of the FP32 offsets).  Even and odd trial points are summed
 // separately and added per test point.
-template <int QT, int KER, int OP, int NBT, int NBS>
+// kWide: the phases may reach |k (r - r0)| <= 1.6 (poly_cos_sin_wide2).
+template <int QT, int KER, int OP, int NBT, int NBS, bool kWide = false>
 __device__ __forceinline__ void far_sums_x2(const Tile& T, int it, const Tile& S, int js,
                                             const RegularRule& rule, const FarPair<QT>& fp,
                                             float blk_re[NBT][NBS], float blk_im[NBT][NBS],
@@ -481,7 +483,10 @@ __device__ __forceinline__ void far_sums_x2(const Tile& T, int it, const Tile& S
         const float2 rinv = rsqrt_approx2(r2);
         const float2 t = fmul2(fmul2(kf2, s), rcp_approx2(ffma2(r2, rinv, r0f2)));  // k (r - r0)
         float2 cs, ss;
-        poly_cos_sin2(t, cs, ss);
+        if (kWide)
+          poly_cos_sin_wide2(t, cs, ss);
+        else
+          poly_cos_sin2(t, cs, ss);
         if (OP == kSL || OP == kHS) {
           f = fmul2(wq, rinv);
           c = cs;
@@ -545,9 +550,11 @@ __device__ __forceinline__ void far_sums_x2(const Tile& T, int it, const Tile& S
   }
 }
 
-// Phase handling of a launch (Helmholtz far pairs): kPhaseRuntime chooses per warp,
-// kPhaseSmall assumes |k (r - r0)| <= 0.8 for every pair of the launch (the host checks
-// k (max rad_x + max rad_y) <= 0.8), kPhaseGeneral reduces every phase.
+// Phase handling of a launch (Helmholtz far pairs): kPhaseRuntime chooses per warp (the
+// unreduced polynomials of |t| <= 0.8 or, for even rules, of |t| <= 1.6 when the warp's
+// k (rad_x + rad_y) allows it, else the reduction), kPhaseSmall assumes |k (r - r0)| <= 0.8
+// for every pair of the launch (the host checks k (max rad_x + max rad_y) <= 0.8),
+// kPhaseGeneral reduces every phase.
 enum PhaseMode : int { kPhaseRuntime = 0, kPhaseSmall = 1, kPhaseGeneral = 2 };
 
 // FP32 local block of a far pair (see the file comment for the formulation).
@@ -579,6 +586,7 @@ __device__ __forceinline__ void block_fp32(const Tile& T, int it, const Tile& S,
   }
   float ph_c = 1.f, ph_s = 0.f;
   bool small_phase = PH != kPhaseGeneral;  // kPhaseRuntime: decided per warp below
+  bool wide_phase = false;
   fp.r0f = fp.kf = 0.f;
   fp.r0sq = fmaf(fdx, fdx, fmaf(fdy, fdy, fdz * fdz));
   if (kC) {
@@ -588,10 +596,13 @@ __device__ __forceinline__ void block_fp32(const Tile& T, int it, const Tile& S,
     fp.r0sq = static_cast<float>(r0sq);
     fp.kf = static_cast<float>(k);
     phase_cos_sin(k * r0, ph_c, ph_s);
-    // warp-uniform choice, so that a warp never runs both variants
-    if (PH == kPhaseRuntime)
-      small_phase = __all_sync(__activemask(), k * (T.G(fRad, it) + S.G(fRad, js)) <=
-                                                   static_cast<double>(kSmallPhaseMax));
+    // warp-uniform choice, so that a warp never runs two variants
+    if (PH == kPhaseRuntime) {
+      const double bound = k * (T.G(fRad, it) + S.G(fRad, js));
+      const unsigned active = __activemask();
+      small_phase = __all_sync(active, bound <= static_cast<double>(kSmallPhaseMax));
+      wide_phase = __all_sync(active, bound <= static_cast<double>(kWidePhaseMax));
+    }
   }
   if (OP == kADL) {
 #pragma unroll
@@ -616,10 +627,14 @@ __device__ __forceinline__ void block_fp32(const Tile& T, int it, const Tile& S,
   } else if (PH == kPhaseGeneral) {
     far_sums<QT, KER, OP, NBT, NBS, false>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
   } else {
-    if (small_phase)
+    if (small_phase) {
       small();
-    else
+    } else if (kPacked && wide_phase) {
+      if constexpr (kPacked)
+        far_sums_x2<QT, KER, OP, NBT, NBS, true>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
+    } else {
       far_sums<QT, KER, OP, NBT, NBS, false>(T, it, S, js, rule, fp, blk_re, blk_im, S_re, S_im);
+    }
   }
   // back to FP64, applying the reference phase e^{ik r0}
   double bre[NBT][NBS], bim[NBT][NBS];
@@ -1008,103 +1023,38 @@ __global__ void __launch_bounds__(kThreads)
 // ------------------------------------------------------------------------------------
 // Batched Helmholtz single-layer DP0 sweep over many wavenumbers and meshes.
 //
-// One persistent launch: every CTA repeatedly takes the next work item (mesh, test tile,
-// trial tile, chunk of wavenumbers) from a global counter (items of the largest mesh
-// first), stages the two tiles once, and for each wavenumber of its chunk writes the
-// complete 32 x 32 block of complex64 entries: far pairs in FP32 (block_fp32), near pairs
-// in FP64 (block_fp64), vertex-sharing pairs by their Duffy rule in FP64 (one warp per
-// pair).  The single layer is symmetric on one mesh, so only tile pairs (test tile >=
-// trial tile) are items: an off-diagonal item also writes the transposed block (through
-// shared memory, coalesced), whose vertex-sharing entries take their own Duffy rule (the
-// rules of the two orders of a pair differ).  No two items write the same entry, so the
-// launch needs no ordering or atomics on the output; the only shared state is the item
-// counter (reset before every launch).
-
-// Adjacency configuration (0..27, the order of singular_configurations()) of two cells
-// with vertex ids a[3] (test) and b[3] (trial) that share at least one vertex.
-__device__ __forceinline__ int adjacency_config(const int a[3], const int b[3], bool same) {
-  if (same) return 27;
-  int ts[3], ss[3], n = 0;
-  for (int si = 0; si < 3; ++si)
-    for (int ti = 0; ti < 3; ++ti)
-      if (a[ti] == b[si]) {
-        ts[n] = ti;
-        ss[n] = si;
-        ++n;
-      }
-  if (n == 1) return ts[0] * 3 + ss[0];
-  // edge: test edge opposite vertex 3 - t0 - t1, trial edge opposite 3 - s0 - s1
-  const int et = 3 - ts[0] - ts[1], es = 3 - ss[0] - ss[1];
-  return 9 + (et * 3 + es) * 2 + (ts[0] < ts[1] ? 0 : 1);
-}
-
-// Single-layer integral of one vertex-sharing pair over its Duffy rule (FP64), summed by
-// a warp; every lane returns the total.
-__device__ void duffy_sl_dp0_warp(const Tile& T, int it, const Tile& S, int js, int cfg,
-                                  const SingularRules& rules, double k, double& re, double& im) {
-  const int lane = threadIdx.x & 31;
-  double v0x[3], t0x[3], t1x[3], v0y[3], t0y[3], t1y[3];
-  for (int d = 0; d < 3; ++d) {
-    t0x[d] = T.G(fT0x + d, it);
-    t1x[d] = T.G(fT1x + d, it);
-    v0x[d] = T.G(fCx + d, it) - (t0x[d] + t1x[d]) / 3.0;
-    t0y[d] = S.G(fT0x + d, js);
-    t1y[d] = S.G(fT1x + d, js);
-    v0y[d] = S.G(fCx + d, js) - (t0y[d] + t1y[d]) / 3.0;
-  }
-  const int off = __ldg(rules.offset + cfg), npts = __ldg(rules.offset + cfg + 1) - off;
-  // |k r| <= k (diam_x + diam_y): no reduction of the phase when that is below pi/4
-  const bool small_phase = k * (T.G(fDiam, it) + S.G(fDiam, js)) <= 0.78;
-  double sr = 0.0, si = 0.0;
-  for (int ii = lane; ii < npts; ii += 32) {
-    const int i = off + ii;
-    const double xi0 = __ldg(rules.test_xi + 2 * i), xi1 = __ldg(rules.test_xi + 2 * i + 1);
-    const double et0 = __ldg(rules.trial_xi + 2 * i), et1 = __ldg(rules.trial_xi + 2 * i + 1);
-    const double w = __ldg(rules.w + i);
-    double r2 = 0.0;
-    for (int d = 0; d < 3; ++d) {
-      const double dd = (v0x[d] + xi0 * t0x[d] + xi1 * t1x[d]) - (v0y[d] + et0 * t0y[d] + et1 * t1y[d]);
-      r2 += dd * dd;
-    }
-    const double rinv = rsqrt_refined(r2);
-    double sn, cs;
-    if (small_phase)
-      sincos_taylor(k * r2 * rinv, sn, cs);
-    else
-      sincos_cw(k * r2 * rinv, sn, cs);
-    sr = fma(w * rinv, cs, sr);
-    si = fma(w * rinv, sn, si);
-  }
-  for (int s = 16; s > 0; s >>= 1) {
-    sr += __shfl_xor_sync(0xffffffffu, sr, s);
-    si += __shfl_xor_sync(0xffffffffu, si, s);
-  }
-  const double sc = T.G(fJdet, it) * S.G(fJdet, js) * kInv4Pi;
-  re = sr * sc;
-  im = si * sc;
-}
+// One persistent launch for the far pairs: every CTA repeatedly takes the next work item
+// (mesh, chunk of wavenumbers, super-tile pair) from a global counter (items of the
+// largest mesh first), stages the tiles once, and for each wavenumber of its chunk writes
+// the far-pair entries of its 32 x 32 blocks in FP32 (block_fp32), complex64.  The pairs
+// the mesh's near field marks (centroid distance below twice the larger diameter, or a
+// shared vertex: the same masks as the one-off mixed assembly) are left to two FP64
+// launches that run beside it (forked in the same captured graph): near pairs by the
+// 6-point rule with the pair-referenced phase, vertex-sharing pairs by their Duffy rules.
+// The single layer is symmetric on one mesh, so only tile pairs (test tile >= trial tile)
+// are items: an off-diagonal block is also written transposed (through shared memory,
+// coalesced).  No two launches or items write the same entry, so nothing orders them;
+// the only shared state is the item counter (reset before every launch).
 
 // TS: tile shape of a work item, TS x TS tiles of 32 cells on each side (a super-tile
 // pair: 1 x 1 or 2 x 2 tile pairs staged together); MINB: CTAs per SM the register
-// allocation must allow (4: up to 128 registers, 6: up to 80).
+// allocation must allow (4: up to 128 registers, 6: up to 80).  Far pairs only: the pairs
+// marked in the mesh's near-field masks (near or vertex-sharing) are written by
+// sweep_near_fp64 / sweep_duffy_fp64.
 template <int TS, int MINB>
 __global__ void __launch_bounds__(kThreads, MINB)
-    sweep_sl_dp0(SweepArgs a, RegularRule rule, SingularRules rules) {
+    sweep_sl_dp0(SweepArgs a, RegularRule rule) {
   const int Q = 6;
   extern __shared__ __align__(16) unsigned char smem[];
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem);  // completion of the tile copies
   unsigned char* cursor = smem + 16;
   Tile Tt[TS], St[TS];
 #pragma unroll
-  for (int i = 0; i < TS; ++i) Tt[i] = carve_tile(cursor, Q, true, 1);
+  for (int i = 0; i < TS; ++i) Tt[i] = carve_tile(cursor, Q, true, 1, false);
 #pragma unroll
-  for (int i = 0; i < TS; ++i) St[i] = carve_tile(cursor, Q, true, 1);
-  unsigned short* nearq = reinterpret_cast<unsigned short*>(cursor);
-  unsigned short* adjq = nearq + kTile * kTile;
-  unsigned char* adjc = reinterpret_cast<unsigned char*>(adjq + kTile * kTile);
-  int* counts = reinterpret_cast<int*>(adjc + kTile * kTile);  // near, adjacent
-  long long* s_item = reinterpret_cast<long long*>(counts + 2);
-  float2* mir = reinterpret_cast<float2*>(s_item + 1);  // [js * (kTile + 1) + it]
+  for (int i = 0; i < TS; ++i) St[i] = carve_tile(cursor, Q, true, 1, false);
+  long long* s_item = reinterpret_cast<long long*>(cursor);
+  float2* mir = reinterpret_cast<float2*>(s_item + 2);  // [js * (kTile + 1) + it]
   unsigned* skip = reinterpret_cast<unsigned*>(mir + kTile * (kTile + 1));  // [it]: bit js
   const int it = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) mbar_init(mbar, 1);
@@ -1126,20 +1076,22 @@ __global__ void __launch_bounds__(kThreads, MINB)
     int TT, ST;
     lower_tile_pair(local % npairs, nsup, 0, nsup, TT, ST);
     const int nc = M.cells.ncells;
-    // every tile of the two super-tiles by bulk (TMA) copies on the mbarrier: rows of 32
-    // cells of the padded grid arrays; the previous item's reads of the tiles ended at
-    // the barriers that closed it
+    // every tile of the two super-tiles by bulk (TMA) copies on the mbarrier (no FP64
+    // points: the far pairs use the FP32 offsets); the previous item's reads of the tiles
+    // ended at the barriers that closed it
     if (threadIdx.x == 0) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       unsigned bytes = 0;
       for (int i = 0; i < TS; ++i) {
-        if (TS * TT + i < M.ntiles) bytes += bulk_tile_bytes(Q, true, true);
-        if (TS * ST + i < M.ntiles) bytes += bulk_tile_bytes(Q, true, true);
+        if (TS * TT + i < M.ntiles) bytes += bulk_tile_bytes(Q, true, false);
+        if (TS * ST + i < M.ntiles) bytes += bulk_tile_bytes(Q, true, false);
       }
       mbar_expect_tx(mbar, bytes);
       for (int i = 0; i < TS; ++i) {
-        if (TS * TT + i < M.ntiles) stage_tile_bulk(Tt[i], M.cells, (TS * TT + i) * kTile, Q, true, mbar, true);
-        if (TS * ST + i < M.ntiles) stage_tile_bulk(St[i], M.cells, (TS * ST + i) * kTile, Q, true, mbar, true);
+        if (TS * TT + i < M.ntiles)
+          stage_tile_bulk(Tt[i], M.cells, (TS * TT + i) * kTile, Q, true, mbar, false);
+        if (TS * ST + i < M.ntiles)
+          stage_tile_bulk(St[i], M.cells, (TS * ST + i) * kTile, Q, true, mbar, false);
       }
     }
     const bool staged = mbar_wait_bounded(mbar, phase);
@@ -1161,31 +1113,12 @@ __global__ void __launch_bounds__(kThreads, MINB)
       const bool mirror = tt > st;
       const int ti0 = tt * kTile, sj0 = st * kTile;
       const int nti = min(kTile, nc - ti0), nsj = min(kTile, nc - sj0);
-      if (threadIdx.x == 0) counts[0] = counts[1] = 0;
-      if (threadIdx.x < kTile) skip[threadIdx.x] = 0u;
+      // the near and vertex-sharing pairs of this tile pair (the relation is symmetric, so
+      // the same bits mark the transposed block)
+      const int moff = __ldg(M.tile_mask + static_cast<int64_t>(tt) * M.ntiles + st);
+      if (threadIdx.x < kTile)
+        skip[threadIdx.x] = moff >= 0 ? __ldg(M.masks + static_cast<int64_t>(moff) * kTile + threadIdx.x) : 0u;
       __syncthreads();
-      // classify the tile pair once: vertex-sharing and near pairs are queued, and marked
-      // in the test cell's skip word for the far-pair loop of every wavenumber
-      if (it < nti) {
-        const int av[3] = {T.vid[it], T.vid[kTile + it], T.vid[2 * kTile + it]};
-        unsigned bits = 0u;
-        for (int js = warp; js < nsj; js += kWarps) {
-          const int bv[3] = {S.vid[js], S.vid[kTile + js], S.vid[2 * kTile + js]};
-          if (share_vertex(av[0], av[1], av[2], bv[0], bv[1], bv[2])) {
-            const int slot = atomicAdd(counts + 1, 1);
-            adjq[slot] = static_cast<unsigned short>(it | (js << 8));
-            adjc[slot] = static_cast<unsigned char>(adjacency_config(av, bv, ti0 + it == sj0 + js));
-            bits |= 1u << js;
-          } else if (near_pair(T, it, S, js)) {
-            const int slot = atomicAdd(counts, 1);
-            nearq[slot] = static_cast<unsigned short>(it | (js << 8));
-            bits |= 1u << js;
-          }
-        }
-        if (bits) atomicOr(skip + it, bits);
-      }
-      __syncthreads();
-      const int nnear = counts[0], nadj = counts[1];
       const unsigned skip_it = it < nti ? skip[it] : ~0u;
       const int k0 = kc * a.kchunk, k1 = min(a.nk, k0 + a.kchunk);
       for (int kk = k0; kk < k1; ++kk) {
@@ -1201,48 +1134,151 @@ __global__ void __launch_bounds__(kThreads, MINB)
             if (mirror) mir[js * (kTile + 1) + it] = v;
           }
         }
-        for (int e = threadIdx.x; e < nnear; e += kThreads) {
-          const int pi = nearq[e] & 0xff, pj = nearq[e] >> 8;
-          double ore[1][1], oim[1][1];
-          // FP64 near pair: phase referenced to the pair when k (rad_x + rad_y) bounds it,
-          // else the in-tree reduced sincos
-          if (k * (T.G(fRad, pi) + S.G(fRad, pj)) <= static_cast<double>(kSmallPhaseMax))
-            block_fp64<6, kHelmholtz, kSL, 1, 1, false, kF64Referenced>(T, pi, S, pj, rule, k, ore, oim);
-          else
-            block_fp64<6, kHelmholtz, kSL, 1, 1, false, kF64Reduced>(T, pi, S, pj, rule, k, ore, oim);
-          const float2 v = make_float2(static_cast<float>(ore[0][0]), static_cast<float>(oim[0][0]));
-          out[static_cast<long long>(sj0 + pj) * nc + ti0 + pi] = v;
-          if (mirror) mir[pj * (kTile + 1) + pi] = v;
-        }
-        for (int e = warp; e < nadj; e += kWarps) {
-          const int pi = adjq[e] & 0xff, pj = adjq[e] >> 8;
-          double re, im;
-          duffy_sl_dp0_warp(T, pi, S, pj, adjc[e], rules, k, re, im);
-          if (it == 0)
-            out[static_cast<long long>(sj0 + pj) * nc + ti0 + pi] =
-                make_float2(static_cast<float>(re), static_cast<float>(im));
-          if (mirror) {
-            // the transposed pair: trial cell pj as the test cell, its own configuration
-            const int av[3] = {S.vid[pj], S.vid[kTile + pj], S.vid[2 * kTile + pj]};
-            const int bv[3] = {T.vid[pi], T.vid[kTile + pi], T.vid[2 * kTile + pi]};
-            duffy_sl_dp0_warp(S, pj, T, pi, adjacency_config(av, bv, false), rules, k, re, im);
-            if (it == 0)
-              mir[pj * (kTile + 1) + pi] = make_float2(static_cast<float>(re), static_cast<float>(im));
-          }
-        }
         if (mirror) {
           // the transposed block, entry (row sj0 + j, column ti0 + i), j fastest: coalesced
           __syncthreads();
           for (int idx = threadIdx.x; idx < kTile * kTile; idx += kThreads) {
             const int i = idx / kTile, j = idx % kTile;
-            if (i < nti && j < nsj)
+            if (i < nti && j < nsj && !((skip[i] >> j) & 1u))
               out[static_cast<long long>(ti0 + i) * nc + sj0 + j] = mir[j * (kTile + 1) + i];
           }
           __syncthreads();  // mir is reused by the next wavenumber
         }
       }
-      __syncthreads();  // the queues and skip words are reused by the next tile pair
+      __syncthreads();  // the skip words are reused by the next tile pair
     }
+  }
+}
+
+// Single-layer DP0 entry of one cell pair (test i, trial j) by the 6-point rule in FP64,
+// points and geometry from the grid arrays: phase referenced to the pair when
+// k (rad_i + rad_j) <= 0.8, else sincos_cw.
+__device__ double2 sl_dp0_pair_fp64(const CellSet& cs, int i, int j, const RegularRule& rule,
+                                    double k) {
+  const int64_t S = cs.stride;
+  const double dcx = g(cs.geom, kCx, cs.stride, i) - g(cs.geom, kCx, cs.stride, j);
+  const double dcy = g(cs.geom, kCy, cs.stride, i) - g(cs.geom, kCy, cs.stride, j);
+  const double dcz = g(cs.geom, kCz, cs.stride, i) - g(cs.geom, kCz, cs.stride, j);
+  const bool ref = k * (g(cs.geom, kRad, cs.stride, i) + g(cs.geom, kRad, cs.stride, j)) <=
+                   static_cast<double>(kSmallPhaseMax);
+  double kr0 = 0.0, pc = 1.0, ps = 0.0;
+  if (ref) {
+    const double r0sq = dcx * dcx + dcy * dcy + dcz * dcz;
+    kr0 = k * (r0sq * rsqrt_refined(r0sq));
+    sincos_cw(kr0, ps, pc);
+  }
+  double yq[6][3];
+#pragma unroll
+  for (int q = 0; q < 6; ++q)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) yq[q][d] = __ldg(cs.qpts + (q * 3 + d) * S + j);
+  double re = 0.0, im = 0.0;
+#pragma unroll 1
+  for (int p = 0; p < 6; ++p) {
+    const double x0 = __ldg(cs.qpts + (p * 3) * S + i), x1 = __ldg(cs.qpts + (p * 3 + 1) * S + i),
+                 x2 = __ldg(cs.qpts + (p * 3 + 2) * S + i);
+    double ur = 0.0, ui = 0.0;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const double dx = x0 - yq[q][0], dy = x1 - yq[q][1], dz = x2 - yq[q][2];
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      const double rinv = rsqrt_refined(r2);
+      const double r = r2 * rinv;
+      double sn, cs_;
+      if (ref)
+        sincos_small(fma(k, r, -kr0), sn, cs_);
+      else
+        sincos_cw(k * r, sn, cs_);
+      const double f = rule.w[q] * rinv;
+      ur = fma(f, cs_, ur);
+      ui = fma(f, sn, ui);
+    }
+    re = fma(rule.w[p], ur, re);
+    im = fma(rule.w[p], ui, im);
+  }
+  const double sc = g(cs.geom, kJdet, cs.stride, i) * g(cs.geom, kJdet, cs.stride, j) * kInv4Pi;
+  return make_double2((re * pc - im * ps) * sc, (re * ps + im * pc) * sc);
+}
+
+// The near pairs (no shared vertex) of every mesh and wavenumber: one thread per (pair,
+// wavenumber), wavenumber fastest.
+__global__ void __launch_bounds__(kThreads)
+    sweep_near_fp64(SweepArgs a, RegularRule rule) {
+  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= a.near_begin[a.nmesh]) return;
+  int m = 0;
+  while (m + 1 < a.nmesh && t >= a.near_begin[m + 1]) ++m;
+  const SweepMesh& M = a.mesh[m];
+  const long long local = t - a.near_begin[m];
+  const int e = static_cast<int>(local / a.nk), kk = static_cast<int>(local % a.nk);
+  const int2 pr = __ldg(M.near_pairs + e);
+  const double2 v = sl_dp0_pair_fp64(M.cells, pr.x, pr.y, rule, a.ks[kk]);
+  const int nc = M.cells.ncells;
+  M.out[static_cast<long long>(kk) * nc * nc + static_cast<long long>(pr.y) * nc + pr.x] =
+      make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+}
+
+// The vertex-sharing pairs of every mesh and wavenumber by their Duffy rules: one warp
+// per (pair, wavenumber), wavenumber fastest; lanes over the rule's points.
+__global__ void __launch_bounds__(kThreads)
+    sweep_duffy_fp64(SweepArgs a, SingularRules rules) {
+  const long long w = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= a.sing_begin[a.nmesh]) return;  // warp-uniform
+  int m = 0;
+  while (m + 1 < a.nmesh && w >= a.sing_begin[m + 1]) ++m;
+  const SweepMesh& M = a.mesh[m];
+  const long long local = w - a.sing_begin[m];
+  const int e = static_cast<int>(local / a.nk), kk = static_cast<int>(local % a.nk);
+  const double k = a.ks[kk];
+  const CellSet& cs = M.cells;
+  const int tc = __ldg(M.sing.test_cell + e), sc = __ldg(M.sing.trial_cell + e);
+  const int cfg = __ldg(M.sing.config + e);
+  double t0x[3], t1x[3], t0y[3], t1y[3], dv[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    t0x[d] = g(cs.geom, kT0x + d, cs.stride, tc);
+    t1x[d] = g(cs.geom, kT1x + d, cs.stride, tc);
+    t0y[d] = g(cs.geom, kT0x + d, cs.stride, sc);
+    t1y[d] = g(cs.geom, kT1x + d, cs.stride, sc);
+    dv[d] = g(cs.geom, kV0x + d, cs.stride, tc) - g(cs.geom, kV0x + d, cs.stride, sc);
+  }
+  const int off = __ldg(rules.offset + cfg), npts = __ldg(rules.offset + cfg + 1) - off;
+  // |k r| <= k (diam_x + diam_y): no reduction of the phase when that is below pi/4
+  const bool small_phase =
+      k * (g(cs.geom, kDiam, cs.stride, tc) + g(cs.geom, kDiam, cs.stride, sc)) <= 0.78;
+  const double2* txi = reinterpret_cast<const double2*>(rules.test_xi);
+  const double2* sxi = reinterpret_cast<const double2*>(rules.trial_xi);
+  double sr = 0.0, si = 0.0;
+  for (int ii = lane; ii < npts; ii += 32) {
+    const int i = off + ii;
+    const double2 xi = __ldg(txi + i), et = __ldg(sxi + i);
+    const double wt = __ldg(rules.w + i);
+    double r2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double dd = fma(xi.x, t0x[d], fma(xi.y, t1x[d], fma(-et.x, t0y[d], fma(-et.y, t1y[d], dv[d]))));
+      r2 = fma(dd, dd, r2);
+    }
+    const double rinv = rsqrt_refined(r2);
+    double sn, cs_;
+    if (small_phase)
+      sincos_taylor(k * r2 * rinv, sn, cs_);
+    else
+      sincos_cw(k * r2 * rinv, sn, cs_);
+    sr = fma(wt * rinv, cs_, sr);
+    si = fma(wt * rinv, sn, si);
+  }
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    sr += __shfl_xor_sync(0xffffffffu, sr, s);
+    si += __shfl_xor_sync(0xffffffffu, si, s);
+  }
+  if (lane == 0) {
+    const double scl = g(cs.geom, kJdet, cs.stride, tc) * g(cs.geom, kJdet, cs.stride, sc) * kInv4Pi;
+    const int nc = cs.ncells;
+    M.out[static_cast<long long>(kk) * nc * nc + static_cast<long long>(sc) * nc + tc] =
+        make_float2(static_cast<float>(sr * scl), static_cast<float>(si * scl));
   }
 }
 
@@ -1429,26 +1465,26 @@ cudaError_t take_stage_timeouts(unsigned* count) {
 }
 
 size_t sweep_smem_bytes(int ts) {
-  size_t b = 0;
-  for (int t = 0; t < 2 * ts; ++t) {
-    b += sizeof(double) * tile_doubles(6) + sizeof(float) * tile_floats(6, true) +
+  size_t b = 16;  // the mbarrier
+  for (int t = 0; t < 2 * ts; ++t) {  // tiles without FP64 points
+    b += sizeof(double) * tile_doubles(6, false) + sizeof(float) * tile_floats(6, true) +
          sizeof(int) * tile_ints(1);
     b = (b + 15) & ~size_t(15);
   }
-  return 16 + b + 2 * sizeof(unsigned short) * kTile * kTile + kTile * kTile + 2 * sizeof(int) +
-         sizeof(long long) + sizeof(float2) * kTile * (kTile + 1) + sizeof(unsigned) * kTile + 32;
+  return b + 2 * sizeof(long long) + sizeof(float2) * kTile * (kTile + 1) +
+         sizeof(unsigned) * kTile + 32;
 }
 
 namespace {
 template <int TS, int MINB>
-cudaError_t launch_sweep_shape(const SweepArgs& args, const RegularRule& rule,
-                               const SingularRules& rules, int blocks, cudaStream_t stream) {
+cudaError_t launch_sweep_shape(const SweepArgs& args, const RegularRule& rule, int blocks,
+                               cudaStream_t stream) {
   const size_t smem = sweep_smem_bytes(TS);
   auto fn = sweep_sl_dp0<TS, MINB>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  fn<<<blocks, kThreads, smem, stream>>>(args, rule, rules);
+  fn<<<blocks, kThreads, smem, stream>>>(args, rule);
   return cudaGetLastError();
 }
 }  // namespace
@@ -1456,15 +1492,36 @@ cudaError_t launch_sweep_shape(const SweepArgs& args, const RegularRule& rule,
 cudaError_t launch_sweep_sl(const SweepArgs& args, const RegularRule& rule,
                             const SingularRules& rules, int blocks_per_sm, int sms,
                             cudaStream_t stream) {
+  (void)rules;
   if (rule.npts != 6) return cudaErrorInvalidValue;
   if (args.tile_shape != 1 && args.tile_shape != 2) return cudaErrorInvalidValue;
   const int blocks = blocks_per_sm * sms;
   // the register cap follows the CTAs per SM asked for (at most 6)
   if (args.tile_shape == 1)
-    return blocks_per_sm > 4 ? launch_sweep_shape<1, 6>(args, rule, rules, blocks, stream)
-                             : launch_sweep_shape<1, 4>(args, rule, rules, blocks, stream);
-  return blocks_per_sm > 4 ? launch_sweep_shape<2, 6>(args, rule, rules, blocks, stream)
-                           : launch_sweep_shape<2, 4>(args, rule, rules, blocks, stream);
+    return blocks_per_sm > 4 ? launch_sweep_shape<1, 6>(args, rule, blocks, stream)
+                             : launch_sweep_shape<1, 4>(args, rule, blocks, stream);
+  return blocks_per_sm > 4 ? launch_sweep_shape<2, 6>(args, rule, blocks, stream)
+                           : launch_sweep_shape<2, 4>(args, rule, blocks, stream);
+}
+
+cudaError_t launch_sweep_near_singular(const SweepArgs& args, const RegularRule& rule,
+                                       const SingularRules& rules, cudaStream_t stream) {
+  if (rule.npts != 6) return cudaErrorInvalidValue;
+  const long long nn = args.near_begin[args.nmesh], ns = args.sing_begin[args.nmesh];
+  if (nn > 0) {
+    const long long blocks = (nn + kThreads - 1) / kThreads;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+    sweep_near_fp64<<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(args, rule);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (ns > 0) {
+    const long long blocks = (ns * 32 + kThreads - 1) / kThreads;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+    sweep_duffy_fp64<<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(args, rules);
+    return cudaGetLastError();
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_regular_dp0(const CellSet& test, const CellSet& trial,

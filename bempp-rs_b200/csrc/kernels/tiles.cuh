@@ -229,6 +229,18 @@ __device__ __forceinline__ float2 rsqrt_approx2(float2 x) {
 __device__ __forceinline__ float2 rcp_approx2(float2 x) {
   return make_float2(rcp_approx(x.x), rcp_approx(x.y));
 }
+// cos(t), sin(t) for |t| <= 1.6 on two arguments: cos of degree 10 and sin of degree 9 in
+// t, discrete minimax fits (fit_phase_polys.py 1.6 5 4; errors 3.0e-10 and 5.7e-9, below
+// FP32 rounding), for pairs whose phases exceed the range of poly_cos_sin2 by at most 2x.
+__device__ __forceinline__ void poly_cos_sin_wide2(float2 t, float2& c, float2& s) {
+  const float2 z = fmul2(t, t);
+  c = ffma2(z, ffma2(z, ffma2(z, ffma2(z, ffma2(z, f2(-2.602302326e-7f), f2(2.475890560e-5f)),
+                                       f2(-1.388834758e-3f)), f2(4.166663666e-2f)),
+                     f2(-4.999999946e-1f)), f2(1.0f));
+  s = fmul2(t, ffma2(z, ffma2(z, ffma2(z, ffma2(z, f2(2.594375954e-6f), f2(-1.980401633e-4f)),
+                                       f2(8.332980908e-3f)), f2(-1.666665560e-1f)), f2(1.0f)));
+}
+
 // poly_cos_sin on two arguments
 __device__ __forceinline__ void poly_cos_sin2(float2 t, float2& c, float2& s) {
   const float2 z = fmul2(t, t);
