@@ -334,6 +334,9 @@ struct FarPair {
   float m2dx, m2dy, m2dz;   // -2 dc, dc = c_x - c_y in FP32
   float fa0, fa1, fa2;      // normal-derivative factors in tangent coordinates
   float r0f, r0sq, kf;      // reference distance (Helmholtz), |dc|^2, wavenumber
+  // Helmholtz, packed loop: s is carried as s' = ks s (ks = k, or 1e-20 when k = 0), so
+  // that k (r - r0) = s' / (r + r0) needs no multiply by k: ks times -2 dc, and 1 / ks
+  float ksm2dx, ksm2dy, ksm2dz, ks, ks_inv;
   float wq[kCap];           // ADL: trial weights times the normal-derivative factor
 };
 
@@ -454,15 +457,19 @@ __device__ __forceinline__ void far_sums_x2(const Tile& T, int it, const Tile& S
   constexpr bool kKahan = NBT == 1 && NBS == 1;
   float cmp_re = 0.f, cmp_im = 0.f;
   const float2 r0sq2 = f2(fp.r0sq), r0f2 = f2(fp.r0f), kf2 = f2(fp.kf), nkf2 = f2(-fp.kf);
+  const float2 ks2 = f2(fp.ks), ksinv2 = f2(fp.ks_inv);
 #pragma unroll 1
   for (int p = 0; p < QT; ++p) {
     const float4 a = T.R4(p, it);
     const float apf = OP == kDL ? fmaf(rule.uf[p], fp.fa1, fmaf(rule.vf[p], fp.fa2, fp.fa0)) : 1.f;
-    // s_pq = A_p + |y_q|^2 + w_p . y_q; Laplace adds |dc|^2 so that it is r^2 itself
-    const float2 wx = f2(fmaf(-2.f, a.x, fp.m2dx)), wy = f2(fmaf(-2.f, a.y, fp.m2dy)),
-                 wz = f2(fmaf(-2.f, a.z, fp.m2dz));
-    const float2 Ap = f2(fmaf(-a.x, fp.m2dx, fmaf(-a.y, fp.m2dy, fmaf(-a.z, fp.m2dz,
-                                                                     a.w + (kC ? 0.f : fp.r0sq)))));
+    // s_pq = A_p + |y_q|^2 + w_p . y_q; Laplace adds |dc|^2 so that it is r^2 itself;
+    // Helmholtz carries s' = ks s (every term of s times ks)
+    const float m2 = kC ? -2.f * fp.ks : -2.f;
+    const float mx = kC ? fp.ksm2dx : fp.m2dx, my = kC ? fp.ksm2dy : fp.m2dy,
+                mz = kC ? fp.ksm2dz : fp.m2dz;
+    const float2 wx = f2(fmaf(m2, a.x, mx)), wy = f2(fmaf(m2, a.y, my)), wz = f2(fmaf(m2, a.z, mz));
+    const float2 Ap = f2(fmaf(-a.x, mx, fmaf(-a.y, my, fmaf(-a.z, mz,
+                                                        kC ? fp.ks * a.w : a.w + fp.r0sq))));
     float2 u_re[NBS], u_im[NBS], g_re = f2(0.f), g_im = f2(0.f);
 #pragma unroll
     for (int b = 0; b < NBS; ++b) u_re[b] = u_im[b] = f2(0.f);
@@ -473,15 +480,18 @@ __device__ __forceinline__ void far_sums_x2(const Tile& T, int it, const Tile& S
                                    : make_float2(fp.wq[2 * j], fp.wq[2 * j + 1]);
       const float2 s = ffma2(wx, make_float2(A.x, A.y),
                              ffma2(wy, make_float2(A.z, A.w),
-                                   ffma2(wz, make_float2(B.x, B.y), fadd2(Ap, make_float2(B.z, B.w)))));
+                                   ffma2(wz, make_float2(B.x, B.y),
+                                         kC ? ffma2(ks2, make_float2(B.z, B.w), Ap)
+                                            : fadd2(Ap, make_float2(B.z, B.w)))));
       float2 f, c = f2(1.f), sn = f2(0.f);  // kernel value = f (c + i sn)
       if (!kC) {
         const float2 rinv = rsqrt_approx2(s);  // s is r^2 here
         f = (OP == kSL || OP == kHS) ? fmul2(wq, rinv) : fmul2(wq, fmul2(fmul2(rinv, rinv), rinv));
       } else {
-        const float2 r2 = fadd2(r0sq2, s);
+        const float2 r2 = ffma2(s, ksinv2, r0sq2);  // s is s' = ks s here
         const float2 rinv = rsqrt_approx2(r2);
-        const float2 t = fmul2(fmul2(kf2, s), rcp_approx2(ffma2(r2, rinv, r0f2)));  // k (r - r0)
+        // k (r - r0) = s' / (r + r0) (exactly when ks = k; 1e-20 s / (r + r0) when k = 0)
+        const float2 t = fmul2(s, rcp_approx2(ffma2(r2, rinv, r0f2)));
         float2 cs, ss;
         if (kWide)
           poly_cos_sin_wide2(t, cs, ss);
@@ -595,6 +605,11 @@ __device__ __forceinline__ void block_fp32(const Tile& T, int it, const Tile& S,
     fp.r0f = static_cast<float>(r0);
     fp.r0sq = static_cast<float>(r0sq);
     fp.kf = static_cast<float>(k);
+    fp.ks = fp.kf != 0.f ? fp.kf : 1e-20f;
+    fp.ks_inv = 1.f / fp.ks;
+    fp.ksm2dx = fp.ks * fp.m2dx;
+    fp.ksm2dy = fp.ks * fp.m2dy;
+    fp.ksm2dz = fp.ks * fp.m2dz;
     phase_cos_sin(k * r0, ph_c, ph_s);
     // warp-uniform choice, so that a warp never runs two variants
     if (PH == kPhaseRuntime) {

@@ -229,14 +229,13 @@ __device__ __forceinline__ float2 rsqrt_approx2(float2 x) {
 __device__ __forceinline__ float2 rcp_approx2(float2 x) {
   return make_float2(rcp_approx(x.x), rcp_approx(x.y));
 }
-// cos(t), sin(t) for |t| <= 1.6 on two arguments: cos of degree 10 and sin of degree 9 in
-// t, discrete minimax fits (fit_phase_polys.py 1.6 5 4; errors 3.0e-10 and 5.7e-9, below
-// FP32 rounding), for pairs whose phases exceed the range of poly_cos_sin2 by at most 2x.
+// cos(t), sin(t) for |t| <= 1.6 on two arguments: cos of degree 8 and sin of degree 9 in
+// t, discrete minimax fits (fit_phase_polys.py 1.6 4 4; errors 6.3e-8 and 5.7e-9, FP32
+// rounding), for pairs whose phases exceed the range of poly_cos_sin2 by at most 2x.
 __device__ __forceinline__ void poly_cos_sin_wide2(float2 t, float2& c, float2& s) {
   const float2 z = fmul2(t, t);
-  c = ffma2(z, ffma2(z, ffma2(z, ffma2(z, ffma2(z, f2(-2.602302326e-7f), f2(2.475890560e-5f)),
-                                       f2(-1.388834758e-3f)), f2(4.166663666e-2f)),
-                     f2(-4.999999946e-1f)), f2(1.0f));
+  c = ffma2(z, ffma2(z, ffma2(z, ffma2(z, f2(2.313598054e-5f), f2(-1.385346181e-3f)),
+                              f2(4.166368189e-2f)), f2(-4.999992169e-1f)), f2(1.0f));
   s = fmul2(t, ffma2(z, ffma2(z, ffma2(z, ffma2(z, f2(2.594375954e-6f), f2(-1.980401633e-4f)),
                                        f2(8.332980908e-3f)), f2(-1.666665560e-1f)), f2(1.0f)));
 }
@@ -244,8 +243,9 @@ __device__ __forceinline__ void poly_cos_sin_wide2(float2 t, float2& c, float2& 
 // poly_cos_sin on two arguments
 __device__ __forceinline__ void poly_cos_sin2(float2 t, float2& c, float2& s) {
   const float2 z = fmul2(t, t);
-  c = ffma2(z, ffma2(z, ffma2(z, ffma2(z, f2(2.437514408e-5f), f2(-1.388660219e-3f)),
-                              f2(4.166661828e-2f)), f2(-4.999999968e-1f)), f2(1.0f));
+  // cos of degree 6 here (fit_phase_polys.py 0.8 3 3: max error 3.7e-8, FP32 rounding)
+  c = ffma2(z, ffma2(z, ffma2(z, f2(-1.358700830e-3f), f2(4.165550692e-2f)),
+                     f2(-4.999988255e-1f)), f2(1.0f));
   s = fmul2(t, ffma2(z, ffma2(z, ffma2(z, f2(-1.948277516e-4f), f2(8.331875683e-3f)),
                               f2(-1.666664881e-1f)), f2(1.0f)));
 }
