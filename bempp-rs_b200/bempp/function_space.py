@@ -130,14 +130,14 @@ class FunctionSpace(object):
 
     def cell_colouring(self) -> typing.Dict[ReferenceCellType, typing.List[typing.List[int]]]:
         """Cells grouped so that no two cells of a group share a DOF entity (the
-        reference's FunctionSpace::cell_colouring): {Triangle: [cells of colour 0, ...]}."""
+        reference's FunctionSpace::cell_colouring): {cell type: [cells of colour 0, ...]}."""
         ncells = len(self._grid.cells)
         colours = np.zeros(ncells, dtype=np.uintp)
         n = _lib.space_cell_colouring(self._rs_space, _ffi.cast("size_t*", colours.ctypes.data))
         groups: typing.List[typing.List[int]] = [[] for _ in range(n)]
         for cell, c in enumerate(colours.tolist()):
             groups[c].append(cell)
-        return {ReferenceCellType.Triangle: groups}
+        return {self._grid.cell_type: groups}
 
     def global_dof_index(self, local_dof_index: int) -> int:
         """Global number of a local DOF (the identity for serial spaces)."""
@@ -201,7 +201,7 @@ def recreate_grid(grid: Grid):
     are the ones the library uses; otherwise points and cells suffice."""
     points = np.ascontiguousarray(grid.points, dtype=np.float64)
     cells = np.ascontiguousarray(grid.cells, dtype=np.uintp)
-    if getattr(grid, "cell_vertices", None) is None:
+    if getattr(grid, "cell_vertices", None) is None and cells.shape[1] == 3:
         g = _lib.bempp_grid_from_points_cells(
             _ffi.cast("void*", points.ctypes.data), len(points), _lib.DType_F64,
             _ffi.cast("size_t*", cells.ctypes.data), len(cells))
@@ -230,16 +230,17 @@ def _ndgrid_create(grid: Grid, points, cells):
     d1 = _ffi.new("size_t*[2]", [ptr(ev), _ffi.NULL])
     d2 = _ffi.new("size_t*[3]", [ptr(cv), ptr(ce), _ffi.NULL])
     down = _ffi.new("size_t**[3]", [d0, d1, d2])
+    nvc = cells.shape[1]  # 3 (triangles) or 4 (quadrilaterals)
     s0 = _ffi.new("size_t[1]", [1])
     s1 = _ffi.new("size_t[2]", [2, 1])
-    s2 = _ffi.new("size_t[3]", [3, 3, 1])
+    s2 = _ffi.new("size_t[3]", [nvc, nvc, 1])
     shape0 = _ffi.new("size_t*[3]", [s0, s1, s2])
-    types = _ffi.new("ReferenceCellType[3]", [_lib.ReferenceCellType_Point,
-                                              _lib.ReferenceCellType_Interval,
-                                              _lib.ReferenceCellType_Triangle])
+    types = _ffi.new("ReferenceCellType[3]", [
+        _lib.ReferenceCellType_Point, _lib.ReferenceCellType_Interval,
+        _lib.ReferenceCellType_Quadrilateral if nvc == 4 else _lib.ReferenceCellType_Triangle])
     g = _lib.single_element_grid_borrowed_create_bempp(
         2, _ffi.NULL, _ffi.NULL, types, ptr(counts), down, shape0, _ffi.NULL, _ffi.NULL,
         _ffi.cast("void*", points.ctypes.data), 3, len(points), _lib.DType_F64, ptr(cells),
-        3, len(cells), 1)
+        nvc, len(cells), 1)
     del keep
     return g

@@ -88,3 +88,51 @@ def ellipsoidal_stretch(points, seed: int, low: float = 0.8, high: float = 1.2):
     rng = np.random.default_rng(seed)
     axes = rng.uniform(low, high, 3)
     return points * axes[None, :]
+
+
+def screen_quads(n: int = 3):
+    """The flat n x n quadrilateral grid of the unit square in the plane z = 0 (points
+    (i/n, j/n, 0), cells [k, k+1, k+n+1, k+n+2] with k = (n+1) j + i: ndelement's vertex
+    order), the grid of the reference's quadrilateral assembly cases
+    (src/boundary_assemblers.rs:840-865 builds it with n = 3)."""
+    pts = np.array([[i / n, j / n, 0.0] for j in range(n + 1) for i in range(n + 1)])
+    cells = np.array([[(n + 1) * j + i, (n + 1) * j + i + 1, (n + 1) * (j + 1) + i,
+                       (n + 1) * (j + 1) + i + 1] for j in range(n) for i in range(n)],
+                     dtype=np.int64)
+    return pts, cells
+
+
+def cube_quads(n: int):
+    """Surface of the cube [-1, 1]^3 as 6 n^2 quadrilaterals with shared vertices, in
+    ndelement's vertex order (v0, v1 along the first face axis, v2 along the second, v3
+    opposite v0) and outward-oriented (first axis x second axis = outward normal)."""
+    faces = []  # (origin corner, first axis, second axis), first x second = outward
+    for ax in range(3):
+        for sgn in (-1.0, 1.0):
+            u = [(ax + 1) % 3, (ax + 2) % 3]
+            if sgn < 0:
+                u = u[::-1]
+            o = np.full(3, -1.0)
+            o[ax] = sgn
+            faces.append((o, u))
+    index = {}
+    pts = []
+    cells = []
+
+    def point(p):
+        key = tuple(np.round(p, 12))
+        if key not in index:
+            index[key] = len(pts)
+            pts.append(p)
+        return index[key]
+
+    for o, (a, b) in faces:
+        for j in range(n):
+            for i in range(n):
+                def corner(di, dj):
+                    p = o.copy()
+                    p[a] += 2.0 * (i + di) / n
+                    p[b] += 2.0 * (j + dj) / n
+                    return point(p)
+                cells.append([corner(0, 0), corner(1, 0), corner(0, 1), corner(1, 1)])
+    return np.array(pts, dtype=np.float64), np.array(cells, dtype=np.int64)

@@ -561,13 +561,17 @@ DType space_dtype(SpaceT* s) { return s ? s->dtype : DType_F64; }
 
 // ------------------------------------------------------------- grids, elements ---
 static GridT* make_grid(const void* points, size_t npoints, size_t gdim, DType dtype,
-                        const size_t* cells, size_t ncells, size_t points_per_cell) {
+                        const size_t* cells, size_t ncells, size_t points_per_cell,
+                        uint8_t cell_type = kTriangle) {
   GridT* out = nullptr;
   guarded([&] {
     if (npoints > 0) require(points, "points");
     if (ncells > 0) require(cells, "cells");
     if (gdim != 3) throw Error(kUnsupported, "only surface grids in 3D are supported");
-    if (points_per_cell < 3) throw Error(kInvalidArgument, "cells need three vertices");
+    const int nv = cell_type == kQuadrilateral ? 4 : 3;
+    if (points_per_cell < static_cast<size_t>(nv))
+      throw Error(kInvalidArgument, nv == 4 ? "quadrilateral cells need four vertices"
+                                            : "cells need three vertices");
     if (dtype != DType_F32 && dtype != DType_F64)
       throw Error(kInvalidArgument, "grid points must be F32 or F64");
     auto* g = new GridT();
@@ -575,19 +579,20 @@ static GridT* make_grid(const void* points, size_t npoints, size_t gdim, DType d
     g->dtype = dtype;
     g->npoints = static_cast<int64_t>(npoints);
     g->ncells = static_cast<int64_t>(ncells);
+    g->cell_type = cell_type;
     g->points.resize(3 * npoints);
     for (size_t i = 0; i < 3 * npoints; ++i)
       g->points[i] = dtype == DType_F64 ? static_cast<const double*>(points)[i]
                                         : static_cast<const float*>(points)[i];
-    g->cells.resize(3 * ncells);
+    g->cells.resize(nv * ncells);
     for (size_t c = 0; c < ncells; ++c)
-      for (int i = 0; i < 3; ++i) {
+      for (int i = 0; i < nv; ++i) {
         size_t v = cells[c * points_per_cell + i];
         if (v >= npoints) {
           delete g;
           throw Error(kInvalidArgument, "cell vertex index out of range");
         }
-        g->cells[3 * c + i] = static_cast<int>(v);
+        g->cells[nv * c + i] = static_cast<int>(v);
       }
     out = g;
   });
@@ -598,12 +603,14 @@ static GridT* make_grid(const void* points, size_t npoints, size_t gdim, DType d
 // SingleElementGrid exposes it: per dimension d = 0..tdim, entity_counts[d] entities;
 // downward_connectivity[d][sd] (sd = 0..d) holds, for each entity of dimension d, its
 // downward_connectivity_shape0[d][sd] sub-entities of dimension sd contiguously (a
-// column-major shape0 x count array).  Used here: cell -> vertex ([2][0], 3 per cell),
-// cell -> edge ([2][1], 3 per cell, local edge i opposite local vertex i) and edge ->
-// vertex ([1][0], 2 per edge).  The topology's vertex ids decide adjacency and vertex
-// DOFs (they may differ from the point indices of `cells`, e.g. when two points at one
-// position are one vertex); the edge numbering is kept.  Entity ids and the upward
-// connectivity carry nothing the assembly needs.
+// column-major shape0 x count array).  Used here: cell -> vertex ([2][0], 3 per triangle,
+// 4 per quadrilateral), and for triangles cell -> edge ([2][1], 3 per cell, local edge i
+// opposite local vertex i) and edge -> vertex ([1][0], 2 per edge).  The topology's
+// vertex ids decide adjacency and vertex DOFs (they may differ from the point indices of
+// `cells`, e.g. when two points at one position are one vertex); the edge numbering is
+// kept.  entity_types[2] (Triangle or Quadrilateral) is the cell type; a quadrilateral's
+// vertices are in the reference square's order (0,0), (1,0), (0,1), (1,1).  Entity ids
+// and the upward connectivity carry nothing the assembly needs.
 GridT* single_element_grid_borrowed_create_bempp(
     size_t tdim, const size_t* id_sizes, const size_t* const* id_pointers,
     const ReferenceCellType* entity_types, const size_t* entity_counts,
@@ -617,15 +624,18 @@ GridT* single_element_grid_borrowed_create_bempp(
   (void)id_pointers;
   (void)upward_connectivity;
   (void)upward_connectivity_lens;
-  if (tdim != 2 || (entity_types && entity_types[2] != ReferenceCellType_Triangle)) {
-    set_last_error("only triangle surface grids are supported");
+  const bool quads = entity_types && entity_types[2] == ReferenceCellType_Quadrilateral;
+  if (tdim != 2 || (entity_types && entity_types[2] != ReferenceCellType_Triangle && !quads)) {
+    set_last_error("only triangle and quadrilateral surface grids are supported");
     return nullptr;
   }
   if (geometry_degree != 1) {
-    set_last_error("only flat (degree-1) cells are supported");
+    set_last_error("only degree-1 (flat triangle, bilinear quadrilateral) cells are supported");
     return nullptr;
   }
-  GridT* g = make_grid(points, npoints, gdim, dtype, cells, ncells, points_per_cell);
+  const size_t nvc = quads ? 4 : 3;  // vertices per cell
+  GridT* g = make_grid(points, npoints, gdim, dtype, cells, ncells, points_per_cell,
+                       quads ? kQuadrilateral : kTriangle);
   if (!g || !downward_connectivity) return g;
   const BemppStatus st = guarded([&] {
     require(entity_counts, "entity_counts");
@@ -644,14 +654,14 @@ GridT* single_element_grid_borrowed_create_bempp(
                                           std::to_string(per) + " entries per entity");
       return require(downward_connectivity[d][sd], "downward connectivity array");
     };
-    const size_t* cv = conn(2, 0, 3);
-    g->topo.resize(3 * ncells);
-    for (size_t i = 0; i < 3 * ncells; ++i) {
+    const size_t* cv = conn(2, 0, nvc);
+    g->topo.resize(nvc * ncells);
+    for (size_t i = 0; i < nvc * ncells; ++i) {
       if (cv[i] >= nv) throw Error(kInvalidArgument, "cell -> vertex index out of range");
       g->topo[i] = static_cast<int>(cv[i]);
     }
     g->nvertices = static_cast<int64_t>(nv);
-    if (ne > 0 && downward_connectivity[2][1] && downward_connectivity[1]) {
+    if (!quads && ne > 0 && downward_connectivity[2][1] && downward_connectivity[1]) {
       const size_t* ce = conn(2, 1, 3);
       const size_t* ev = conn(1, 0, 2);
       g->given_edge_vertices.resize(2 * ne);
@@ -876,6 +886,38 @@ size_t bempp_singular_rule(size_t config, size_t order, double* test_points,
   size_t n = 0;
   guarded([&] {
     DuffyRule r = duffy_rule(static_cast<int>(config), static_cast<int>(order));
+    n = r.w.size();
+    if (test_points) std::memcpy(test_points, r.test_xi.data(), r.test_xi.size() * sizeof(double));
+    if (trial_points)
+      std::memcpy(trial_points, r.trial_xi.data(), r.trial_xi.size() * sizeof(double));
+    if (weights) std::memcpy(weights, r.w.data(), r.w.size() * sizeof(double));
+  });
+  return n;
+}
+
+size_t bempp_quadrilateral_regular_rule(size_t npoints, double* points, double* weights) {
+  size_t n = 0;
+  guarded([&] {
+    const QuadGaussRule r = quad_gauss_rule(npoints);
+    for (int i = 0; i < r.n; ++i)
+      for (int j = 0; j < r.n; ++j) {
+        const int p = i * r.n + j;
+        if (points) {
+          points[2 * p] = r.x[i];
+          points[2 * p + 1] = r.x[j];
+        }
+        if (weights) weights[p] = r.w[i] * r.w[j];
+      }
+    n = static_cast<size_t>(r.n) * r.n;
+  });
+  return n;
+}
+
+size_t bempp_quadrilateral_singular_rule(size_t config, size_t order, double* test_points,
+                                         double* trial_points, double* weights) {
+  size_t n = 0;
+  guarded([&] {
+    DuffyRule r = quad_duffy_rule(static_cast<int>(config), static_cast<int>(order));
     n = r.w.size();
     if (test_points) std::memcpy(test_points, r.test_xi.data(), r.test_xi.size() * sizeof(double));
     if (trial_points)

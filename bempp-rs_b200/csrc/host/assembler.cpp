@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <tuple>
 
 #include "core.h"
 
@@ -58,17 +59,21 @@ struct DeviceRules {
   int total = 0;
 };
 std::mutex g_rules_mu;
-std::map<std::pair<int, int>, std::unique_ptr<DeviceRules>> g_rules;
+std::map<std::tuple<int, int, bool>, std::unique_ptr<DeviceRules>> g_rules;
 
-const DeviceRules& device_rules(int device, int order) {
+// the 28 triangle configurations, or the 49 quadrilateral ones
+const DeviceRules& device_rules(int device, int order, bool quads = false) {
   std::lock_guard<std::mutex> lock(g_rules_mu);
-  auto& slot = g_rules[{device, order}];
+  auto& slot = g_rules[std::make_tuple(device, order, quads)];
   if (!slot) {
     auto r = std::make_unique<DeviceRules>();
     std::vector<int> off{0};
     std::vector<double> txi, sxi, w;
-    for (size_t c = 0; c < singular_configurations().size(); ++c) {
-      DuffyRule d = duffy_rule(static_cast<int>(c), order);
+    const size_t ncfg =
+        quads ? quad_singular_configurations().size() : singular_configurations().size();
+    for (size_t c = 0; c < ncfg; ++c) {
+      DuffyRule d = quads ? quad_duffy_rule(static_cast<int>(c), order)
+                          : duffy_rule(static_cast<int>(c), order);
       txi.insert(txi.end(), d.test_xi.begin(), d.test_xi.end());
       sxi.insert(sxi.end(), d.trial_xi.begin(), d.trial_xi.end());
       w.insert(w.end(), d.w.begin(), d.w.end());
@@ -192,7 +197,32 @@ SpaceTiles space_tiles(const SpaceT& s) {
 
 void check_spaces(const BoundaryAssemblerT& a, const SpaceT& trial, const SpaceT& test) {
   if (!trial.grid || !test.grid) throw Error(kInvalidArgument, "space without grid");
+  if (trial.grid->quads() != test.grid->quads())
+    throw Error(kUnsupported, "a triangle grid and a quadrilateral grid cannot be paired");
   (void)a;
+}
+
+QuadCells quad_cells(const GridT& g) {
+  QuadCells q;
+  q.ncells = static_cast<int>(g.ncells);
+  q.points = g.d_points.as<double>();
+  q.cells = g.d_cells.as<int>();
+  q.vids = g.topo.empty() ? g.d_cells.as<int>() : g.d_topo.as<int>();
+  return q;
+}
+
+// Regular rule and Duffy order of quadrilateral pairs from the options.
+void quad_rules(const Options& o, QuadGaussRule& rule, int& order) {
+  const auto qit = o.regular.find(kQuadrilateral);
+  if (qit == o.regular.end())
+    throw Error(kInvalidArgument, "no regular quadrature degree for quadrilaterals");
+  const auto sit = o.singular.find({kQuadrilateral, kQuadrilateral});
+  if (sit == o.singular.end())
+    throw Error(kInvalidArgument, "no singular quadrature degree for quadrilateral pairs");
+  if (sit->second < 1 || sit->second > 16)
+    throw Error(kUnsupported, "quadrilateral Duffy rules of order 1..16 only");
+  rule = quad_gauss_rule(qit->second);
+  order = static_cast<int>(sit->second);
 }
 
 struct Timer {
@@ -218,6 +248,7 @@ struct Timer {
 }  // namespace
 
 int effective_chunks(const SpaceT& trial, int want) {
+  if (trial.grid->quads()) return 1;  // one launch per part
   const int tiles = static_cast<int>((trial.grid->ncells + 31) / 32);
   return std::max(1, std::min(want, tiles));
 }
@@ -250,9 +281,93 @@ const ColumnRuns& chunk_columns(SpaceT& trial, int nchunks) {
   return slot;
 }
 
+namespace {
+
+// Quadrilateral grids: the regular part (every pair that shares no vertex, Gauss tensor
+// rule on both cells) and the singular part (the 49 Duffy configurations), FP64 whatever
+// the precision option, added into the zeroed output in one chunk.
+void assemble_quad_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d_out,
+                          cudaStream_t stream, const std::function<void(int)>& chunk_done) {
+  const int device = current_device();
+  QuadGaussRule rule;
+  int order;
+  quad_rules(a.options, rule, order);
+  const bool same_grid = trial.grid == test.grid;
+  const int64_t nt = test.ndofs, ns = trial.ndofs;
+  const bool single = a.dtype == 0 || a.dtype == 2;
+  const bool cplx = a.kernel == kHelmholtz;
+  a.launches = 0;
+  ensure_space_device(test, device);
+  ensure_space_device(trial, device);
+  {
+    std::lock_guard<std::mutex> lock(test.grid->mu);
+    ensure_grid_device(*test.grid, device);
+  }
+  {
+    std::lock_guard<std::mutex> lock(trial.grid->mu);
+    ensure_grid_device(*trial.grid, device);
+  }
+  Timer timer(a, stream);
+  timer.mark();  // no geometry phase
+  void* out = d_out;
+  const size_t esize = cplx ? 16 : 8;
+  if (single) {
+    a.convert.alloc(static_cast<size_t>(nt) * ns * esize);
+    out = a.convert.ptr;
+  }
+  const bool empty = nt == 0 || ns == 0;
+  if (!empty) BEMPP_CUDA(cudaMemsetAsync(out, 0, static_cast<size_t>(nt) * ns * esize, stream));
+  timer.mark();
+  QuadPairArgs g{};
+  g.kernel = a.kernel;
+  g.op = a.op;
+  g.k = a.k;
+  g.nbt = test.nbasis;
+  g.nbs = trial.nbasis;
+  g.test = quad_cells(*test.grid);
+  g.trial = quad_cells(*trial.grid);
+  g.test_dofs = test.d_dofs.as<int>();
+  g.trial_dofs = trial.d_dofs.as<int>();
+  g.rule = rule;
+  g.same_grid = same_grid ? 1 : 0;
+  g.out = out;
+  g.ld = nt;
+  if (!empty) {
+    g.singular = false;
+    BEMPP_CUDA(launch_quad_pairs(g, stream));
+    ++a.launches;
+  }
+  timer.mark();
+  if (!empty && same_grid) {
+    SingularPairList& pl = grid_pairs(*test.grid, device);
+    const DeviceRules& dr = device_rules(device, order, true);
+    g.rules = SingularRules{dr.offset.as<int>(), dr.test_xi.as<double>(), dr.trial_xi.as<double>(),
+                            dr.w.as<double>()};
+    g.pairs = SingularPairs{static_cast<int>(pl.test_cell.size()), pl.d_test.as<int>(),
+                            pl.d_trial.as<int>(), pl.d_config.as<int>()};
+    g.singular = true;
+    BEMPP_CUDA(launch_quad_pairs(g, stream));
+    ++a.launches;
+  }
+  if (single && !empty) {
+    BEMPP_CUDA(launch_convert_to_single(static_cast<const double*>(out), d_out,
+                                        static_cast<size_t>(nt) * ns * (cplx ? 2 : 1), stream));
+    ++a.launches;
+  }
+  if (chunk_done) chunk_done(0);
+  timer.mark();
+  timer.finish();
+}
+
+}  // namespace
+
 void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d_out,
                      cudaStream_t stream, int nchunks, const std::function<void(int)>& chunk_done) {
   check_spaces(a, trial, test);
+  if (trial.grid->quads()) {
+    assemble_quad_device(a, trial, test, d_out, stream, chunk_done);
+    return;
+  }
   const int device = current_device();
   const auto qit = a.options.regular.find(kTriangle);
   if (qit == a.options.regular.end())
@@ -453,6 +568,8 @@ void check_potential(const BoundaryAssemblerT& a, const SpaceT& space, int64_t n
   if (a.op != kSL && a.op != kDL)
     throw Error(kUnsupported, "potential operators: single and double layer only");
   if (npoints < 0 || npoints > 0x7fffffff) throw Error(kInvalidArgument, "point count");
+  if (space.grid->quads())
+    throw Error(kUnsupported, "potential operators on quadrilateral grids are not supported");
   if (space.nbasis != 1 && space.nbasis != 3 && space.nbasis != 6)
     throw Error(kUnsupported, "potential operators: Lagrange spaces of degree 0, 1 or 2");
 }
@@ -521,6 +638,7 @@ SingularRules sweep_rules(int device, int order) {
 void helmholtz_sl_gradient_device(GridT& g, const Options& opts, double k, const double* d_lam,
                                   const double* d_mu, double* d_totals, double* d_grad_points,
                                   cudaStream_t stream) {
+  if (g.quads()) throw Error(kUnsupported, "the adjoint gradient needs a triangle grid");
   const int device = current_device();
   const auto qit = opts.regular.find(kTriangle);
   const auto sit = opts.singular.find({kTriangle, kTriangle});
@@ -559,7 +677,38 @@ MatrixT* assemble_singular_csr(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& tes
   std::vector<int64_t> rows, cols;
   std::vector<double> vals;  // FP64 (interleaved complex)
   const int nvals = test.nbasis * trial.nbasis * (cplx ? 2 : 1);
-  if (trial.grid == test.grid && test.ndofs > 0 && trial.ndofs > 0) {
+  int np = 0;
+  const SingularPairList* pl_used = nullptr;
+  if (trial.grid == test.grid && test.ndofs > 0 && trial.ndofs > 0 && test.grid->quads()) {
+    QuadGaussRule qrule;
+    int order;
+    quad_rules(a.options, qrule, order);
+    ensure_space_device(test, device);
+    ensure_space_device(trial, device);
+    SingularPairList& pl = grid_pairs(*test.grid, device);
+    const DeviceRules& dr = device_rules(device, order, true);
+    np = static_cast<int>(pl.test_cell.size());
+    a.pair_values.alloc(sizeof(double) * std::max(1, np * nvals));
+    QuadPairArgs g{};
+    g.kernel = a.kernel;
+    g.op = a.op;
+    g.k = a.k;
+    g.nbt = test.nbasis;
+    g.nbs = trial.nbasis;
+    g.test = g.trial = quad_cells(*test.grid);
+    g.test_dofs = test.d_dofs.as<int>();
+    g.trial_dofs = trial.d_dofs.as<int>();
+    g.rule = qrule;
+    g.rules = SingularRules{dr.offset.as<int>(), dr.test_xi.as<double>(), dr.trial_xi.as<double>(),
+                            dr.w.as<double>()};
+    g.pairs = SingularPairs{np, pl.d_test.as<int>(), pl.d_trial.as<int>(), pl.d_config.as<int>()};
+    g.singular = true;
+    g.same_grid = 1;
+    g.out = nullptr;
+    g.pair_values = a.pair_values.as<double>();
+    BEMPP_CUDA(launch_quad_pairs(g, nullptr));
+    pl_used = &pl;
+  } else if (trial.grid == test.grid && test.ndofs > 0 && trial.ndofs > 0) {
     const auto sit = a.options.singular.find({kTriangle, kTriangle});
     if (sit == a.options.singular.end())
       throw Error(kInvalidArgument, "no singular quadrature degree for triangle pairs");
@@ -571,7 +720,7 @@ MatrixT* assemble_singular_csr(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& tes
     const GridGeometry& geo = grid_geometry(*test.grid, device, rule, nullptr, launches);
     SingularPairList& pl = grid_pairs(*test.grid, device);
     const DeviceRules& dr = device_rules(device, static_cast<int>(sit->second));
-    const int np = static_cast<int>(pl.test_cell.size());
+    np = static_cast<int>(pl.test_cell.size());
     a.pair_values.alloc(sizeof(double) * std::max(1, np * nvals));
     SingularRules rules{dr.offset.as<int>(), dr.test_xi.as<double>(), dr.trial_xi.as<double>(),
                         dr.w.as<double>()};
@@ -581,6 +730,10 @@ MatrixT* assemble_singular_csr(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& tes
     const CellSet cs = cell_set(*test.grid, geo);
     BEMPP_CUDA(launch_singular(cs, test.d_dofs.as<int>(), test.nbasis, cs, trial.d_dofs.as<int>(),
                                trial.nbasis, rules, pairs, sa, nullptr));
+    pl_used = &pl;
+  }
+  if (pl_used) {
+    const SingularPairList& pl = *pl_used;
     std::vector<double> pv(static_cast<size_t>(np) * nvals);
     BEMPP_CUDA(cudaMemcpy(pv.data(), a.pair_values.ptr, pv.size() * sizeof(double),
                           cudaMemcpyDeviceToHost));

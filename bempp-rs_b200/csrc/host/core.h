@@ -113,6 +113,13 @@ struct DuffyRule {
   std::vector<double> test_xi, trial_xi, w;
 };
 DuffyRule duffy_rule(int config, int order);
+// Quadrilaterals: the n x n Gauss tensor rule for a request of `npoints` (n the smallest
+// with n^2 >= npoints), the 49 vertex pairings of two quadrilaterals that share a vertex
+// (16 vertex, 32 edge, 1 identical) and their Duffy rules of 1-D order n.
+int quad_gauss_order(size_t npoints);
+QuadGaussRule quad_gauss_rule(size_t npoints);
+const std::vector<std::vector<std::pair<int, int>>>& quad_singular_configurations();
+DuffyRule quad_duffy_rule(int config, int order);
 
 // --------------------------------------------------------------------- grid/space ---
 struct GridGeometry {  // device geometry for one regular rule
@@ -145,15 +152,21 @@ using bempp_b200::DeviceBuffer;
 struct GridT {
   uint64_t uid = 0;            // unique per grid object (plans keyed by it)
   std::vector<double> points;  // npoints x 3
-  std::vector<int> cells;      // ncells x 3 (triangle vertices as point indices: geometry)
+  // ncells x nv (nv = 3 for triangles, 4 for quadrilaterals; cell vertices as point
+  // indices: geometry)
+  std::vector<int> cells;
   int64_t npoints = 0, ncells = 0;
-  // Topology vertex of each cell corner (ncells x 3), when the grid came with ndgrid's
+  uint8_t cell_type = bempp_b200::kTriangle;  // kTriangle or kQuadrilateral
+  int nv() const { return cell_type == bempp_b200::kQuadrilateral ? 4 : 3; }
+  bool quads() const { return cell_type == bempp_b200::kQuadrilateral; }
+  // Topology vertex of each cell corner (ncells x nv), when the grid came with ndgrid's
   // cell -> vertex connectivity; empty: the point indices of `cells` are the vertices.
   // Adjacency (singular pairs, near-field vertex tests) and vertex DOFs use these ids.
   std::vector<int> topo;
   int64_t nvertices = 0;
   // ndgrid's cell -> edge connectivity (local edge i opposite local vertex i) and edge ->
-  // vertex connectivity, when given; build_topology then keeps ndgrid's edge numbering.
+  // vertex connectivity, when given; build_topology then keeps ndgrid's edge numbering
+  // (triangles; quadrilateral grids keep no edges, their spaces have no edge DOFs).
   std::vector<int> given_cell_edges;    // ncells x 3
   std::vector<int> given_edge_vertices; // nedges x 2
   const int* vtx() const { return topo.empty() ? cells.data() : topo.data(); }

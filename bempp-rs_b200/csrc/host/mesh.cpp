@@ -23,9 +23,11 @@
 void GridT::build_topology() {
   if (!vertex_cells.empty() || ncells == 0) return;
   const int* vx = vtx();
+  const int n = nv();
   vertex_cells.assign(nverts(), {});
   for (int64_t c = 0; c < ncells; ++c)
-    for (int i = 0; i < 3; ++i) vertex_cells[vx[3 * c + i]].push_back(static_cast<int>(c));
+    for (int i = 0; i < n; ++i) vertex_cells[vx[n * c + i]].push_back(static_cast<int>(c));
+  if (quads()) return;  // quadrilateral spaces (degree <= 1) have no edge DOFs
   if (!given_cell_edges.empty()) {
     // ndgrid's own edge numbering (validated when the grid was created)
     const int64_t ne = static_cast<int64_t>(given_edge_vertices.size() / 2);
@@ -68,6 +70,8 @@ SpaceT* make_space(GridT* grid, const ElementFamilyT& fam) {
   if (fam.degree > 2)
     throw Error(kUnsupported, "only Lagrange degree 0, 1 and 2 spaces are supported");
   std::lock_guard<std::mutex> lock(grid->mu);
+  if (grid->quads() && fam.degree > 1)
+    throw Error(kUnsupported, "quadrilateral grids: Lagrange degree 0 and 1 spaces only");
   grid->build_topology();
   auto* s = new SpaceT();
   s->grid = grid;
@@ -78,7 +82,24 @@ SpaceT* make_space(GridT* grid, const ElementFamilyT& fam) {
   s->entity_dofs[0].assign(grid->nverts(), {});
   s->entity_dofs[1].assign(grid->edges.size(), {});
   s->entity_dofs[2].assign(nc, {});
-  if (fam.degree == 0) {
+  if (grid->quads() && fam.degree == 1) {
+    // Q1 (one DOF per vertex, first visit) or DQ1 (four interior DOFs per cell)
+    s->nbasis = 4;
+    s->cell_dofs.resize(4 * nc);
+    int64_t size = 0;
+    for (int64_t c = 0; c < nc; ++c)
+      for (int i = 0; i < 4; ++i) {
+        if (s->continuous) {
+          auto& ed = s->entity_dofs[0][grid->vtx()[4 * c + i]];
+          if (ed.empty()) ed.push_back(size++);
+          s->cell_dofs[4 * c + i] = ed[0];
+        } else {
+          s->cell_dofs[4 * c + i] = size;
+          s->entity_dofs[2][c].push_back(size++);
+        }
+      }
+    s->ndofs = size;
+  } else if (fam.degree == 0) {
     // DP0: one DOF on the cell itself (Lagrange degree 0 is discontinuous)
     s->nbasis = 1;
     s->cell_dofs.resize(nc);
@@ -138,11 +159,12 @@ std::vector<std::vector<int64_t>> cell_colouring(const SpaceT& s) {
   const bool vertex_based = s.continuous;
   std::vector<std::vector<int64_t>> colours;
   std::vector<std::vector<int>> entity_colours(vertex_based ? g.nverts() : g.ncells);
+  const int nv = g.nv();
   for (int64_t c = 0; c < g.ncells; ++c) {
-    int ents[3];
+    int ents[4];
     int ne = 0;
     if (vertex_based)
-      for (int i = 0; i < 3; ++i) ents[ne++] = g.vtx()[3 * c + i];
+      for (int i = 0; i < nv; ++i) ents[ne++] = g.vtx()[nv * c + i];
     else
       ents[ne++] = static_cast<int>(c);
     int col = 0;
@@ -160,6 +182,34 @@ std::vector<std::vector<int64_t>> cell_colouring(const SpaceT& s) {
   return colours;
 }
 
+namespace {
+
+// Index in quad_singular_configurations() of the shared-vertex pairing (ts[i], ss[i]),
+// i < n, trial local ascending: 16 vertex pairings (test * 4 + trial), 32 edge pairings
+// (16 + (test edge * 4 + trial edge) * 2 + orientation, edges [0,1], [0,2], [1,3],
+// [2,3]), the identical cell 48; -1 for anything else.
+int quad_configuration(const int* ts, const int* ss, int n) {
+  auto edge = [](int a, int b) {
+    const int lo = std::min(a, b), hi = std::max(a, b);
+    if (lo == 0 && hi == 1) return 0;
+    if (lo == 0 && hi == 2) return 1;
+    if (lo == 1 && hi == 3) return 2;
+    if (lo == 2 && hi == 3) return 3;
+    return -1;
+  };
+  if (n == 1) return ts[0] * 4 + ss[0];
+  if (n == 2) {
+    const int et = edge(ts[0], ts[1]), es = edge(ss[0], ss[1]);
+    if (et < 0 || es < 0) return -1;
+    // orientation 0: the trial edge's first vertex meets the test edge's first vertex
+    return 16 + (et * 4 + es) * 2 + (ts[0] < ts[1] ? 0 : 1);
+  }
+  if (n == 4 && ts[0] == 0 && ts[1] == 1 && ts[2] == 2 && ts[3] == 3) return 48;
+  return -1;
+}
+
+}  // namespace
+
 // Singular pair enumeration; pairs grouped by configuration (as cell_pairs[config] in
 // make_cell_blocks), vertices visited in increasing order.
 void build_singular_pairs(GridT& g, SingularPairList& out) {
@@ -167,7 +217,10 @@ void build_singular_pairs(GridT& g, SingularPairList& out) {
   // vertex.  Contiguous vertex ranges go to host threads; concatenating their per-
   // configuration lists in range order gives exactly the serial order (configuration,
   // then vertex, then test cell, then trial cell).
-  const int ncfg = static_cast<int>(singular_configurations().size());
+  const bool quads = g.quads();
+  const int cv = g.nv();  // vertices per cell
+  const int ncfg = static_cast<int>(quads ? quad_singular_configurations().size()
+                                          : singular_configurations().size());
   const int64_t nv = g.nverts();
   const int nthreads = static_cast<int>(std::max<int64_t>(
       1, std::min<int64_t>({static_cast<int64_t>(std::thread::hardware_concurrency()), 16,
@@ -185,12 +238,12 @@ void build_singular_pairs(GridT& g, SingularPairList& out) {
         for (int sc : g.vertex_cells[v]) {
           // shared vertices as (test local, trial local), trial local ascending; the pair
           // belongs to its smallest shared vertex
-          int ts[3], ss[3], n = 0;
+          int ts[4], ss[4], n = 0;
           bool smallest = true;
-          for (int si = 0; si < 3 && smallest; ++si)
-            for (int ti = 0; ti < 3; ++ti)
-              if (cells[3 * tc + ti] == cells[3 * sc + si]) {
-                if (cells[3 * tc + ti] < v) {
+          for (int si = 0; si < cv && smallest; ++si)
+            for (int ti = 0; ti < cv; ++ti)
+              if (cells[cv * tc + ti] == cells[cv * sc + si]) {
+                if (cells[cv * tc + ti] < v) {
                   smallest = false;
                   break;
                 }
@@ -203,7 +256,9 @@ void build_singular_pairs(GridT& g, SingularPairList& out) {
           // pairings (test * 3 + trial), 18 edge pairings (edges opposite et / es, two
           // orientations), identical cells last
           int cfg = -1;
-          if (n == 1) {
+          if (quads) {
+            cfg = quad_configuration(ts, ss, n);
+          } else if (n == 1) {
             cfg = ts[0] * 3 + ss[0];
           } else if (n == 2) {
             const int et = 3 - ts[0] - ts[1], es = 3 - ss[0] - ss[1];
@@ -314,12 +369,17 @@ double GridT::max_circumradius() {
   std::lock_guard<std::mutex> lock(mu);
   if (max_rad >= 0.0) return max_rad;
   double m = 0.0;
+  const int n = nv();
   for (int64_t c = 0; c < ncells; ++c) {
-    const double* v[3] = {&points[3 * cells[3 * c]], &points[3 * cells[3 * c + 1]],
-                          &points[3 * cells[3 * c + 2]]};
+    const double* v[4];
+    for (int i = 0; i < n; ++i) v[i] = &points[3 * cells[n * c + i]];
     double cen[3];
-    for (int d = 0; d < 3; ++d) cen[d] = (v[0][d] + v[1][d] + v[2][d]) / 3.0;
-    for (int i = 0; i < 3; ++i) {
+    for (int d = 0; d < 3; ++d) {
+      cen[d] = 0.0;
+      for (int i = 0; i < n; ++i) cen[d] += v[i][d];
+      cen[d] /= n;
+    }
+    for (int i = 0; i < n; ++i) {
       const double x = v[i][0] - cen[0], y = v[i][1] - cen[1], z = v[i][2] - cen[2];
       m = std::max(m, std::sqrt(x * x + y * y + z * z));
     }

@@ -15,7 +15,9 @@
 // That's vertices P0=(0,0), P1=(1,0), P2=(1,1) (barycentric (1-x1, x1-x2, x2)) are
 // mapped onto the cells' local vertices so that the shared vertex is P0 and the shared
 // edge is P0-P1 in both cells.
+#include <algorithm>
 #include <cmath>
+#include <functional>
 #include <stdexcept>
 #include <string>
 
@@ -219,6 +221,156 @@ DuffyRule duffy_rule(int config, int order) {
             r.trial_xi.push_back(v);
             r.w.push_back(gw[i0] * gw[i1] * gw[i2] * gw[i3] * p.jac);
           }
+  return r;
+}
+
+// ------------------------------------------------------------------ quadrilaterals ---
+// Quadrilateral rules (ndelement's reference square: v0 = (0,0), v1 = (1,0), v2 = (0,1),
+// v3 = (1,1); edges [0,1], [0,2], [1,3], [2,3]).
+//
+// Regular: Gauss-Legendre tensor rules of n x n points on [0,1]^2 (weights sum to 1), n
+// the smallest with n^2 >= the requested number of points (37, the default, gives 7 x 7).
+//
+// Singular (Sauter & Schwab, Boundary Element Methods, section 5.2, for squares), on a
+// canonical configuration mapped onto the shared entity of each cell by a symmetry of the
+// square, n-point Gauss-Legendre on every coordinate of [0,1]^4:
+//   identical: z = x - y split by the signs of z1, z2 and by which of |z1|, |z2| is larger
+//     (|z| = (xi, xi eta) or (xi eta, xi), Jacobian xi), y on the overlap of the square
+//     and its shift, y_i = max(0, -z_i) + (1 - |z_i|) t_i: 8 regions;
+//   edge (shared edge x2 = y2 = 0, x1 = y1 on it): (|x1 - y1|, x2, y2) in 3 pyramids by the
+//     largest coordinate (Jacobian xi^2), 2 signs of x1 - y1, y1 on the overlap: 6 regions;
+//   vertex (shared vertex x = y = 0): (x1, x2, y1, y2) in 4 pyramids by the largest
+//     coordinate (Jacobian xi^3): 4 regions.
+namespace {
+
+const double kQV[4][2] = {{0.0, 0.0}, {1.0, 0.0}, {0.0, 1.0}, {1.0, 1.0}};
+const int kQE[4][2] = {{0, 1}, {0, 2}, {1, 3}, {2, 3}};
+
+// x -> o + x0 d + x1 m: the symmetry of the square taking (0,0) to vertex p and (1,0) to
+// vertex q (q < 0: the reflection that keeps the axes)
+struct SquareSymmetry {
+  double o[2], d[2], m[2];
+  SquareSymmetry(int p, int q) {
+    o[0] = kQV[p][0];
+    o[1] = kQV[p][1];
+    const double sx = kQV[p][0] == 0.0 ? 1.0 : -1.0, sy = kQV[p][1] == 0.0 ? 1.0 : -1.0;
+    if (q < 0) {
+      d[0] = sx; d[1] = 0.0; m[0] = 0.0; m[1] = sy;
+      return;
+    }
+    d[0] = kQV[q][0] - kQV[p][0];
+    d[1] = kQV[q][1] - kQV[p][1];
+    if (d[0] != 0.0) {
+      m[0] = 0.0; m[1] = sy;
+    } else {
+      m[0] = sx; m[1] = 0.0;
+    }
+  }
+  void apply(double a, double b, std::vector<double>& out) const {
+    out.push_back(o[0] + a * d[0] + b * m[0]);
+    out.push_back(o[1] + a * d[1] + b * m[1]);
+  }
+};
+
+}  // namespace
+
+int quad_gauss_order(size_t npoints) {
+  int n = 1;
+  while (static_cast<size_t>(n) * n < npoints) ++n;
+  if (n > kMaxQuadGauss)
+    throw Error(kUnsupported, "quadrilateral regular rules have at most " +
+                                  std::to_string(kMaxQuadGauss * kMaxQuadGauss) + " points; " +
+                                  std::to_string(npoints) + " asked");
+  return n;
+}
+
+QuadGaussRule quad_gauss_rule(size_t npoints) {
+  const int n = quad_gauss_order(npoints);
+  std::vector<double> g, gw;
+  gauss_legendre_01(n, g, gw);
+  QuadGaussRule r{};
+  r.n = n;
+  for (int i = 0; i < n; ++i) {
+    r.x[i] = g[i];
+    r.w[i] = gw[i];
+  }
+  return r;
+}
+
+const std::vector<std::vector<std::pair<int, int>>>& quad_singular_configurations() {
+  static const std::vector<std::vector<std::pair<int, int>>> configs = [] {
+    std::vector<std::vector<std::pair<int, int>>> out;
+    for (int t = 0; t < 4; ++t)
+      for (int s = 0; s < 4; ++s) out.push_back({{t, s}});
+    for (int te = 0; te < 4; ++te)
+      for (int se = 0; se < 4; ++se) {
+        out.push_back({{kQE[te][0], kQE[se][0]}, {kQE[te][1], kQE[se][1]}});
+        out.push_back({{kQE[te][1], kQE[se][0]}, {kQE[te][0], kQE[se][1]}});
+      }
+    out.push_back({{0, 0}, {1, 1}, {2, 2}, {3, 3}});
+    return out;
+  }();
+  return configs;
+}
+
+DuffyRule quad_duffy_rule(int config, int order) {
+  const auto& configs = quad_singular_configurations();
+  if (config < 0 || config >= static_cast<int>(configs.size()) || order < 1)
+    throw Error(kInvalidArgument, "quadrilateral Duffy rule: bad configuration or order");
+  const auto& pairs = configs[config];
+  std::vector<double> g, gw;
+  gauss_legendre_01(order, g, gw);
+  const SquareSymmetry mt = pairs.size() == 4   ? SquareSymmetry(0, 1)
+                            : pairs.size() == 2 ? SquareSymmetry(pairs[0].first, pairs[1].first)
+                                                : SquareSymmetry(pairs[0].first, -1);
+  const SquareSymmetry ms = pairs.size() == 4   ? SquareSymmetry(0, 1)
+                            : pairs.size() == 2 ? SquareSymmetry(pairs[0].second, pairs[1].second)
+                                                : SquareSymmetry(pairs[0].second, -1);
+  DuffyRule r;
+  auto push = [&](double x1, double x2, double y1, double y2, double w) {
+    mt.apply(x1, x2, r.test_xi);
+    ms.apply(y1, y2, r.trial_xi);
+    r.w.push_back(w);
+  };
+  const int n = order;
+  // region loops outermost, then the Gauss points of (xi, a, b, c)
+  auto gauss4 = [&](const std::function<void(double, double, double, double, double)>& f) {
+    for (int i0 = 0; i0 < n; ++i0)
+      for (int i1 = 0; i1 < n; ++i1)
+        for (int i2 = 0; i2 < n; ++i2)
+          for (int i3 = 0; i3 < n; ++i3)
+            f(g[i0], g[i1], g[i2], g[i3], gw[i0] * gw[i1] * gw[i2] * gw[i3]);
+  };
+  if (pairs.size() == 4) {
+    for (int s1 = -1; s1 <= 1; s1 += 2)
+      for (int s2 = -1; s2 <= 1; s2 += 2)
+        for (int first = 1; first >= 0; --first)  // |z1| >= |z2| first
+          gauss4([&](double xi, double a, double b, double c, double wq) {
+            const double z1 = s1 * (first ? xi : xi * a), z2 = s2 * (first ? xi * a : xi);
+            const double y1 = std::max(0.0, -z1) + (1.0 - std::fabs(z1)) * b;
+            const double y2 = std::max(0.0, -z2) + (1.0 - std::fabs(z2)) * c;
+            push(y1 + z1, y2 + z2, y1, y2,
+                 wq * xi * (1.0 - std::fabs(z1)) * (1.0 - std::fabs(z2)));
+          });
+  } else if (pairs.size() == 2) {
+    for (int s = -1; s <= 1; s += 2)
+      for (int pyr = 0; pyr < 3; ++pyr)  // the largest of (|x1 - y1|, x2, y2)
+        gauss4([&](double xi, double a, double b, double c, double wq) {
+          double u[3];
+          for (int k = 0, e = 0; k < 3; ++k) u[k] = k == pyr ? xi : xi * (e++ == 0 ? a : b);
+          const double z = s * u[0];
+          const double y1 = std::max(0.0, -z) + (1.0 - u[0]) * c;
+          push(y1 + z, u[1], y1, u[2], wq * xi * xi * (1.0 - u[0]));
+        });
+  } else {
+    for (int pyr = 0; pyr < 4; ++pyr)  // the largest of (x1, x2, y1, y2)
+      gauss4([&](double xi, double a, double b, double c, double wq) {
+        const double e[3] = {a, b, c};
+        double u[4];
+        for (int k = 0, j = 0; k < 4; ++k) u[k] = k == pyr ? xi : xi * e[j++];
+        push(u[0], u[1], u[2], u[3], wq * xi * xi * xi);
+      });
+  }
   return r;
 }
 

@@ -83,6 +83,8 @@ void helmholtz_sl_sweep_device(GridT* const* grids, size_t ngrids, const double*
   if (ngrids == 0 || nk == 0) return;
   if (ngrids > static_cast<size_t>(kMaxSweepMeshes))
     throw Error(kUnsupported, "at most 8 meshes per sweep");
+  for (size_t i = 0; i < ngrids; ++i)
+    if (grids[i]->quads()) throw Error(kUnsupported, "the sweep needs triangle grids");
   const auto qit = opts.regular.find(kTriangle);
   const auto sit = opts.singular.find({kTriangle, kTriangle});
   if (qit == opts.regular.end() || qit->second != 6)

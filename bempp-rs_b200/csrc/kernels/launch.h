@@ -150,6 +150,43 @@ struct GenericPairArgs {
 };
 cudaError_t launch_generic_pairs(const GenericPairArgs& g, cudaStream_t stream);
 
+// Quadrilateral grids (quad.cu): bilinear cells given by their four vertices in the
+// reference square's order (0,0), (1,0), (0,1), (1,1).
+constexpr int kMaxQuadGauss = 16;
+struct QuadGaussRule {  // n-point Gauss-Legendre rule on [0, 1]; the cell rule is n x n
+  int n;
+  double x[kMaxQuadGauss];
+  double w[kMaxQuadGauss];
+};
+struct QuadCells {
+  int ncells;
+  const double* points;  // npoints x 3
+  const int* cells;      // ncells x 4 point indices (geometry)
+  const int* vids;       // ncells x 4 topology vertex ids (adjacency)
+};
+// Cell-pair quadrature of DP0 / Q1 / DQ1 spaces (nbt, nbs in {1, 4}), FP64, one warp per
+// pair, as GenericPairArgs: the regular part over every (test cell, trial cell in
+// [trial_lo, trial_hi)) pair (vertex-sharing pairs skipped on one grid) with the n x n
+// Gauss rule on both cells, or the singular list with the quadrilateral Duffy rules.
+struct QuadPairArgs {
+  int kernel, op;
+  double k;
+  int nbt, nbs;
+  QuadCells test, trial;
+  const int* test_dofs;
+  const int* trial_dofs;
+  QuadGaussRule rule;
+  SingularRules rules;
+  SingularPairs pairs;
+  bool singular;
+  int same_grid;
+  void* out;
+  int64_t ld;
+  int trial_lo = 0, trial_hi = 0x7fffffff;
+  double* pair_values = nullptr;
+};
+cudaError_t launch_quad_pairs(const QuadPairArgs& g, cudaStream_t stream);
+
 // Allocation-free regular DP0 assembly between two distinct meshes (noalloc.cu); the
 // scratch lives in a static device array of noalloc_max_cells() cells per mesh and
 // noalloc_max_points() regular points.  The vertex indices are checked on the device

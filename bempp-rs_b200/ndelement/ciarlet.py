@@ -22,7 +22,8 @@ class Continuity(IntEnum):
 
 class CiarletElement:
     """Lagrange element on a triangle: degree 0 (one DOF), 1 (three) or 2 (six: the
-    vertices, then the midpoints of edges [1,2], [0,2], [0,1])."""
+    vertices, then the midpoints of edges [1,2], [0,2], [0,1]); on a quadrilateral:
+    degree 0 (one DOF) or 1 (four, one per vertex)."""
 
     def __init__(self, cell: ReferenceCellType, degree: int, continuity: Continuity):
         self.cell_type = cell
@@ -31,6 +32,8 @@ class CiarletElement:
 
     @property
     def dim(self) -> int:
+        if self.cell_type == ReferenceCellType.Quadrilateral:
+            return {0: 1, 1: 4, 2: 9}[self.degree]
         return {0: 1, 1: 3, 2: 6}[self.degree]
 
 

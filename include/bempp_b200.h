@@ -392,9 +392,21 @@ size_t bempp_regular_rule(size_t npoints, double *points, double *weights);
  * `order`.  Returns the number of points (arrays of 2n, 2n, n; NULL to query), or 0. */
 size_t bempp_singular_rule(size_t config, size_t order, double *test_points,
                            double *trial_points, double *weights);
+/* Addition: the regular rule used on quadrilaterals for a requested count of `npoints`:
+ * the n x n Gauss-Legendre tensor rule on [0,1]^2, n the smallest with n^2 >= npoints
+ * (at most 16).  Points as x0,y0,x1,y1,... (point i * n + j at (g_i, g_j)), weights
+ * summing to 1.  Returns n^2 (0 on error); either array may be NULL. */
+size_t bempp_quadrilateral_regular_rule(size_t npoints, double *points, double *weights);
+/* Addition: the Duffy rule of quadrilateral configuration `config` (0..48: 16 vertex
+ * pairings test * 4 + trial, 32 edge pairings 16 + (test edge * 4 + trial edge) * 2 +
+ * orientation with the edges [0,1], [0,2], [1,3], [2,3], the identical cell 48) with 1-D
+ * order `order`: 4, 6 or 8 regions of order^4 points.  Returns the number of points. */
+size_t bempp_quadrilateral_singular_rule(size_t config, size_t order, double *test_points,
+                                         double *trial_points, double *weights);
 /* Addition: the ordered cell pairs of a grid that share a vertex (the singular part),
- * grouped by configuration as src/boundary_assemblers.rs:564-606 groups them.  Returns
- * the number of pairs; arrays may be NULL to query. */
+ * grouped by configuration as src/boundary_assemblers.rs:564-606 groups them (the 28
+ * triangle or the 49 quadrilateral configurations).  Returns the number of pairs; arrays
+ * may be NULL to query. */
 size_t bempp_grid_singular_pairs(GridT *grid, size_t *test_cells, size_t *trial_cells,
                                  size_t *configs);
 

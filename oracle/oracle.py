@@ -74,6 +74,17 @@ def lib():
             L.oracle_duffy_rule.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, dp]
             L.oracle_simplex_rule.restype = ctypes.c_int
             L.oracle_simplex_rule.argtypes = [ctypes.c_int, dp, dp]
+            L.oracle_quad_assemble_dense.restype = ctypes.c_int
+            L.oracle_quad_assemble_dense.argtypes = [
+                ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, ctypes.c_int64, i64p,
+                ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+            L.oracle_quad_last_error.restype = ctypes.c_char_p
+            L.oracle_quad_cell_dofs.restype = ctypes.c_int64
+            L.oracle_quad_cell_dofs.argtypes = [i64p, ctypes.c_int64, ctypes.c_int64,
+                                                ctypes.c_int, ctypes.c_int, i64p]
+            L.oracle_quad_duffy_rule.restype = ctypes.c_int
+            L.oracle_quad_duffy_rule.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, dp]
             _lib = L
     return _lib
 
@@ -155,4 +166,48 @@ def assemble(points, cells, kernel, operator, *, k=0.0, test_degree=0, test_cont
         out.ctypes.data_as(ctypes.c_void_p))
     if rc != 0:
         raise RuntimeError(lib().oracle_last_error().decode())
+    return out
+
+
+# ------------------------------------------------------------ quadrilateral grids ---
+def quad_cell_dofs(points, cells, degree, continuous):
+    """DOF map of a Lagrange degree-0 / 1 space on a quadrilateral grid (ncells x 4)."""
+    cells = np.ascontiguousarray(cells, dtype=np.int64)
+    nb = 1 if degree == 0 else 4
+    out = np.empty(cells.shape[0] * nb, dtype=np.int64)
+    n = lib().oracle_quad_cell_dofs(_ptr(cells, ctypes.c_int64), cells.shape[0], len(points),
+                                    degree, int(continuous), _ptr(out, ctypes.c_int64))
+    return out.reshape(-1, nb), int(n)
+
+
+def quad_duffy_rule(config, order):
+    L = lib()
+    n = L.oracle_quad_duffy_rule(config, order, None, None, None)
+    tp = np.empty(2 * n)
+    sp = np.empty(2 * n)
+    w = np.empty(n)
+    L.oracle_quad_duffy_rule(config, order, _ptr(tp, ctypes.c_double), _ptr(sp, ctypes.c_double),
+                             _ptr(w, ctypes.c_double))
+    return tp.reshape(n, 2), sp.reshape(n, 2), w
+
+
+def quad_assemble(points, cells, kernel, operator, *, k=0.0, test_degree=0,
+                  test_continuous=False, trial_degree=0, trial_continuous=False, q_regular=16,
+                  q_singular=4, nthreads=0, parts=3):
+    """Dense FP64 matrix of a boundary operator on a quadrilateral grid (ncells x 4 cells in
+    ndelement's vertex order), Gauss tensor regular rule of n x n points, n the smallest
+    with n^2 >= q_regular."""
+    points = np.ascontiguousarray(points, dtype=np.float64)
+    cells = np.ascontiguousarray(cells, dtype=np.int64)
+    helm = kernel == "helmholtz"
+    _, n_test = quad_cell_dofs(points, cells, test_degree, test_continuous)
+    _, n_trial = quad_cell_dofs(points, cells, trial_degree, trial_continuous)
+    out = np.zeros((n_test, n_trial), dtype=np.complex128 if helm else np.float64, order="F")
+    rc = lib().oracle_quad_assemble_dense(
+        int(helm), OPERATORS[operator], float(k), _ptr(points, ctypes.c_double), len(points),
+        _ptr(cells, ctypes.c_int64), cells.shape[0], test_degree, int(test_continuous),
+        trial_degree, int(trial_continuous), q_regular, q_singular, nthreads, parts,
+        out.ctypes.data_as(ctypes.c_void_p))
+    if rc != 0:
+        raise RuntimeError(lib().oracle_quad_last_error().decode())
     return out

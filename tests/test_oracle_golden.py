@@ -133,3 +133,68 @@ def test_oracle_p2_potential_restricted_to_p1():
     p1 = potential.potential(x, pts, cells, "helmholtz", "double_layer", k=2.0, degree=1,
                              continuous=True, q_regular=6)
     assert np.linalg.norm(p2 @ T - p1) / np.linalg.norm(p1) <= 1e-13
+
+
+# ------------------------------------------------------------ quadrilateral rules ---
+def _quad_configs():
+    edges = [(0, 1), (0, 2), (1, 3), (2, 3)]
+    out = [[(t, s)] for t in range(4) for s in range(4)]
+    for te in range(4):
+        for se in range(4):
+            out.append([(edges[te][0], edges[se][0]), (edges[te][1], edges[se][1])])
+            out.append([(edges[te][1], edges[se][0]), (edges[te][0], edges[se][1])])
+    out.append([(0, 0), (1, 1), (2, 2), (3, 3)])
+    return out
+
+
+def test_quad_duffy_identical_rule_gives_the_coulomb_energy_of_a_square():
+    """int_Q int_Q 1/|x - y| over the unit square = 4 ln(1 + sqrt 2) - (4/3)(sqrt 2 - 1)."""
+    exact = 4 * np.log(1 + np.sqrt(2)) - 4 / 3 * (np.sqrt(2) - 1)
+    tp, sp, w = oracle.quad_duffy_rule(48, 10)
+    assert abs(np.sum(w / np.linalg.norm(tp - sp, axis=1)) - exact) <= 1e-12
+
+
+def _bilinear(v, xi):
+    s, t = xi[:, 0:1], xi[:, 1:2]
+    return v[0] * (1 - s) * (1 - t) + v[1] * s * (1 - t) + v[2] * (1 - s) * t + v[3] * s * t
+
+
+def _quad_pair_integral(x, y, order):
+    pairs = [(ti, si) for si in range(4) for ti in range(4) if np.allclose(x[ti], y[si])]
+    tp, sp, w = oracle.quad_duffy_rule(_quad_configs().index(pairs), order)
+    return np.sum(w / np.linalg.norm(_bilinear(x, tp) - _bilinear(y, sp), axis=1))
+
+
+def test_quad_duffy_edge_and_vertex_rules_split_the_coulomb_energy():
+    """Two unit squares sharing an edge: E(2 x 1 rectangle) = 2 E(square) + 2 I_edge;
+    four squares of a 2 x 2 square: 8 E = 4 E + 8 I_edge + 4 I_vertex.  Checked for every
+    local numbering of the cells (each maps the shared entity by another symmetry)."""
+    e = 4 * np.log(1 + np.sqrt(2)) - 4 / 3 * (np.sqrt(2) - 1)
+    tp, sp, w = oracle.quad_duffy_rule(48, 16)
+    d = tp - sp
+    d[:, 0] *= 2.0
+    e_rect = 4.0 * np.sum(w / np.linalg.norm(d, axis=1))  # the 2 x 1 rectangle
+    i_edge = (e_rect - 2 * e) / 2
+    i_vertex = e - 2 * i_edge
+    a = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [1, 1, 0]], float)
+    b = a + np.array([1.0, 0.0, 0.0])
+    c = a + np.array([1.0, 1.0, 0.0])
+    # the eight numberings of a square's vertices that keep it a valid cell (D4)
+    perms = [[0, 1, 2, 3], [1, 3, 0, 2], [3, 2, 1, 0], [2, 0, 3, 1],
+             [1, 0, 3, 2], [0, 2, 1, 3], [2, 3, 0, 1], [3, 1, 2, 0]]
+    for pa in perms:
+        for pb in perms[::3]:
+            assert abs(_quad_pair_integral(a[pa], b[pb], 10) - i_edge) <= 1e-12
+            assert abs(_quad_pair_integral(a[pa], c[pb], 10) - i_vertex) <= 1e-12
+
+
+@pytest.mark.parametrize("config", [0, 5, 15, 16, 23, 47, 48])
+def test_quad_duffy_rules_integrate_polynomials(config):
+    """The rules cover both squares exactly: products of monomials in the reference
+    coordinates of the two cells integrate to the products of their 1-D moments."""
+    tp, sp, w = oracle.quad_duffy_rule(config, 8)  # Gauss order 8: exact to degree 15 per axis
+    assert abs(w.sum() - 1.0) <= 1e-13
+    for a_, b_, c_, d_ in [(1, 0, 0, 0), (0, 1, 1, 0), (2, 1, 0, 3), (1, 1, 1, 1), (3, 0, 2, 2)]:
+        f = tp[:, 0] ** a_ * tp[:, 1] ** b_ * sp[:, 0] ** c_ * sp[:, 1] ** d_
+        exact = 1.0 / ((a_ + 1) * (b_ + 1) * (c_ + 1) * (d_ + 1))
+        assert abs(np.sum(w * f) - exact) <= 1e-12
