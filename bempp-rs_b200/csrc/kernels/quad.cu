@@ -25,7 +25,7 @@ constexpr int kWarpsPerBlock = kThreads / 32;
 template <int NB>
 __device__ __forceinline__ void quad_basis(double s, double t, double v[NB], double d0[NB],
                                            double d1[NB]) {
-  if (NB == 1) {
+  if constexpr (NB == 1) {
     v[0] = 1.0;
     d0[0] = d1[0] = 0.0;
   } else {
