@@ -404,6 +404,13 @@ void qassemble(const QMesh& m, const QSpace& ts, const QSpace& ss, int op, bool 
         pts[2 * (i * nreg + j) + 1] = g[j];
         wts[i * nreg + j] = gw[i] * gw[j];
       }
+    // per trial cell its entries, added serially afterwards in trial-cell order: cells of
+    // a continuous space share DOFs, so threads must not add into one column at once
+    struct Trip {
+      int64_t row, col;
+      T val;
+    };
+    std::vector<std::vector<Trip>> per_cell(m.ncells);
 #pragma omp parallel for schedule(dynamic, 4)
     for (int64_t sc = 0; sc < m.ncells; ++sc) {
       std::vector<PGeom> sg(Q), tg(Q);
@@ -425,10 +432,12 @@ void qassemble(const QMesh& m, const QSpace& ts, const QSpace& ss, int op, bool 
                                         t1[4 * p + a], sv[4 * q + b], s0[4 * q + b],
                                         s1[4 * q + b]) *
                      (wts[p] * wts[q]);
-            out[ts.cell_dofs[tc * ntb + a] + nt * ss.cell_dofs[sc * nsb + b]] += e;
+            per_cell[sc].push_back({ts.cell_dofs[tc * ntb + a], ss.cell_dofs[sc * nsb + b], e});
           }
       }
     }
+    for (const auto& cell : per_cell)
+      for (const Trip& tr : cell) out[tr.row + nt * tr.col] += tr.val;
   }
   if (parts & 2) {
     auto configs = quad_configurations();

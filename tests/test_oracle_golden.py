@@ -198,3 +198,15 @@ def test_quad_duffy_rules_integrate_polynomials(config):
         f = tp[:, 0] ** a_ * tp[:, 1] ** b_ * sp[:, 0] ** c_ * sp[:, 1] ** d_
         exact = 1.0 / ((a_ + 1) * (b_ + 1) * (c_ + 1) * (d_ + 1))
         assert abs(np.sum(w * f) - exact) <= 1e-12
+
+
+def test_quad_oracle_is_deterministic_across_threads():
+    """Continuous spaces share DOFs between cells: the quadrilateral oracle's threads must
+    not add into one entry at once (equal results for 1 and 8 threads, bit for bit)."""
+    pts, cells = shapes.cube_quads(3)
+    rng = np.random.default_rng(3)
+    pts = pts * (1 + 0.04 * rng.standard_normal((len(pts), 1)))
+    kw = dict(k=2.0, test_degree=1, test_continuous=True, trial_degree=1, trial_continuous=True)
+    one = oracle.quad_assemble(pts, cells, "helmholtz", "adjoint_double_layer", nthreads=1, **kw)
+    many = oracle.quad_assemble(pts, cells, "helmholtz", "adjoint_double_layer", nthreads=8, **kw)
+    assert np.array_equal(one, many)
