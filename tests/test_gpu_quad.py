@@ -158,7 +158,8 @@ def test_quad_device_memory_and_single_precision(cube):
     o = oracle_quad(cube, "helmholtz", "single_layer", 2.0, test=Q1, trial=Q1)
     assert rel_err(dev.cpu().numpy().T, o) <= FP64_TOL
     a32 = assembler("helmholtz", "single_layer", 2.0, quad_options(), np.complex64)
-    m32 = a32.assemble(sp, sp)
+    sp32 = function_space(cube, create_family(Family.Lagrange, 1, dtype=np.float32))
+    m32 = a32.assemble(sp32, sp32)
     assert m32.dtype == np.complex64
     assert rel_err(m32, o) <= 1e-6
 
