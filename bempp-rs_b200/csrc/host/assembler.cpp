@@ -211,6 +211,28 @@ QuadCells quad_cells(const GridT& g) {
   return q;
 }
 
+// Device data of a quadrilateral grid, with its geometry at the rule's n x n points
+// (computed on first use and cached in the grid, as grid_geometry does for triangles).
+QuadCells quad_cells(GridT& g, int device, const QuadGaussRule& rule, cudaStream_t stream,
+                     size_t& launches) {
+  std::lock_guard<std::mutex> lock(g.mu);
+  ensure_grid_device(g, device);
+  QuadCells q = quad_cells(g);
+  auto& slot = g.quad_geometry[rule.n];
+  if (!slot) {
+    auto buf = std::make_unique<DeviceBuffer>();
+    buf->alloc(sizeof(double) * kQuadGeomFields * static_cast<size_t>(g.ncells) * rule.n * rule.n);
+    BEMPP_CUDA(launch_quad_geometry(q, rule, buf->as<double>(), stream));
+    ++launches;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    BEMPP_CUDA(cudaStreamIsCapturing(stream, &cap));
+    if (cap == cudaStreamCaptureStatusNone) BEMPP_CUDA(cudaStreamSynchronize(stream));
+    slot = std::move(buf);
+  }
+  q.qgeom = slot->as<double>();
+  return q;
+}
+
 // Regular rule and Duffy order of quadrilateral pairs from the options.
 void quad_rules(const Options& o, QuadGaussRule& rule, int& order) {
   const auto qit = o.regular.find(kQuadrilateral);
@@ -299,16 +321,10 @@ void assemble_quad_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, vo
   a.launches = 0;
   ensure_space_device(test, device);
   ensure_space_device(trial, device);
-  {
-    std::lock_guard<std::mutex> lock(test.grid->mu);
-    ensure_grid_device(*test.grid, device);
-  }
-  {
-    std::lock_guard<std::mutex> lock(trial.grid->mu);
-    ensure_grid_device(*trial.grid, device);
-  }
   Timer timer(a, stream);
-  timer.mark();  // no geometry phase
+  const QuadCells tq = quad_cells(*test.grid, device, rule, stream, a.launches);
+  const QuadCells sq = quad_cells(*trial.grid, device, rule, stream, a.launches);
+  timer.mark();
   void* out = d_out;
   const size_t esize = cplx ? 16 : 8;
   if (single) {
@@ -324,8 +340,8 @@ void assemble_quad_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, vo
   g.k = a.k;
   g.nbt = test.nbasis;
   g.nbs = trial.nbasis;
-  g.test = quad_cells(*test.grid);
-  g.trial = quad_cells(*trial.grid);
+  g.test = tq;
+  g.trial = sq;
   g.test_dofs = test.d_dofs.as<int>();
   g.trial_dofs = trial.d_dofs.as<int>();
   g.rule = rule;

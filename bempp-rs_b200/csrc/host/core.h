@@ -178,6 +178,8 @@ struct GridT {
   int device = -1;
   DeviceBuffer d_points, d_cells, d_topo;
   std::map<int, std::unique_ptr<bempp_b200::GridGeometry>> geometry;  // keyed by regular npts
+  // quadrilateral grids: geometry at the n x n regular points, keyed by n
+  std::map<int, std::unique_ptr<DeviceBuffer>> quad_geometry;
   std::unique_ptr<bempp_b200::SingularPairList> pairs;
   DeviceBuffer adjoint_scratch;  // per-cell vertex gradients of the adjoint kernel
   double max_rad = -1.0;         // largest centroid-to-vertex distance (computed on demand)

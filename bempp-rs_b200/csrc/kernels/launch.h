@@ -163,7 +163,15 @@ struct QuadCells {
   const double* points;  // npoints x 3
   const int* cells;      // ncells x 4 point indices (geometry)
   const int* vids;       // ncells x 4 topology vertex ids (adjacency)
+  // geometry at the n x n regular points (launch_quad_geometry), read by the regular part
+  const double* qgeom = nullptr;
 };
+// Geometry of every cell at the rule's n x n points: field f of point p of cell c at
+// out[f * ncells * n^2 + c * n^2 + p], fields x (3), jdet, unit normal (3), J0 (3), J1 (3)
+// (13 * ncells * n^2 doubles).
+constexpr int kQuadGeomFields = 13;
+cudaError_t launch_quad_geometry(const QuadCells& cells, const QuadGaussRule& rule, double* out,
+                                 cudaStream_t stream);
 // Cell-pair quadrature of DP0 / Q1 / DQ1 spaces (nbt, nbs in {1, 4}), FP64, one warp per
 // pair, as GenericPairArgs: the regular part over every (test cell, trial cell in
 // [trial_lo, trial_hi)) pair (vertex-sharing pairs skipped on one grid) with the n x n

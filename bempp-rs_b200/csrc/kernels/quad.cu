@@ -6,8 +6,10 @@
 //
 // Degree-1 quadrilaterals are bilinear, x(s, t) = v0 (1-s)(1-t) + v1 s (1-t) + v2 (1-s) t
 // + v3 s t (ndelement's vertex order), so the Jacobian columns J0 = dx/ds, J1 = dx/dt, the
-// Jacobian determinant |J0 x J1| and the unit normal are formed at every point (the
-// geometry map that bempp-rs takes from ndgrid, cell_pair_assemblers.rs:87-108).  The
+// Jacobian determinant |J0 x J1| and the unit normal vary per point (the geometry map that
+// bempp-rs takes from ndgrid, cell_pair_assemblers.rs:87-108): they are precomputed for
+// every cell at the n x n regular points (quad_geometry_kernel, read back per point pair
+// from L1 / L2) and formed at both points of every Duffy point pair.  The
 // integrands are those of src/boundary_assemblers/integrands/*.rs; the hypersingular one
 // uses the surface curl (J1 d0 phi - J0 d1 phi) / jdet, so that
 //   jdet_x jdet_y curl phi_a . curl psi_b = (J1x d0 phi - J0x d1 phi) . (J1y d0 psi - J0y d1 psi),
@@ -69,6 +71,29 @@ __device__ __forceinline__ void quad_point(const QuadCell& q, double s, double t
   n[2] = cz * inv;
 }
 
+// Geometry of every cell at the n x n regular points: field f of point p of cell c at
+// out[f * ncells * n^2 + c * n^2 + p]; fields x (3), jdet, unit normal (3), J0 (3), J1 (3).
+__global__ void __launch_bounds__(256)
+    quad_geometry_kernel(QuadCells cells, QuadGaussRule rule, double* __restrict__ out) {
+  const int m = rule.n * rule.n;
+  const int64_t total = static_cast<int64_t>(cells.ncells) * m;
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const int c = static_cast<int>(i / m), p = static_cast<int>(i - static_cast<int64_t>(c) * m);
+  QuadCell q;
+  load_quad(cells, c, q);
+  double x[3], j0[3], j1[3], n[3], jdet;
+  quad_point(q, rule.x[p / rule.n], rule.x[p % rule.n], x, j0, j1, n, jdet);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    out[d * total + i] = x[d];
+    out[(4 + d) * total + i] = n[d];
+    out[(7 + d) * total + i] = j0[d];
+    out[(10 + d) * total + i] = j1[d];
+  }
+  out[3 * total + i] = jdet;
+}
+
 template <int KER, int OP, int NBT, int NBS, bool SING>
 __global__ void __launch_bounds__(kThreads)
     quad_pairs(QuadCells test, const int* __restrict__ tdofs, QuadCells trial,
@@ -105,8 +130,10 @@ __global__ void __launch_bounds__(kThreads)
   }
   if (sc < trial_lo || sc >= trial_hi) return;  // warp-uniform
   QuadCell X, Y;
-  load_quad(test, tc, X);
-  load_quad(trial, sc, Y);
+  if (SING) {
+    load_quad(test, tc, X);
+    load_quad(trial, sc, Y);
+  }
 
   double acc_re[NBT][NBS], acc_im[NBT][NBS];
 #pragma unroll
@@ -114,8 +141,16 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
     for (int b = 0; b < NBS; ++b) acc_re[a][b] = acc_im[a][b] = 0.0;
 
+  // fields of the precomputed regular points each operator reads
+  constexpr bool kXN = OP == kADL || (OP == kHS && kC);
+  constexpr bool kYN = OP == kDL || (OP == kHS && kC);
+  constexpr bool kJ = OP == kHS;
+  const int m = rule.n * rule.n;  // regular points per cell
+  const int64_t tstride = static_cast<int64_t>(test.ncells) * m;
+  const int64_t sstride = static_cast<int64_t>(trial.ncells) * m;
   for (int ii = lane; ii < npts; ii += 32) {
     double xs, xt, ys, yt, wt;
+    double x[3], xj0[3], xj1[3], xn[3], xjd, y[3], yj0[3], yj1[3], yn[3], yjd;
     if (SING) {
       const int i = off + ii;
       xs = __ldg(srules.test_xi + 2 * i);
@@ -123,19 +158,36 @@ __global__ void __launch_bounds__(kThreads)
       ys = __ldg(srules.trial_xi + 2 * i);
       yt = __ldg(srules.trial_xi + 2 * i + 1);
       wt = __ldg(srules.w + i);
+      quad_point(X, xs, xt, x, xj0, xj1, xn, xjd);
+      quad_point(Y, ys, yt, y, yj0, yj1, yn, yjd);
     } else {
-      // ii = ((test s * n + test t) * n + trial s) * n + trial t
+      // ii = test point * m + trial point; point p = (s index) * n + (t index)
       const int n = rule.n;
-      const int q1 = ii % n, q0 = (ii / n) % n, p1 = (ii / (n * n)) % n, p0 = ii / (n * n * n);
+      const int p = ii / m, q = ii - p * m;
+      const int p0 = p / n, p1 = p - p0 * n, q0 = q / n, q1 = q - q0 * n;
       xs = rule.x[p0];
       xt = rule.x[p1];
       ys = rule.x[q0];
       yt = rule.x[q1];
       wt = rule.w[p0] * rule.w[p1] * rule.w[q0] * rule.w[q1];
+      const double* tg = test.qgeom + static_cast<int64_t>(tc) * m + p;
+      const double* sg = trial.qgeom + static_cast<int64_t>(sc) * m + q;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        x[c] = __ldg(tg + c * tstride);
+        y[c] = __ldg(sg + c * sstride);
+        if (kXN) xn[c] = __ldg(tg + (4 + c) * tstride);
+        if (kYN) yn[c] = __ldg(sg + (4 + c) * sstride);
+        if (kJ) {
+          xj0[c] = __ldg(tg + (7 + c) * tstride);
+          xj1[c] = __ldg(tg + (10 + c) * tstride);
+          yj0[c] = __ldg(sg + (7 + c) * sstride);
+          yj1[c] = __ldg(sg + (10 + c) * sstride);
+        }
+      }
+      xjd = __ldg(tg + 3 * tstride);
+      yjd = __ldg(sg + 3 * sstride);
     }
-    double x[3], xj0[3], xj1[3], xn[3], xjd, y[3], yj0[3], yj1[3], yn[3], yjd;
-    quad_point(X, xs, xt, x, xj0, xj1, xn, xjd);
-    quad_point(Y, ys, yt, y, yj0, yj1, yn, yjd);
     const double d[3] = {x[0] - y[0], x[1] - y[1], x[2] - y[2]};
     const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
     const double rinv = rsqrt_refined(r2);
@@ -272,6 +324,16 @@ cudaError_t launch_op(const QuadPairArgs& g, cudaStream_t stream) {
 }
 
 }  // namespace
+
+cudaError_t launch_quad_geometry(const QuadCells& cells, const QuadGaussRule& rule, double* out,
+                                 cudaStream_t stream) {
+  const int64_t total = static_cast<int64_t>(cells.ncells) * rule.n * rule.n;
+  if (total <= 0) return cudaSuccess;
+  const int64_t blocks = (total + 255) / 256;
+  if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+  quad_geometry_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(cells, rule, out);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_quad_pairs(const QuadPairArgs& g, cudaStream_t stream) {
   return g.kernel == kLaplace ? launch_op<kLaplace>(g, stream) : launch_op<kHelmholtz>(g, stream);
