@@ -22,7 +22,7 @@ import torch
 from bempp._lib import check as _check
 from bempp._lib import ffi as _ffi
 from bempp._lib import lib as _lib
-from bempp.assembly.boundary import BoundaryAssemblerOptions
+from bempp.assembly.boundary import BoundaryAssemblerOptions, check_device
 from ndelement.reference_cell import ReferenceCellType
 
 
@@ -63,7 +63,9 @@ def energy_and_gradient(points, cells, k, lam, mu, regular_points=6, singular_or
             _ffi.cast("void*", mu_d.data_ptr()), _ffi.cast("double*", out.data_ptr()),
             _ffi.cast("double*", grad.data_ptr()), _ffi.cast("void*", stream)),
             "adjoint gradient")
-        torch.cuda.synchronize(device)
+        # waits for the stream; raises if a block's tile copies timed out (its pairs
+        # would be missing from the gradient)
+        check_device(stream)
     finally:
         _lib.grid_t_free_bempp(g)
     return out[0], out[1], grad

@@ -774,6 +774,12 @@ BemppStatus bempp_helmholtz_single_layer_dp0_gradient(GridT* grid,
     BEMPP_CUDA(cudaMemcpy(tot, d_out.ptr, sizeof(tot), cudaMemcpyDeviceToHost));
     BEMPP_CUDA(cudaMemcpy(grad_points, d_grad.ptr, sizeof(double) * 3 * np,
                           cudaMemcpyDeviceToHost));
+    unsigned n = 0;
+    BEMPP_CUDA(take_stage_timeouts(&n));
+    if (n)
+      throw Error(kIncomplete, std::to_string(n) +
+                                   " tile blocks timed out staging their input; the gradient "
+                                   "misses their pairs");
     *value = tot[0];
     *grad_k = tot[1];
   });

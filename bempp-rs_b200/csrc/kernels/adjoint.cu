@@ -18,7 +18,9 @@
 // last kernel scatters the per-cell-vertex gradients to the vertices.
 //
 // Regular pairs use the tiled mapping of regular.cu (32 x 32 cell tiles, lane = test
-// cell); adjacent pairs use one warp per pair over their Duffy rule.  FP64, or mixed:
+// cell, both tiles staged in shared memory by TMA bulk copies on an mbarrier with the
+// regular kernels' bounded wait and timeout counter); adjacent pairs use one warp per pair
+// over their Duffy rule.  FP64, or mixed:
 // far pairs (centroid distance >= 2 diameters) in FP32 with centroid-relative points and
 // the reference phase e^{ik r0} folded into the pair weight, as in regular.cu.
 #include "launch.h"
@@ -47,7 +49,8 @@ template <int QT, bool MIXED>
 __global__ void __launch_bounds__(kThreads, 3)
     adjoint_sl_regular(CellSet cs, RegularRule rule, double k, const double2* __restrict__ lam,
                        const double2* __restrict__ mu, double* __restrict__ grad_cell,
-                       double* __restrict__ totals) {
+                       double* __restrict__ totals, unsigned* __restrict__ stage_timeouts,
+                       int stage_polls) {
   const int Q = QT > 0 ? QT : rule.npts;
   // A_ij = A_ji on far pairs (one cell set and one rule on both sides), so only tile pairs
   // tx >= sy are visited; an off-diagonal tile takes c_ij + c_ji for both orders of its pairs
@@ -58,16 +61,32 @@ __global__ void __launch_bounds__(kThreads, 3)
   const int ti0 = tx * kTile, sj0 = sy * kTile;
   const int nti = min(kTile, cs.ncells - ti0), nsj = min(kTile, cs.ncells - sj0);
   extern __shared__ __align__(16) unsigned char smem[];
-  unsigned char* cursor = smem;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem);  // completion of the tile copies
+  unsigned char* cursor = smem + 16;
   const Tile T = carve_tile(cursor, Q, MIXED, 1);
   const Tile S = carve_tile(cursor, Q, MIXED, 1);
   double* s_test = reinterpret_cast<double*>(cursor);  // [kTile][9] test-cell gradients
   double* s_trial = s_test + kTile * 9;                // [kTile][9] trial-cell gradients
   double* s_tot = s_trial + kTile * 9;                 // J, dJ/dk
-  for (int e = threadIdx.x; e < 2 * kTile * 9 + 2; e += kThreads) s_test[e] = 0.0;
-  load_tile(T, cs, ti0, nti, Q, MIXED, nullptr, 1);
-  load_tile(S, cs, sj0, nsj, Q, MIXED, nullptr, 1);
+  // both tiles by bulk (TMA) copies on one mbarrier, issued by one thread, while the
+  // others clear the gradient accumulators
+  if (threadIdx.x == 0) mbar_init(mbar, 1);
   __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(mbar, 2 * bulk_tile_bytes(Q, MIXED));
+    stage_tile_bulk(T, cs, ti0, Q, MIXED, mbar);
+    stage_tile_bulk(S, cs, sj0, Q, MIXED, mbar);
+  }
+  for (int e = threadIdx.x; e < 2 * kTile * 9 + 2; e += kThreads) s_test[e] = 0.0;
+  const bool staged = mbar_wait_bounded(mbar, 0, stage_polls);
+  if (__syncthreads_or(!staged)) {
+    // the copies did not complete in time: record it, give them a last bounded wait and
+    // add nothing (the host reports the failure)
+    if (threadIdx.x == 0) atomicAdd(stage_timeouts, 1u);
+    mbar_wait_bounded(mbar, 0);
+    return;
+  }
 
   const int it = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool valid = it < nti;
@@ -449,9 +468,13 @@ cudaError_t launch_adjoint_sl(const CellSet& cs, const RegularRule& rule,
     return e;
   if ((e = cudaMemsetAsync(totals, 0, sizeof(double) * 2, stream)) != cudaSuccess) return e;
   if (cs.ncells <= 0) return cudaSuccess;
-  const size_t smem = 2 * (sizeof(double) * tile_doubles(rule.npts) +
+  const size_t smem = 16 /* mbarrier */ +
+                      2 * (sizeof(double) * tile_doubles(rule.npts) +
                            sizeof(float) * tile_floats(rule.npts, mixed) + sizeof(int) * tile_ints(1) + 16) +
                       sizeof(double) * (2 * kTile * 9 + 2) + 16;
+  unsigned* timeouts = nullptr;
+  int polls = 0;
+  if ((e = stage_wait_state(&timeouts, &polls)) != cudaSuccess) return e;
   const long long ntt = (cs.ncells + kTile - 1) / kTile;
   if (ntt * (ntt + 1) / 2 > 0x7fffffffLL) return cudaErrorInvalidValue;
   const dim3 grid(static_cast<unsigned>(ntt * (ntt + 1) / 2));  // tile pairs tx >= sy
@@ -460,7 +483,7 @@ cudaError_t launch_adjoint_sl(const CellSet& cs, const RegularRule& rule,
   auto fn = rule.npts == 6 ? (mixed ? adjoint_sl_regular<6, true> : adjoint_sl_regular<6, false>)
                            : (mixed ? adjoint_sl_regular<0, true> : adjoint_sl_regular<0, false>);
   cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  fn<<<grid, kThreads, smem, stream>>>(cs, rule, k, l2, m2, grad_cell, totals);
+  fn<<<grid, kThreads, smem, stream>>>(cs, rule, k, l2, m2, grad_cell, totals, timeouts, polls);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (pairs.npairs > 0) {
     adjoint_sl_singular<<<(pairs.npairs + 7) / 8, 256, 0, stream>>>(cs, rules, pairs, k, l2, m2,

@@ -17,6 +17,9 @@ cudaError_t take_stage_timeouts(unsigned* count);
 // Polls of the regular kernels' first wait for their tile copies on the current device
 // (default kStagePolls; a test hook: 0 makes every block give up and write nothing).
 cudaError_t set_stage_poll_limit(int polls);
+// Device address of the timeout counter and the current first-wait poll limit, for kernels
+// of other files that stage tiles the same way (the adjoint gradient's regular kernel).
+cudaError_t stage_wait_state(unsigned** counter, int* polls);
 
 // Per-cell FP64 geometry, regular quadrature points and vertex ids of a flat-triangle
 // grid (points: npoints x 3 FP64; cells: ncells x 3 int32 point indices; topo: ncells x 3

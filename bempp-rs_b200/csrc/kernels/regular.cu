@@ -1468,8 +1468,18 @@ cudaError_t dispatch(const CellSet& test, const SpaceTiles& tt, const CellSet& t
 
 int scatter_tile_cells() { return kTile; }
 
+namespace {
+int g_host_poll_limit = tiles::kStagePolls;  // host copy of g_stage_poll_limit
+}  // namespace
+
 cudaError_t set_stage_poll_limit(int polls) {
+  g_host_poll_limit = polls;
   return cudaMemcpyToSymbol(g_stage_poll_limit, &polls, sizeof(int));
+}
+
+cudaError_t stage_wait_state(unsigned** counter, int* polls) {
+  *polls = g_host_poll_limit;
+  return cudaGetSymbolAddress(reinterpret_cast<void**>(counter), g_stage_timeouts);
 }
 
 cudaError_t take_stage_timeouts(unsigned* count) {

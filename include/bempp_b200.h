@@ -327,7 +327,9 @@ BemppStatus bempp_helmholtz_single_layer_dp0_gradient(GridT *grid,
                                                       const void *mu, double *value,
                                                       double *grad_k, double *grad_points);
 /* Addition: the same with device pointers, enqueued on `stream`; value_and_grad_k holds
- * {J, dJ/dk}. */
+ * {J, dJ/dk}.  Its tile copies have the bounded wait of the assembly kernels: the host
+ * version returns BemppStatus_Incomplete if one gave up, and after this one
+ * bempp_device_status(stream) does. */
 BemppStatus bempp_helmholtz_single_layer_dp0_gradient_device(
     GridT *grid, const BoundaryAssemblerOptionsT *options, double k, const void *lambda,
     const void *mu, double *value_and_grad_k, double *grad_points, void *stream);

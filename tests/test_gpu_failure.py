@@ -6,7 +6,8 @@ wait to zero, so every block gives up at once: it records the failure in a devic
 counter, drains its copies with a second full-length wait and returns without writing.
 The device entry point must then report BemppStatus_Incomplete through
 bempp_device_status (and leave the output untouched), the host entry point must raise,
-and once the limit is back the next assembly must match the FP64 oracle.
+and once the limit is back the next assembly must match the FP64 oracle.  The adjoint
+gradient's regular kernel stages its tiles the same way and reports the same way.
 """
 
 import numpy as np
@@ -101,3 +102,23 @@ def test_check_device_raises_after_a_wait_that_ran_out(stage_polls):
     with pytest.raises(RuntimeError, match="timed out"):
         a.assemble_into_device(trial, test, out, None, check=True)
     check_device(None)  # the count was taken by the failed check
+
+
+def test_adjoint_gradient_reports_a_wait_that_ran_out(stage_polls):
+    import torch
+
+    from bempp.autograd import energy_and_gradient
+
+    pts, cells = shapes.icosphere(2)
+    pts = shapes.radial_perturbation(pts, seed=8)
+    rng = np.random.default_rng(1)
+    lam = rng.standard_normal(len(cells)) + 1j * rng.standard_normal(len(cells))
+    mu = rng.standard_normal(len(cells)) + 1j * rng.standard_normal(len(cells))
+    j0, dk0, g0 = energy_and_gradient(pts, cells, 2.0, lam, mu)
+    stage_polls(0)
+    with pytest.raises(RuntimeError, match="timed out"):
+        energy_and_gradient(pts, cells, 2.0, lam, mu)
+    stage_polls(DEFAULT_POLLS)
+    j1, dk1, g1 = energy_and_gradient(pts, cells, 2.0, lam, mu)
+    assert float(j1) == float(j0) or abs(float(j1) - float(j0)) <= 1e-12 * abs(float(j0))
+    assert torch.allclose(g1, g0, rtol=1e-12, atol=1e-12 * float(g0.abs().max()))
