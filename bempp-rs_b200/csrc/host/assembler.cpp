@@ -422,6 +422,12 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
   ra.same_grid = same_grid ? 1 : 0;
   // one space on both sides and a symmetric kernel: lower-triangle tile pairs, mirrored
   ra.symmetric = (&trial == &test && same_grid && (a.op == kSL || a.op == kHS)) ? 1 : 0;
+  // one P1 / DP1 space, Laplace double layer or its adjoint, FP64, 6-point rule: the pair
+  // (i, j) and the pair (j, i) share their kernel values, so both blocks of a tile pair
+  // come from one pass
+  if (&trial == &test && same_grid && a.kernel == kLaplace && (a.op == kDL || a.op == kADL) &&
+      a.options.precision != 1 && test.nbasis == 3 && rule.npts == 6)
+    ra.symmetric = 2;
   ra.precision = a.options.precision == 1 ? kRegularMixed : kRegularFP64;
   ra.out_type = cplx ? kOutC128 : kOutF64;
   ra.ld = nt;

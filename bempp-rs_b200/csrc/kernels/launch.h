@@ -61,8 +61,10 @@ struct RegularArgs {
   int small_phase = 0;   // Helmholtz, mixed: k (max rad_test + max rad_trial) <= 0.8, so
                          // |k (r - r0)| <= 0.8 for every far pair (no phase reduction)
   NearArgs near{};       // mixed: near field (null: near pairs found per pair in the kernel)
-  int symmetric = 0;     // test and trial are one space and the operator is symmetric (SL,
-                         // HS): only tile pairs (tx >= sy) are computed, then mirrored
+  int symmetric = 0;     // 1: test and trial are one space and the operator is symmetric
+                         // (SL, HS): only tile pairs (tx >= sy) are computed, then mirrored;
+                         // 2: one P1 / DP1 space, Laplace DL or ADL, FP64, 6-point rule:
+                         // tile pairs (tx >= sy), each integrated in both orders
   int trial_tile0 = 0;   // first trial tile of this launch
   int trial_tiles = 0;   // trial tiles of this launch (0: all from trial_tile0 on)
 };

@@ -327,6 +327,84 @@ __device__ __forceinline__ void block_fp64(const Tile& T, int it, const Tile& S,
     block_fp64_pq<QT, KER, OP, NBT, NBS, kUnroll, FPH>(T, it, S, js, rule, k, ore, oim);
 }
 
+// Laplace double layer of a cell pair in both orders, FP64, for one P1 / DP1 space on both
+// sides (the same rule on both cells): from one 1/r^3 per point pair (x_p in cell i of the
+// test tile, y_q in cell j of the trial tile)
+//   dij[a][b] = DL(test i, trial j)_ab = sum_p w_p phi_a(p) (x_p - y).n_j sum_q w_q phi_b(q) / r^3
+//   dji[a][b] = DL(test j, trial i)_ba = sum_q w_q phi_b(q) (y_q - x).n_i sum_p w_p phi_a(p) / r^3
+// ((x - y).n is constant over the plane of the normal's cell, in the tangent coordinates of
+// block_fp64_pq).  The adjoint double layer is the same pair of blocks swapped:
+// ADL(i, j)_ab = DL(j, i)_ba.  Q = 6 keeps the per-trial-point sums in registers.
+template <int Q>
+__device__ __forceinline__ void block_fp64_dl_pair(const Tile& T, int it, const Tile& S, int js,
+                                                   const RegularRule& rule, double dij[3][3],
+                                                   double dji[3][3]) {
+  static_assert(Q > 0, "the paired double layer needs a compile-time rule size");
+  const double dcx = T.G(fCx, it) - S.G(fCx, js), dcy = T.G(fCy, it) - S.G(fCy, js),
+               dcz = T.G(fCz, it) - S.G(fCz, js);
+  const double njx = S.G(fNx, js), njy = S.G(fNy, js), njz = S.G(fNz, js);
+  const double nix = T.G(fNx, it), niy = T.G(fNy, it), niz = T.G(fNz, it);
+  // (x_p - y).n_j = dc.n_j + u_p t0_i.n_j + v_p t1_i.n_j
+  const double f0 = dcx * njx + dcy * njy + dcz * njz;
+  const double f1 = T.G(fT0x, it) * njx + T.G(fT0y, it) * njy + T.G(fT0z, it) * njz;
+  const double f2 = T.G(fT1x, it) * njx + T.G(fT1y, it) * njy + T.G(fT1z, it) * njz;
+  // (y_q - x).n_i = -dc.n_i + u_q t0_j.n_i + v_q t1_j.n_i
+  const double g0 = -(dcx * nix + dcy * niy + dcz * niz);
+  const double g1 = S.G(fT0x, js) * nix + S.G(fT0y, js) * niy + S.G(fT0z, js) * niz;
+  const double g2 = S.G(fT1x, js) * nix + S.G(fT1y, js) * niy + S.G(fT1z, js) * niz;
+  double bij[3][3], bji[3][3];
+  double wsum[Q][3];  // sum_p w_p phi_a(p) / r_pq^3 per trial point q
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) bij[a][b] = bji[a][b] = 0.0;
+#pragma unroll
+  for (int q = 0; q < Q; ++q) wsum[q][0] = wsum[q][1] = wsum[q][2] = 0.0;
+#pragma unroll 1
+  for (int p = 0; p < Q; ++p) {
+    const double x0 = T.P(p, 0, it), x1 = T.P(p, 1, it), x2 = T.P(p, 2, it);
+    const double c0 = rule.wphi[0][p], c1 = rule.wphi[1][p], c2 = rule.wphi[2][p];
+    double u0 = 0.0, u1 = 0.0, u2 = 0.0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const double dx = x0 - S.P(q, 0, js), dy = x1 - S.P(q, 1, js), dz = x2 - S.P(q, 2, js);
+      const double kern = rinv3_refined(dx * dx + dy * dy + dz * dz);
+      u0 = fma(kern, rule.wphi[0][q], u0);
+      u1 = fma(kern, rule.wphi[1][q], u1);
+      u2 = fma(kern, rule.wphi[2][q], u2);
+      wsum[q][0] = fma(kern, c0, wsum[q][0]);
+      wsum[q][1] = fma(kern, c1, wsum[q][1]);
+      wsum[q][2] = fma(kern, c2, wsum[q][2]);
+    }
+    const double ap = fma(rule.u[p], f1, fma(rule.v[p], f2, f0));
+    const double e[3] = {c0 * ap, c1 * ap, c2 * ap};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      bij[a][0] = fma(e[a], u0, bij[a][0]);
+      bij[a][1] = fma(e[a], u1, bij[a][1]);
+      bij[a][2] = fma(e[a], u2, bij[a][2]);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const double bq = fma(rule.u[q], g1, fma(rule.v[q], g2, g0));
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      const double e = rule.wphi[b][q] * bq;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) bji[a][b] = fma(e, wsum[q][a], bji[a][b]);
+    }
+  }
+  const double sc = T.G(fJdet, it) * S.G(fJdet, js) * kInv4Pi;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      dij[a][b] = bij[a][b] * sc;
+      dji[a][b] = bji[a][b] * sc;
+    }
+}
+
 // Per-pair constants of the FP32 far-pair quadrature.
 template <int QT>
 struct FarPair {
@@ -718,17 +796,26 @@ enum NearMode : int { kNearInKernel = 0, kNearMasked = 1 };
 // Resident CTAs per SM the register allocation must allow: 5 for the FP64 Laplace
 // hypersingular kernel (it fits in 96 registers without spills), 6 for the mixed
 // Helmholtz DP0 kernels (80 registers; with no FP64 points in their tiles six CTAs also
-// fit in shared memory), 4 elsewhere.
-template <int KER, int OP, bool MIXED, bool DIRECT>
+// fit in shared memory), 4 elsewhere (the paired double layer too: at 128 registers it
+// spills about 100 bytes, and is still 1.5 % faster than at 3 CTAs with 168).
+template <int KER, int OP, bool MIXED, bool DIRECT, bool PAIRED = false>
 constexpr int min_ctas() {
   return (KER == kLaplace && OP == kHS && !MIXED) ? 5 : (MIXED && DIRECT && KER == kHelmholtz) ? 6 : 4;
 }
 
-template <int QT, int KER, int OP, int NBT, int NBS, bool MIXED, bool DIRECT, int PH, int NM>
-__global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT>())
+// PAIRED (Laplace DL / ADL, FP64, one P1 / DP1 space on both sides, Q = 6): the tile
+// pairs tx >= sy, each off-diagonal one integrated in both orders from one evaluation of
+// the kernel per point pair (block_fp64_dl_pair), the (sy, tx) blocks accumulated
+// separately and added at the transposed entries.
+template <int QT, int KER, int OP, int NBT, int NBS, bool MIXED, bool DIRECT, int PH, int NM,
+          bool PAIRED = false>
+__global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAIRED>())
     regular_tiles(CellSet test, SpaceTiles tt, CellSet trial, SpaceTiles st, RegularRule rule,
                   double k, int same_grid, double* __restrict__ out, int64_t ld, int tile_y0,
                   int tile_y1, NearArgs near, int symmetric) {
+  static_assert(!PAIRED || (KER == kLaplace && (OP == kDL || OP == kADL) && NBT == 3 &&
+                            NBS == 3 && !MIXED && !DIRECT && QT == 6),
+                "paired blocks: Laplace DL / ADL, FP64, P1 / DP1, 6-point rule");
   constexpr bool kC = KER == kHelmholtz;
   constexpr bool kQueue = MIXED && NM == kNearInKernel;
   constexpr bool kRel = MIXED;  // FP32 offsets staged
@@ -740,7 +827,7 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT>())
   // real FP64 P1 blocks (not the hypersingular kernel, which keeps 5 CTAs per SM; not the
   // mixed kernels, whose larger tiles would then limit the CTAs per SM): one accumulator
   // per warp, updated with plain adds, summed at the flush
-  constexpr int kAcc = (kGather && !kC && !MIXED && OP != kHS) ? kWarps : 1;
+  constexpr int kAcc = (kGather && !kC && !MIXED && OP != kHS && !PAIRED) ? kWarps : 1;
   const int Q = QT > 0 ? QT : rule.npts;
   // symmetric operator on one space (single layer, hypersingular): only the tile pairs with
   // tx >= sy are computed, the blocks with tx > sy also written transposed
@@ -774,6 +861,9 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT>())
     acc_im = acc_re + cap;
     cursor += sizeof(double) * cap * (kC ? 2 : 1) * kAcc;
   }
+  // PAIRED: the (sy, tx) blocks, indexed as acc_re (test-tile DOF + ndt * trial-tile DOF)
+  double* acc_t = reinterpret_cast<double*>(cursor);
+  if (PAIRED) cursor += sizeof(double) * cap;
   double* stage_re = nullptr;  // kGather: [warp][(a * NBS + b) * kTile + lane]
   double* stage_im = nullptr;
   uint8_t* inc_off = nullptr;  // kGather: the test tile's DOF incidence
@@ -812,6 +902,8 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT>())
         acc_re[w * cap + idx] = 0.0;
         if (kC) acc_im[idx] = 0.0;
       }
+    if (PAIRED)
+      for (int idx = threadIdx.x; idx < ndt * nds; idx += kThreads) acc_t[idx] = 0.0;
     load_ldof(T, ti0, nti, tt.cell_ldof, NBT);
     load_ldof(S, sj0, nsj, st.cell_ldof, NBS);
     if (kGather)
@@ -842,6 +934,7 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT>())
   }
   for (int js = warp; js < nsj; js += kWarps) {  // warp-uniform trip count
     double ore[NBT][NBS], oim[NBT][NBS];
+    double otr[NBT][NBS];  // PAIRED: the (sy, tx) block, [test-tile basis][trial-tile basis]
     bool have = false;
     if (lane_cell) {
       const int64_t o = static_cast<int64_t>(sj0 + js) * ld + ti0 + it;
@@ -864,11 +957,22 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT>())
         const int slot = atomicAdd(qcount, 1);
         queue[slot] = static_cast<unsigned short>(it | (js << 8));
       } else {
-        if (MIXED)
+        if constexpr (PAIRED) {
+#pragma unroll
+          for (int a = 0; a < NBT; ++a)
+#pragma unroll
+            for (int b = 0; b < NBS; ++b) oim[a][b] = 0.0;  // real blocks
+          // DL: (i, j) block here, (j, i) at the transposed entries; ADL: swapped
+          if (OP == kDL)
+            block_fp64_dl_pair<QT>(T, it, S, js, rule, ore, otr);
+          else
+            block_fp64_dl_pair<QT>(T, it, S, js, rule, otr, ore);
+        } else if (MIXED) {
           block_fp32<QT, KER, OP, NBT, NBS, PH>(T, it, S, js, rule, k, ore, oim);
-        else
+        } else {
           block_fp64<QT, KER, OP, NBT, NBS, true,
                      PH == kPhaseSmall ? kF64Referenced : kF64Sincos>(T, it, S, js, rule, k, ore, oim);
+        }
         have = true;
         if (DIRECT) {
           if (kC)
@@ -881,14 +985,17 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT>())
         }
       }
     }
-    if (kGather) {
+    // PAIRED off the diagonal: a second pass gathers the (sy, tx) blocks into acc_t
+#pragma unroll 1
+    for (int pass = 0; pass < ((PAIRED && mirror) ? 2 : (kGather ? 1 : 0)); ++pass) {
       double* sr = stage_re + warp * (kTile * NBT * NBS);
       double* si = stage_im + warp * (kTile * NBT * NBS);
+      double* acc = pass == 0 ? acc_re : acc_t;
 #pragma unroll
       for (int a = 0; a < NBT; ++a)
 #pragma unroll
         for (int b = 0; b < NBS; ++b) {
-          sr[(a * NBS + b) * kTile + it] = have ? ore[a][b] : 0.0;
+          sr[(a * NBS + b) * kTile + it] = have ? (pass == 0 ? ore[a][b] : otr[a][b]) : 0.0;
           if (kC) si[(a * NBS + b) * kTile + it] = have ? oim[a][b] : 0.0;
         }
       __syncwarp();
@@ -909,9 +1016,9 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT>())
         for (int b = 0; b < NBS; ++b) {
           const int idx = d + ndt * S.ldof[b * kTile + js];
           if (kAcc > 1) {
-            acc_re[warp * cap + idx] += g_re[b];  // this warp's copy; distinct per lane
+            acc[warp * cap + idx] += g_re[b];  // this warp's copy; distinct per lane
           } else {
-            atomicAdd(acc_re + idx, g_re[b]);
+            atomicAdd(acc + idx, g_re[b]);
             if (kC) atomicAdd(acc_im + idx, g_im[b]);
           }
         }
@@ -977,6 +1084,9 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT>())
             atomicAdd(out + 2 * om + 1, im);
           }
         }
+      } else if (PAIRED) {
+        if (re != 0.0) atomicAdd(out + o, re);
+        if (mirror && acc_t[idx] != 0.0) atomicAdd(out + om, acc_t[idx]);
       } else if (re != 0.0) {
         atomicAdd(out + o, re);
         if (mirror) atomicAdd(out + om, re);
@@ -1314,15 +1424,21 @@ size_t smem_bytes(int q, bool rel, bool queue, bool direct, bool cplx, int max_t
   return b + 16;
 }
 
-template <int QT, int KER, int OP, int NBT, int NBS, bool MIXED, bool DIRECT, int PH, int NM>
+template <int QT, int KER, int OP, int NBT, int NBS, bool MIXED, bool DIRECT, int PH, int NM,
+          bool PAIRED = false>
 cudaError_t launch_mode(const CellSet& test, const SpaceTiles& tt, const CellSet& trial,
                         const SpaceTiles& st, const RegularRule& rule, const RegularArgs& a,
                         int ty0, int ty1, cudaStream_t stream) {
-  constexpr int kAcc = (!DIRECT && NBT == 3 && KER != kHelmholtz && !MIXED && OP != kHS) ? kWarps : 1;
+  // accumulator copies: one per warp for the real FP64 P1 blocks; PAIRED: one for the
+  // (tx, sy) and one for the (sy, tx) blocks
+  constexpr int kAcc = PAIRED ? 2
+                              : (!DIRECT && NBT == 3 && KER != kHelmholtz && !MIXED && OP != kHS)
+                                    ? kWarps
+                                    : 1;
   const size_t smem = smem_bytes(rule.npts, MIXED, MIXED && NM == kNearInKernel, DIRECT,
                                  KER == kHelmholtz, tt.max_tile_dofs, st.max_tile_dofs, NBT, NBS,
                                  kAcc, a.symmetric != 0, !MIXED || NM == kNearInKernel);
-  auto fn = regular_tiles<QT, KER, OP, NBT, NBS, MIXED, DIRECT, PH, NM>;
+  auto fn = regular_tiles<QT, KER, OP, NBT, NBS, MIXED, DIRECT, PH, NM, PAIRED>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
@@ -1376,6 +1492,16 @@ cudaError_t launch_one(const CellSet& test, const SpaceTiles& tt, const CellSet&
   if (ny <= 0) return cudaSuccess;
   const int ty0 = a.trial_tile0, ty1 = a.trial_tile0 + ny;
   if constexpr (!MIXED) {
+    if (a.symmetric == 2) {
+      // one P1 / DP1 space, Laplace DL / ADL: both orders of each pair from one kernel
+      // evaluation (the host asks for it only there)
+      if constexpr (KER == kLaplace && (OP == kDL || OP == kADL) && NBT == 3 && NBS == 3 &&
+                    !DIRECT && QT == 6)
+        return launch_mode<QT, KER, OP, NBT, NBS, false, DIRECT, kPhaseSmall, kNearInKernel, true>(
+            test, tt, trial, st, rule, a, ty0, ty1, stream);
+      else
+        return cudaErrorInvalidValue;
+    }
     // FP64 Helmholtz: phases referenced to the pair (kPhaseSmall) when the host's bound
     // allows it, else CUDA's sincos of every phase
     if (KER == kHelmholtz && !a.small_phase)

@@ -182,11 +182,16 @@ def test_singular_csr_matches_dense():
     ("laplace", "hypersingular", 0.0, (1, True)),
     ("helmholtz", "single_layer", 5.0, (0, False)),
     ("helmholtz", "hypersingular", 5.0, (1, True)),
+    ("laplace", "double_layer", 0.0, (1, True)),
+    ("laplace", "adjoint_double_layer", 0.0, (1, True)),
+    ("laplace", "double_layer", 0.0, (1, False)),
+    ("laplace", "adjoint_double_layer", 0.0, (1, False)),
 ])
 def test_one_space_symmetric_operators_match_oracle(kernel, op, k, sp):
-    """Single layer and hypersingular on one space object: only tile pairs (tx >= sy) are
-    computed and the rest is mirrored; the matrix matches the oracle (which computes every
-    pair; its far-pair entries are symmetric to rounding)."""
+    """Operators on one space object.  Single layer and hypersingular: only tile pairs
+    (tx >= sy) are computed and the rest is mirrored.  Laplace double layer and its adjoint
+    on P1 / DP1: tile pairs (tx >= sy), each integrated in both orders from one kernel
+    evaluation per point pair.  The matrix matches the oracle, which computes every pair."""
     pts, cells = shapes.icosphere(3)
     grid = Grid(shapes.radial_perturbation(pts, seed=11), cells)
     a = gpu_assemble(grid, kernel, op, k, test=sp, trial=sp, one_space=True)
