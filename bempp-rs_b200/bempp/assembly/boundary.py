@@ -299,11 +299,13 @@ class BoundaryAssembler(object):
 
     def host_copy_stats(self) -> typing.Dict[str, float]:
         """Host side of the last host-memory assembly: DMA wait and host copy times (ms),
-        copy groups, assembly chunks and copy threads."""
-        buf = np.zeros(6, dtype=np.float64)
+        copy groups, assembly chunks, copy threads, page prefault time, and for page-locked
+        destinations the device time to the end of the kernels and of the last DMA."""
+        buf = np.zeros(8, dtype=np.float64)
         n = _lib.boundary_assembler_host_copy_stats(
-            self._rs_assembler, _ffi.cast("double*", buf.ctypes.data), 6)
-        keys = ("dma_wait_ms", "host_copy_ms", "groups", "chunks", "threads", "prefault_ms")
+            self._rs_assembler, _ffi.cast("double*", buf.ctypes.data), 8)
+        keys = ("dma_wait_ms", "host_copy_ms", "groups", "chunks", "threads", "prefault_ms",
+                "compute_ms", "dma_end_ms")
         return {k: float(v) for k, v in zip(keys[:n], buf[:n])}
 
     def launch_count(self) -> int:

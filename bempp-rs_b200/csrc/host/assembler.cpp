@@ -267,6 +267,21 @@ struct Timer {
   void finish() { a.events_recorded = on ? next : 0; }
 };
 
+// The side stream (and its fork / join events) of the assembler on `device`.
+void ensure_side_stream(BoundaryAssemblerT& a, int device) {
+  if (a.side && a.side_device == device) return;
+  if (a.side) {
+    cudaStreamDestroy(a.side);
+    cudaEventDestroy(a.fork_ev);
+    cudaEventDestroy(a.join_ev);
+    a.side = nullptr;
+  }
+  BEMPP_CUDA(cudaStreamCreateWithFlags(&a.side, cudaStreamNonBlocking));
+  BEMPP_CUDA(cudaEventCreateWithFlags(&a.fork_ev, cudaEventDisableTiming));
+  BEMPP_CUDA(cudaEventCreateWithFlags(&a.join_ev, cudaEventDisableTiming));
+  a.side_device = device;
+}
+
 }  // namespace
 
 int effective_chunks(const SpaceT& trial, int want) {
@@ -425,8 +440,11 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
   // one P1 / DP1 space, Laplace double layer or its adjoint, FP64, 6-point rule: the pair
   // (i, j) and the pair (j, i) share their kernel values, so both blocks of a tile pair
   // come from one pass
+  // (one-launch assemblies only: a chunked host-memory assembly keeps the full tile grid,
+  // whose columns finish evenly through the chunks and go out by DMA meanwhile, where the
+  // tx >= sy half finishes most columns only in its last chunks)
   if (&trial == &test && same_grid && a.kernel == kLaplace && (a.op == kDL || a.op == kADL) &&
-      a.options.precision != 1 && test.nbasis == 3 && rule.npts == 6)
+      a.options.precision != 1 && test.nbasis == 3 && rule.npts == 6 && nchunks == 1)
     ra.symmetric = 2;
   ra.precision = a.options.precision == 1 ? kRegularMixed : kRegularFP64;
   ra.out_type = cplx ? kOutC128 : kOutF64;
@@ -502,18 +520,7 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
     timer.mark();  // no memset phase
     const bool fork = singular && nchunks == 1 && ra.precision == kRegularMixed;
     if (fork) {
-      if (!a.side || a.side_device != device) {
-        if (a.side) {
-          cudaStreamDestroy(a.side);
-          cudaEventDestroy(a.fork_ev);
-          cudaEventDestroy(a.join_ev);
-          a.side = nullptr;
-        }
-        BEMPP_CUDA(cudaStreamCreateWithFlags(&a.side, cudaStreamNonBlocking));
-        BEMPP_CUDA(cudaEventCreateWithFlags(&a.fork_ev, cudaEventDisableTiming));
-        BEMPP_CUDA(cudaEventCreateWithFlags(&a.join_ev, cudaEventDisableTiming));
-        a.side_device = device;
-      }
+      ensure_side_stream(a, device);
       BEMPP_CUDA(cudaEventRecord(a.fork_ev, stream));
       BEMPP_CUDA(cudaStreamWaitEvent(a.side, a.fork_ev, 0));
       run_singular(0, 0x7fffffff, a.side);
@@ -551,8 +558,17 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
   } else {
     if (!empty) BEMPP_CUDA(cudaMemsetAsync(out, 0, static_cast<size_t>(nt) * ns * esize, stream));
     timer.mark();
-    // chunked: each chunk adds its regular pairs and the singular pairs of its trial cells
-    // (all adds commute), so its columns are final when it ends
+    // chunked: the whole singular part runs on a side stream beside the first chunks'
+    // regular kernels (all adds commute), and every chunk's completion also waits for it,
+    // so a chunk's columns are final when it ends
+    const bool side_singular = singular && nchunks > 1;
+    if (side_singular) {
+      ensure_side_stream(a, device);
+      BEMPP_CUDA(cudaEventRecord(a.fork_ev, stream));
+      BEMPP_CUDA(cudaStreamWaitEvent(a.side, a.fork_ev, 0));
+      run_singular(0, 0x7fffffff, a.side);
+      BEMPP_CUDA(cudaEventRecord(a.join_ev, a.side));
+    }
     for (int c = 0; c < nchunks; ++c) {
       int t0, t1;
       tile_range(c, t0, t1);
@@ -562,7 +578,7 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
         BEMPP_CUDA(launch_regular_scatter(tcs, space_tiles(test), scs, space_tiles(trial), rule,
                                           ra, stream));
         a.launches += regular_launches;
-        if (singular && nchunks > 1) run_singular(32 * t0, c + 1 == nchunks ? 0x7fffffff : 32 * t1, stream);
+        if (side_singular && c == 0) BEMPP_CUDA(cudaStreamWaitEvent(stream, a.join_ev, 0));
       }
       if (nchunks == 1) {
         timer.mark();
@@ -835,6 +851,8 @@ BoundaryAssemblerT::~BoundaryAssemblerT() {
   if (stream) cudaStreamDestroy(stream);
   if (copy_stream) cudaStreamDestroy(copy_stream);
   for (auto e : chunk_ev) cudaEventDestroy(e);
+  for (auto e : copy_timing)
+    if (e) cudaEventDestroy(e);
   if (side) {
     cudaStreamDestroy(side);
     cudaEventDestroy(fork_ev);

@@ -240,14 +240,17 @@ struct BoundaryAssemblerT {
   cudaStream_t stream = nullptr;  // host-memory assembly stream (created on first use)
   cudaStream_t copy_stream = nullptr;     // page-locked destinations: direct DMA stream
   std::vector<cudaEvent_t> chunk_ev;      // and its per-chunk events
-  // side stream and fork / join events: the singular kernel of a mixed-precision DP0
-  // assembly runs beside the regular kernels (created on first use, on side_device)
+  // side stream and fork / join events: the singular kernel of a one-chunk mixed-precision
+  // DP0 assembly, and of a chunked non-DP0 one, runs beside the regular kernels (created on
+  // first use, on side_device)
   cudaStream_t side = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   int side_device = -1;
   // last host-memory assembly: ms waiting for DMA, ms of host copy, copy groups, chunks,
-  // host copy threads, ms of destination page prefaulting
-  std::array<double, 6> host_copy_stats{};
+  // host copy threads, ms of destination page prefaulting, device ms to the end of the
+  // last chunk's kernels and to the end of the last DMA (page-locked destinations)
+  std::array<double, 8> host_copy_stats{};
+  cudaEvent_t copy_timing[3] = {nullptr, nullptr, nullptr};  // start, compute end, DMA end
   DeviceBuffer convert;  // FP64 staging for F32 / C32 outputs
   DeviceBuffer pair_values;
   std::mutex mu;

@@ -296,6 +296,8 @@ void assemble_host(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* dat
       BEMPP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
       a.chunk_ev.push_back(e);
     }
+    for (auto& e : a.copy_timing)
+      if (!e) BEMPP_CUDA(cudaEventCreate(&e));
     struct Drain {
       cudaStream_t s0, s1;
       ~Drain() {
@@ -303,9 +305,11 @@ void assemble_host(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* dat
         cudaStreamSynchronize(s1);
       }
     } drain{a.stream, a.copy_stream};
+    BEMPP_CUDA(cudaEventRecord(a.copy_timing[0], a.stream));
     assemble_device(a, trial, test, a.work.ptr, a.stream, nchunks, [&](int c) {
       BEMPP_CUDA(cudaEventRecord(a.chunk_ev[c], a.stream));
     });
+    BEMPP_CUDA(cudaEventRecord(a.copy_timing[1], a.stream));
     const char* src = static_cast<const char*>(a.work.ptr);
     size_t ncopies = 0;
     // Runs of a chunk whose gap is at most kMergeGap columns go in one DMA: a gap column
@@ -332,11 +336,15 @@ void assemble_host(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* dat
         r = q;
       }
     }
+    BEMPP_CUDA(cudaEventRecord(a.copy_timing[2], a.copy_stream));
     BEMPP_CUDA(cudaStreamSynchronize(a.copy_stream));
     BEMPP_CUDA(cudaStreamSynchronize(a.stream));
     check_stage_timeouts();
+    float compute_ms = 0.f, dma_ms = 0.f;
+    BEMPP_CUDA(cudaEventElapsedTime(&compute_ms, a.copy_timing[0], a.copy_timing[1]));
+    BEMPP_CUDA(cudaEventElapsedTime(&dma_ms, a.copy_timing[0], a.copy_timing[2]));
     a.host_copy_stats = {0.0, 0.0, static_cast<double>(ncopies), static_cast<double>(nchunks),
-                         0.0, 0.0};
+                         0.0, 0.0, compute_ms, dma_ms};
     return;
   }
   const std::vector<Group> groups = plan_groups(runs, col_bytes);

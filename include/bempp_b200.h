@@ -183,7 +183,9 @@ size_t boundary_assembler_last_launch_count(BoundaryAssemblerT *assembler);
  * assembly (boundary_assembler_assemble_into_memory[_ex] / boundary_assembler_assemble):
  * [ms the host waited for device-to-host DMA, ms of host copies into the caller's array,
  * copy groups, assembly chunks, host copy threads, ms spent taking the destination's page
- * faults ahead of the copies]; returns the number written (<= n). */
+ * faults ahead of the copies, device ms from the first launch to the end of the last
+ * chunk's kernels and to the end of the last DMA (page-locked destinations, else 0)];
+ * returns the number written (<= n). */
 size_t boundary_assembler_host_copy_stats(BoundaryAssemblerT *assembler, double *out, size_t n);
 /* Addition: off-surface potential operators, the single and double layer potentials of
  * the assembler's kernel (OperatorType SingleLayer or DoubleLayer; others fail with
