@@ -812,7 +812,7 @@ template <int QT, int KER, int OP, int NBT, int NBS, bool MIXED, bool DIRECT, in
 __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAIRED>())
     regular_tiles(CellSet test, SpaceTiles tt, CellSet trial, SpaceTiles st, RegularRule rule,
                   double k, int same_grid, double* __restrict__ out, int64_t ld, int tile_y0,
-                  int tile_y1, NearArgs near, int symmetric) {
+                  int tile_y1, NearArgs near, int symmetric, int acc_copies) {
   static_assert(!PAIRED || (KER == kLaplace && (OP == kDL || OP == kADL) && NBT == 3 &&
                             NBS == 3 && !MIXED && !DIRECT && QT == 6),
                 "paired blocks: Laplace DL / ADL, FP64, P1 / DP1, 6-point rule");
@@ -827,7 +827,10 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAI
   // real FP64 P1 blocks (not the hypersingular kernel, which keeps 5 CTAs per SM; not the
   // mixed kernels, whose larger tiles would then limit the CTAs per SM): one accumulator
   // per warp, updated with plain adds, summed at the flush
-  constexpr int kAcc = (kGather && !kC && !MIXED && OP != kHS && !PAIRED) ? kWarps : 1;
+  constexpr int kAccMax = (kGather && !kC && !MIXED && OP != kHS && !PAIRED) ? kWarps : 1;
+  // the host passes 1 when kAccMax copies of the largest DOF block do not fit in shared
+  // memory (DP1 x DP1: 96 x 96 DOFs per tile pair); the warps then add with atomics
+  const int kAcc = kAccMax > 1 && acc_copies > 1 ? kAccMax : 1;
   const int Q = QT > 0 ? QT : rule.npts;
   // symmetric operator on one space (single layer, hypersingular): only the tile pairs with
   // tx >= sy are computed, the blocks with tx > sy also written transposed
@@ -1435,9 +1438,24 @@ cudaError_t launch_mode(const CellSet& test, const SpaceTiles& tt, const CellSet
                               : (!DIRECT && NBT == 3 && KER != kHelmholtz && !MIXED && OP != kHS)
                                     ? kWarps
                                     : 1;
-  const size_t smem = smem_bytes(rule.npts, MIXED, MIXED && NM == kNearInKernel, DIRECT,
-                                 KER == kHelmholtz, tt.max_tile_dofs, st.max_tile_dofs, NBT, NBS,
-                                 kAcc, a.symmetric != 0, !MIXED || NM == kNearInKernel);
+  auto bytes = [&](int copies) {
+    return smem_bytes(rule.npts, MIXED, MIXED && NM == kNearInKernel, DIRECT, KER == kHelmholtz,
+                      tt.max_tile_dofs, st.max_tile_dofs, NBT, NBS, copies, a.symmetric != 0,
+                      !MIXED || NM == kNearInKernel);
+  };
+  int copies = kAcc;
+  size_t smem = bytes(copies);
+  if (copies == kWarps) {
+    int device = 0, limit = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e == cudaSuccess)
+      e = cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (e != cudaSuccess) return e;
+    if (smem > static_cast<size_t>(limit)) {  // one shared accumulator, atomic adds
+      copies = 1;
+      smem = bytes(1);
+    }
+  }
   auto fn = regular_tiles<QT, KER, OP, NBT, NBS, MIXED, DIRECT, PH, NM, PAIRED>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
@@ -1452,7 +1470,7 @@ cudaError_t launch_mode(const CellSet& test, const SpaceTiles& tt, const CellSet
   }
   fn<<<grid, kThreads, smem, stream>>>(test, tt, trial, st, rule, a.k, a.same_grid,
                                        static_cast<double*>(a.out), a.ld, ty0, ty1, a.near,
-                                       a.symmetric);
+                                       a.symmetric, copies);
   return cudaGetLastError();
 }
 
