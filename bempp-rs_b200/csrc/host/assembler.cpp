@@ -561,14 +561,20 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
     // chunked: the whole singular part runs on a side stream beside the first chunks'
     // regular kernels (all adds commute), and every chunk's completion also waits for it,
     // so a chunk's columns are final when it ends
-    const bool side_singular = singular && nchunks > 1;
+    // Chunked: the full tile grid (columns finish evenly through the chunks) runs the
+    // whole singular part on a side stream; its launch is enqueued after the first two
+    // chunks' regular launches, so that on a fresh grid the host builds the pair list while
+    // they run, and the completion of those chunks is reported after it.  The tx >= sy
+    // launches (which finish most columns late) add each chunk's singular pairs after its
+    // regular pairs instead, so that its first columns go out as early as they can.
+    const bool side_singular = singular && nchunks > 1 && !ra.symmetric;
+    const int fork_after = side_singular ? std::min(1, nchunks - 1) : -1;
     if (side_singular) {
       ensure_side_stream(a, device);
       BEMPP_CUDA(cudaEventRecord(a.fork_ev, stream));
       BEMPP_CUDA(cudaStreamWaitEvent(a.side, a.fork_ev, 0));
-      run_singular(0, 0x7fffffff, a.side);
-      BEMPP_CUDA(cudaEventRecord(a.join_ev, a.side));
     }
+    int done = 0;  // chunks whose completion has been reported
     for (int c = 0; c < nchunks; ++c) {
       int t0, t1;
       tile_range(c, t0, t1);
@@ -578,7 +584,13 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
         BEMPP_CUDA(launch_regular_scatter(tcs, space_tiles(test), scs, space_tiles(trial), rule,
                                           ra, stream));
         a.launches += regular_launches;
-        if (side_singular && c == 0) BEMPP_CUDA(cudaStreamWaitEvent(stream, a.join_ev, 0));
+        if (singular && nchunks > 1 && !side_singular)
+          run_singular(32 * t0, c + 1 == nchunks ? 0x7fffffff : 32 * t1, stream);
+      }
+      if (c == fork_after) {
+        run_singular(0, 0x7fffffff, a.side);
+        BEMPP_CUDA(cudaEventRecord(a.join_ev, a.side));
+        BEMPP_CUDA(cudaStreamWaitEvent(stream, a.join_ev, 0));
       }
       if (nchunks == 1) {
         timer.mark();
@@ -589,7 +601,9 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
           ++a.launches;
         }
       }
-      if (chunk_done) chunk_done(c);
+      if (c >= fork_after)
+        for (; done <= c; ++done)
+          if (chunk_done) chunk_done(done);
     }
   }
   timer.mark();
