@@ -67,9 +67,9 @@ FLOPS_PER_PAIR = {
 # DRAM bytes (read + write) per launch of the dominant regular kernel, from one ncu capture
 # of the full-size workload (profiles/dram_traffic_laplace_p1_ico5_fp64.md).
 DRAM_TRAFFIC_PER_LAUNCH = {
-    ("laplace", "double_layer", "p1", 20480): 1022.82e6 + 1050.81e6,
-    ("laplace", "adjoint_double_layer", "p1", 20480): 1023.66e6 + 1048.39e6,
-    ("laplace", "hypersingular", "p1", 20480): 1010.35e6 + 1002.57e6,
+    ("laplace", "double_layer", "p1", 20480): 1013.84e6 + 1021.62e6,
+    ("laplace", "adjoint_double_layer", "p1", 20480): 1013.84e6 + 1018.73e6,
+    ("laplace", "hypersingular", "p1", 20480): 1010.52e6 + 1001.86e6,
 }
 
 WORKLOADS = {
