@@ -200,6 +200,28 @@ def test_one_space_symmetric_operators_match_oracle(kernel, op, k, sp):
 
 
 
+@pytest.mark.parametrize("op", ["double_layer", "adjoint_double_layer"])
+@pytest.mark.parametrize("mesh", ["ico1", "open_cap"])
+def test_paired_double_layer_on_ragged_tiles(op, mesh):
+    """The paired launch (one P1 space object, Laplace DL / ADL) on meshes whose cell count
+    is not a multiple of the 32-cell tile: the 80-cell icosphere (tiles of 32, 32, 16) and
+    the 1,280-cell sphere with a polar cap removed (an open surface, last tile partial)."""
+    pts, cells = shapes.icosphere(1 if mesh == "ico1" else 3)
+    pts = shapes.radial_perturbation(pts, seed=31)
+    if mesh == "open_cap":
+        keep = pts[cells].mean(axis=1)[:, 2] < 0.8
+        cells = cells[keep]
+        used = np.unique(cells)
+        remap = np.full(len(pts), -1)
+        remap[used] = np.arange(len(used))
+        pts, cells = pts[used], remap[cells]
+        assert len(cells) % 32 != 0
+    grid = Grid(pts, cells)
+    a = gpu_assemble(grid, "laplace", op, test=(1, True), trial=(1, True), one_space=True)
+    o = oracle_assemble(grid, "laplace", op, test=(1, True), trial=(1, True))
+    assert rel_err(a, o) <= FP64_TOL
+
+
 # ------------------------------------------------- singular part as CSR (row f1) ---
 @pytest.mark.parametrize("kernel,op,k,sp", [
     ("laplace", "single_layer", 0.0, "dp0"),
