@@ -558,9 +558,6 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
   } else {
     if (!empty) BEMPP_CUDA(cudaMemsetAsync(out, 0, static_cast<size_t>(nt) * ns * esize, stream));
     timer.mark();
-    // chunked: the whole singular part runs on a side stream beside the first chunks'
-    // regular kernels (all adds commute), and every chunk's completion also waits for it,
-    // so a chunk's columns are final when it ends
     // Chunked: the full tile grid (columns finish evenly through the chunks) runs the
     // whole singular part on a side stream; its launch is enqueued after the first two
     // chunks' regular launches, so that on a fresh grid the host builds the pair list while
