@@ -93,6 +93,14 @@ RegularRule simplex_rule(int npoints) {
         r.phif[b][i] = static_cast<float>(phi[b]);
         r.wphi[b][i] = e.weights[i] * phi[b];
       }
+      // degree 2: l (2 l - 1) at the vertices, 4 l_a l_b on edges [1,2], [0,2], [0,1]
+      const double p2[6] = {phi[0] * (2.0 * phi[0] - 1.0), phi[1] * (2.0 * phi[1] - 1.0),
+                            phi[2] * (2.0 * phi[2] - 1.0), 4.0 * phi[1] * phi[2],
+                            4.0 * phi[0] * phi[2], 4.0 * phi[0] * phi[1]};
+      for (int b = 0; b < 6; ++b) {
+        r.phi2[b][i] = p2[b];
+        r.wphi2[b][i] = e.weights[i] * p2[b];
+      }
     }
     return r;
   }

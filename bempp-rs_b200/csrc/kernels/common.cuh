@@ -59,7 +59,28 @@ struct RegularRule {
   double u[kMaxRegularPoints];
   double v[kMaxRegularPoints];
   double wphi[3][kMaxRegularPoints];
+  // Lagrange degree 2 (vertices, then the midpoints of edges [1,2], [0,2], [0,1]) at each
+  // point, and times the weights
+  double phi2[6][kMaxRegularPoints];
+  double wphi2[6][kMaxRegularPoints];
 };
+
+#ifdef __CUDACC__
+// Basis value of function b at rule point q for a space of nb functions per cell (1, 3 or
+// 6), plain or times the weight.
+template <int NB>
+__device__ __forceinline__ double rule_phi(const RegularRule& r, int b, int q) {
+  if constexpr (NB == 6) return r.phi2[b][q];
+  else if constexpr (NB == 3) return r.phi[b][q];
+  else return 1.0;
+}
+template <int NB>
+__device__ __forceinline__ double rule_wphi(const RegularRule& r, int b, int q) {
+  if constexpr (NB == 6) return r.wphi2[b][q];
+  else if constexpr (NB == 3) return r.wphi[b][q];
+  else return r.w[q];
+}
+#endif
 
 struct CellSet {
   int ncells;

@@ -86,7 +86,7 @@ __device__ __forceinline__ void finish_block(const Tile& T, int it, const Tile& 
                                              double S_im, double ore[NBT][NBS],
                                              double oim[NBT][NBS]) {
   const double jj = T.G(fJdet, it) * S.G(fJdet, js);
-  if (OP != kHS) {
+  if constexpr (OP != kHS) {
     const double sc = jj * kInv4Pi;
 #pragma unroll
     for (int a = 0; a < NBT; ++a)
@@ -188,7 +188,7 @@ __device__ __forceinline__ void block_fp64_pq(const Tile& T, int it, const Tile&
           u_re[0] = fma(kern, rule.w[q], u_re[0]);
         } else {
 #pragma unroll
-          for (int b = 0; b < NBS; ++b) u_re[b] = fma(kern, rule.wphi[b][q], u_re[b]);
+          for (int b = 0; b < NBS; ++b) u_re[b] = fma(kern, rule_wphi<NBS>(rule, b, q), u_re[b]);
         }
         continue;
       }
@@ -226,8 +226,8 @@ __device__ __forceinline__ void block_fp64_pq(const Tile& T, int it, const Tile&
         } else {
 #pragma unroll
           for (int b = 0; b < NBS; ++b) {
-            u_re[b] = fma(kre, rule.phi[b][q], u_re[b]);
-            if (kC) u_im[b] = fma(kim, rule.phi[b][q], u_im[b]);
+            u_re[b] = fma(kre, rule_phi<NBS>(rule, b, q), u_re[b]);
+            if (kC) u_im[b] = fma(kim, rule_phi<NBS>(rule, b, q), u_im[b]);
           }
         }
       }
@@ -240,7 +240,7 @@ __device__ __forceinline__ void block_fp64_pq(const Tile& T, int it, const Tile&
       const double wp = rule.w[p] * ap;
 #pragma unroll
       for (int a = 0; a < NBT; ++a) {
-        const double f = NBT == 1 ? wp : wp * rule.phi[a][p];
+        const double f = NBT == 1 ? wp : wp * rule_phi<NBT>(rule, a, p);
 #pragma unroll
         for (int b = 0; b < NBS; ++b) {
           blk_re[a][b] = fma(f, u_re[b], blk_re[a][b]);
@@ -302,12 +302,12 @@ __device__ __forceinline__ void block_fp64_adl_laplace(const Tile& T, int it, co
         v[0] = fma(kern, rule.w[p], v[0]);
       } else {
 #pragma unroll
-        for (int a = 0; a < NBT; ++a) v[a] = fma(kern, rule.wphi[a][p], v[a]);
+        for (int a = 0; a < NBT; ++a) v[a] = fma(kern, rule_wphi<NBT>(rule, a, p), v[a]);
       }
     }
 #pragma unroll
     for (int b = 0; b < NBS; ++b) {
-      const double f = (NBS == 1 ? rule.w[q] : rule.wphi[b][q]) * bq;
+      const double f = rule_wphi<NBS>(rule, b, q) * bq;
 #pragma unroll
       for (int a = 0; a < NBT; ++a) blk_re[a][b] = fma(v[a], f, blk_re[a][b]);
     }
@@ -1450,7 +1450,10 @@ cudaError_t launch_mode(const CellSet& test, const SpaceTiles& tt, const CellSet
   auto fn = regular_tiles<QT, KER, OP, NBT, NBS, MIXED, DIRECT, PH, NM, PAIRED>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
-  if (e != cudaSuccess) return e;
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // not sticky: clear it, so that it is not reported by a later launch
+    return e;
+  }
   const int ntt = (test.ncells + kTile - 1) / kTile;
   dim3 grid(ntt, ty1 - ty0);
   if (a.symmetric) {
@@ -1479,7 +1482,10 @@ cudaError_t launch_near_pairs(const CellSet& test, const CellSet& trial, const R
                           : near_pairs_fp64<QT, KER, OP, NBT, NBS, DIRECT, kF64Reduced>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
-  if (e != cudaSuccess) return e;
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // not sticky: clear it, so that it is not reported by a later launch
+    return e;
+  }
   const int threads = 32 * warps;
   const int blocks = (a.near.npairs + threads - 1) / threads;
   const int lo = ty0 * kTile;
@@ -1562,6 +1568,11 @@ cudaError_t launch_spaces(const CellSet& test, const SpaceTiles& tt, const CellS
     return launch_one<QT, KER, OP, 3, 1, MIXED, false>(test, tt, trial, st, rule, a, stream);
   if (tt.nbasis == 3 && st.nbasis == 3)
     return launch_one<QT, KER, OP, 3, 3, MIXED, false>(test, tt, trial, st, rule, a, stream);
+  if constexpr (!MIXED && KER == kLaplace && OP != kHS) {
+    // degree 2 on both sides (P2 / DP2), FP64
+    if (tt.nbasis == 6 && st.nbasis == 6)
+      return launch_one<QT, KER, OP, 6, 6, false, false>(test, tt, trial, st, rule, a, stream);
+  }
   return cudaErrorInvalidValue;
 }
 
@@ -1643,7 +1654,10 @@ cudaError_t launch_sweep_shape(const SweepArgs& args, const RegularRule& rule, i
   auto fn = sweep_sl_dp0<TS, MINB>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
-  if (e != cudaSuccess) return e;
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // not sticky: clear it, so that it is not reported by a later launch
+    return e;
+  }
   fn<<<blocks, kThreads, smem, stream>>>(args, rule);
   return cudaGetLastError();
 }
@@ -1697,9 +1711,16 @@ cudaError_t launch_regular_scatter(const CellSet& test, const SpaceTiles& tt,
                                    const CellSet& trial, const SpaceTiles& st,
                                    const RegularRule& rule, const RegularArgs& a,
                                    cudaStream_t stream) {
-  if (tt.nbasis > 3 || st.nbasis > 3) {
-    // degree-2 spaces: the generic warp-per-pair kernel (FP64) over this launch's trial
-    // cells
+  // degree 2 on both sides, Laplace single / double / adjoint double layer, FP64: the
+  // tiled kernel (6 x 6 blocks per cell pair)
+  // (when the DOF block of a tile pair fits in shared memory: P2, not DP2)
+  const bool tiled_p2 = tt.nbasis == 6 && st.nbasis == 6 && a.kernel == kLaplace &&
+                        a.op != kHS && a.precision == kRegularFP64 &&
+                        static_cast<size_t>(tt.max_tile_dofs) * st.max_tile_dofs * sizeof(double) <=
+                            (size_t(96) << 10);
+  if ((tt.nbasis > 3 || st.nbasis > 3) && !tiled_p2) {
+    // other pairings with a degree-2 side: the generic warp-per-pair kernel (FP64) over
+    // this launch's trial cells
     GenericPairArgs g;
     g.kernel = a.kernel;
     g.op = a.op;

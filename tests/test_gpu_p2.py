@@ -1,10 +1,12 @@
 """Degree-2 Lagrange spaces (P2 and DP2, alone and paired with DP0 / P1) on the GPU
 against the FP64 oracle, relative Frobenius error <= 1e-12.
 
-These spaces go through the warp-per-cell-pair kernel (generic.cu) for the regular and
-the singular part.  The oracle's degree-2 basis is pinned to its P1 matrices, and those
-to the bempp-cl goldens, by tests/test_oracle_golden.py (the P2 matrix restricted to the
-P1 subspace is the P1 matrix).
+These spaces go through the warp-per-cell-pair kernel (generic.cu) for the singular part
+and for the regular part of every pairing but Laplace single / double / adjoint double
+layer on P2 x P2, which the tiled kernel of regular.cu assembles.  The oracle's degree-2
+basis is pinned to its P1 matrices, and those to the bempp-cl goldens, by
+tests/test_oracle_golden.py (the P2 matrix restricted to the P1 subspace is the P1
+matrix).
 """
 
 import numpy as np
@@ -65,6 +67,18 @@ def test_degree2_one_space_object_and_rules(grid):
         o = oracle_assemble(grid, "helmholtz", "hypersingular", 4.0, test=P2, trial=P2, q=q,
                             order=order)
         assert rel_err(a, o) <= FP64_TOL
+
+
+@pytest.mark.parametrize("op", ["single_layer", "double_layer", "adjoint_double_layer"])
+def test_degree2_tiled_kernel_on_several_tiles(op):
+    """Laplace P2 x P2 (single, double, adjoint double layer) goes through the tiled
+    kernel (6 x 6 blocks per cell pair, per-tile DOF accumulation): 320 cells (10 tiles),
+    one space object (the single layer then computes the tile pairs tx >= sy only)."""
+    pts, cells = shapes.icosphere(2)
+    g = Grid(shapes.radial_perturbation(pts, seed=23), cells)
+    a = gpu_assemble(g, "laplace", op, test=P2, trial=P2, one_space=True)
+    o = oracle_assemble(g, "laplace", op, test=P2, trial=P2)
+    assert rel_err(a, o) <= FP64_TOL
 
 
 def test_degree2_mixed_precision_option_gives_fp64(grid):
