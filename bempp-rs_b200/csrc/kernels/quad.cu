@@ -148,6 +148,12 @@ __global__ void __launch_bounds__(kThreads)
   const int m = rule.n * rule.n;  // regular points per cell
   const int64_t tstride = static_cast<int64_t>(test.ncells) * m;
   const int64_t sstride = static_cast<int64_t>(trial.ncells) * m;
+  // regular part: the lane's point pair ii = p * m + q is stepped by 32 without dividing,
+  // and a point index splits into its (s, t) Gauss indices by an exact FP32 product
+  // (indices below 256, so (i + 0.5) / n never rounds across an integer)
+  int p = lane / m, q = lane - (lane / m) * m;
+  const int dp = 32 / m, dq = 32 - dp * m;
+  const float inv_n = 1.f / static_cast<float>(rule.n);
   for (int ii = lane; ii < npts; ii += 32) {
     double xs, xt, ys, yt, wt;
     double x[3], xj0[3], xj1[3], xn[3], xjd, y[3], yj0[3], yj1[3], yn[3], yjd;
@@ -163,8 +169,8 @@ __global__ void __launch_bounds__(kThreads)
     } else {
       // ii = test point * m + trial point; point p = (s index) * n + (t index)
       const int n = rule.n;
-      const int p = ii / m, q = ii - p * m;
-      const int p0 = p / n, p1 = p - p0 * n, q0 = q / n, q1 = q - q0 * n;
+      const int p0 = static_cast<int>((static_cast<float>(p) + 0.5f) * inv_n), p1 = p - p0 * n;
+      const int q0 = static_cast<int>((static_cast<float>(q) + 0.5f) * inv_n), q1 = q - q0 * n;
       xs = rule.x[p0];
       xt = rule.x[p1];
       ys = rule.x[q0];
@@ -237,6 +243,14 @@ __global__ void __launch_bounds__(kThreads)
         acc_re[a][b] = fma(kre, f, acc_re[a][b]);
         if (kC) acc_im[a][b] = fma(kim, f, acc_im[a][b]);
       }
+    if (!SING) {
+      p += dp;
+      q += dq;
+      if (q >= m) {
+        q -= m;
+        ++p;
+      }
+    }
   }
 #pragma unroll
   for (int a = 0; a < NBT; ++a)
