@@ -437,15 +437,6 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
   ra.same_grid = same_grid ? 1 : 0;
   // one space on both sides and a symmetric kernel: lower-triangle tile pairs, mirrored
   ra.symmetric = (&trial == &test && same_grid && (a.op == kSL || a.op == kHS)) ? 1 : 0;
-  // one P1 / DP1 space, Laplace double layer or its adjoint, FP64, 6-point rule: the pair
-  // (i, j) and the pair (j, i) share their kernel values, so both blocks of a tile pair
-  // come from one pass
-  // (one-launch assemblies only: a chunked host-memory assembly keeps the full tile grid,
-  // whose columns finish evenly through the chunks and go out by DMA meanwhile, where the
-  // tx >= sy half finishes most columns only in its last chunks)
-  if (&trial == &test && same_grid && a.kernel == kLaplace && (a.op == kDL || a.op == kADL) &&
-      a.options.precision != 1 && test.nbasis == 3 && rule.npts == 6 && nchunks == 1)
-    ra.symmetric = 2;
   ra.precision = a.options.precision == 1 ? kRegularMixed : kRegularFP64;
   ra.out_type = cplx ? kOutC128 : kOutF64;
   ra.ld = nt;
@@ -456,6 +447,16 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
                              (test.grid->max_circumradius() + trial.grid->max_circumradius()) *
                              (1.0 + 1e-6);
   ra.small_phase = phase_bound <= 0.8 ? 1 : 0;
+  // one P1 / DP1 space, double layer or its adjoint, FP64, 6-point rule (Helmholtz: with
+  // the phases referenced to the pair): the pair (i, j) and the pair (j, i) share their
+  // kernel values, so both blocks of a tile pair come from one pass (one-launch assemblies
+  // only: a chunked host-memory assembly keeps the full tile grid, whose columns finish
+  // evenly through the chunks and go out by DMA meanwhile, where the tx >= sy half
+  // finishes most columns only in its last chunks)
+  if (&trial == &test && same_grid && (a.kernel == kLaplace || ra.small_phase) &&
+      (a.op == kDL || a.op == kADL) && a.options.precision != 1 && test.nbasis == 3 &&
+      rule.npts == 6 && nchunks == 1)
+    ra.symmetric = 2;
   if (ra.precision == kRegularMixed && nt > 0 && ns > 0) {
     const NearField& nf = near_field(*test.grid, *trial.grid);
     ra.near.tile_mask = nf.tile_mask.as<int>();

@@ -396,6 +396,86 @@ __device__ __forceinline__ void block_fp64_dl_pair(const Tile& T, int it, const 
     }
 }
 
+// The Helmholtz double layer of a cell pair in both orders, FP64, as block_fp64_dl_pair:
+// one kernel value e^{ikr} (1 - ikr) / r^3 per point pair, the phase referenced to the
+// pair (e^{ikr} = e^{ik r0} e^{ik (r - r0)}, |k (r - r0)| <= 0.8 checked on the host), both
+// blocks rotated by e^{ik r0} at the end.
+template <int Q>
+__device__ __forceinline__ void block_fp64_dl_pair_helmholtz(
+    const Tile& T, int it, const Tile& S, int js, const RegularRule& rule, double k,
+    double dij_re[3][3], double dij_im[3][3], double dji_re[3][3], double dji_im[3][3]) {
+  static_assert(Q > 0, "the paired double layer needs a compile-time rule size");
+  const double dcx = T.G(fCx, it) - S.G(fCx, js), dcy = T.G(fCy, it) - S.G(fCy, js),
+               dcz = T.G(fCz, it) - S.G(fCz, js);
+  const double njx = S.G(fNx, js), njy = S.G(fNy, js), njz = S.G(fNz, js);
+  const double nix = T.G(fNx, it), niy = T.G(fNy, it), niz = T.G(fNz, it);
+  const double f0 = dcx * njx + dcy * njy + dcz * njz;
+  const double f1 = T.G(fT0x, it) * njx + T.G(fT0y, it) * njy + T.G(fT0z, it) * njz;
+  const double f2 = T.G(fT1x, it) * njx + T.G(fT1y, it) * njy + T.G(fT1z, it) * njz;
+  const double g0 = -(dcx * nix + dcy * niy + dcz * niz);
+  const double g1 = S.G(fT0x, js) * nix + S.G(fT0y, js) * niy + S.G(fT0z, js) * niz;
+  const double g2 = S.G(fT1x, js) * nix + S.G(fT1y, js) * niy + S.G(fT1z, js) * niz;
+  const double r0sq = dcx * dcx + dcy * dcy + dcz * dcz;
+  const double kr0 = k * (r0sq * rsqrt_refined(r0sq));
+  double bij_re[3][3], bij_im[3][3], bji_re[3][3], bji_im[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) bij_re[a][b] = bij_im[a][b] = bji_re[a][b] = bji_im[a][b] = 0.0;
+#pragma unroll 1
+  for (int p = 0; p < Q; ++p) {
+    const double x0 = T.P(p, 0, it), x1 = T.P(p, 1, it), x2 = T.P(p, 2, it);
+    double ur[3] = {0.0, 0.0, 0.0}, ui[3] = {0.0, 0.0, 0.0};
+    double vr[3] = {0.0, 0.0, 0.0}, vi[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const double dx = x0 - S.P(q, 0, js), dy = x1 - S.P(q, 1, js), dz = x2 - S.P(q, 2, js);
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      const double rinv = rsqrt_refined(r2);
+      const double r = r2 * rinv, kr = k * r;
+      double sn, cs;
+      sincos_small(fma(k, r, -kr0), sn, cs);  // e^{ik (r - r0)}
+      const double f = rinv * rinv * rinv;
+      const double kre = f * fma(kr, sn, cs), kim = f * fma(-kr, cs, sn);
+      const double bq = fma(rule.u[q], g1, fma(rule.v[q], g2, g0));
+      const double bre = kre * bq, bim = kim * bq;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const double w = rule.wphi[b][q];
+        ur[b] = fma(kre, w, ur[b]);
+        ui[b] = fma(kim, w, ui[b]);
+        vr[b] = fma(bre, w, vr[b]);
+        vi[b] = fma(bim, w, vi[b]);
+      }
+    }
+    const double ap = fma(rule.u[p], f1, fma(rule.v[p], f2, f0));
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double c = rule.wphi[a][p], e = c * ap;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        bij_re[a][b] = fma(e, ur[b], bij_re[a][b]);
+        bij_im[a][b] = fma(e, ui[b], bij_im[a][b]);
+        bji_re[a][b] = fma(c, vr[b], bji_re[a][b]);
+        bji_im[a][b] = fma(c, vi[b], bji_im[a][b]);
+      }
+    }
+  }
+  double ps, pc;
+  sincos_cw(kr0, ps, pc);
+  const double sc = T.G(fJdet, it) * S.G(fJdet, js) * kInv4Pi;
+  const double cr = pc * sc, ci = ps * sc;  // e^{ik r0} jdet_i jdet_j / (4 pi)
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      dij_re[a][b] = bij_re[a][b] * cr - bij_im[a][b] * ci;
+      dij_im[a][b] = bij_re[a][b] * ci + bij_im[a][b] * cr;
+      dji_re[a][b] = bji_re[a][b] * cr - bji_im[a][b] * ci;
+      dji_im[a][b] = bji_re[a][b] * ci + bji_im[a][b] * cr;
+    }
+}
+
 // Per-pair constants of the FP32 far-pair quadrature.
 template <int QT>
 struct FarPair {
@@ -791,7 +871,10 @@ enum NearMode : int { kNearInKernel = 0, kNearMasked = 1 };
 // spills 48 bytes).
 template <int KER, int OP, bool MIXED, bool DIRECT, bool PAIRED = false>
 constexpr int min_ctas() {
-  return (KER == kLaplace && OP == kHS && !MIXED) ? 5 : (MIXED && DIRECT && KER == kHelmholtz) ? 6 : 4;
+  return (PAIRED && KER == kHelmholtz)             ? 3
+         : (KER == kLaplace && OP == kHS && !MIXED) ? 5
+         : (MIXED && DIRECT && KER == kHelmholtz)   ? 6
+                                                    : 4;
 }
 
 // PAIRED (Laplace DL / ADL, FP64, one P1 / DP1 space on both sides, Q = 6): the tile
@@ -804,9 +887,10 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAI
     regular_tiles(CellSet test, SpaceTiles tt, CellSet trial, SpaceTiles st, RegularRule rule,
                   double k, int same_grid, double* __restrict__ out, int64_t ld, int tile_y0,
                   int tile_y1, NearArgs near, int symmetric, int acc_copies) {
-  static_assert(!PAIRED || (KER == kLaplace && (OP == kDL || OP == kADL) && NBT == 3 &&
-                            NBS == 3 && !MIXED && !DIRECT && QT == 6),
-                "paired blocks: Laplace DL / ADL, FP64, P1 / DP1, 6-point rule");
+  static_assert(!PAIRED || ((OP == kDL || OP == kADL) && NBT == 3 && NBS == 3 && !MIXED &&
+                            !DIRECT && QT == 6 && (KER == kLaplace || PH == kPhaseSmall)),
+                "paired blocks: DL / ADL, FP64, P1 / DP1, 6-point rule (Helmholtz: phases "
+                "referenced to the pair)");
   constexpr bool kC = KER == kHelmholtz;
   constexpr bool kQueue = MIXED && NM == kNearInKernel;
   constexpr bool kRel = MIXED;  // FP32 offsets staged
@@ -855,9 +939,10 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAI
     acc_im = acc_re + cap;
     cursor += sizeof(double) * cap * (kC ? 2 : 1) * kAcc;
   }
-  // PAIRED: the (sy, tx) blocks, indexed as acc_re (test-tile DOF + ndt * trial-tile DOF)
+  // PAIRED: the (sy, tx) blocks, indexed as acc_re (test-tile DOF + ndt * trial-tile DOF),
+  // imaginary parts (Helmholtz) cap further on
   double* acc_t = reinterpret_cast<double*>(cursor);
-  if (PAIRED) cursor += sizeof(double) * cap;
+  if (PAIRED) cursor += sizeof(double) * cap * (kC ? 2 : 1);
   double* stage_re = nullptr;  // kGather: [warp][(a * NBS + b) * kTile + lane]
   double* stage_im = nullptr;
   uint8_t* inc_off = nullptr;  // kGather: the test tile's DOF incidence
@@ -897,7 +982,10 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAI
         if (kC) acc_im[idx] = 0.0;
       }
     if (PAIRED)
-      for (int idx = threadIdx.x; idx < ndt * nds; idx += kThreads) acc_t[idx] = 0.0;
+      for (int idx = threadIdx.x; idx < ndt * nds; idx += kThreads) {
+        acc_t[idx] = 0.0;
+        if (kC) acc_t[cap + idx] = 0.0;
+      }
     load_ldof(T, ti0, nti, tt.cell_ldof, NBT);
     load_ldof(S, sj0, nsj, st.cell_ldof, NBS);
     if (kGather)
@@ -928,7 +1016,8 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAI
   }
   for (int js = warp; js < nsj; js += kWarps) {  // warp-uniform trip count
     double ore[NBT][NBS], oim[NBT][NBS];
-    double otr[NBT][NBS];  // PAIRED: the (sy, tx) block, [test-tile basis][trial-tile basis]
+    double otr[NBT][NBS], oti[NBT][NBS];  // PAIRED: the (sy, tx) block, [test-tile
+                                          // basis][trial-tile basis], real and imaginary
     bool have = false;
     if (lane_cell) {
       const int64_t o = static_cast<int64_t>(sj0 + js) * ld + ti0 + it;
@@ -952,15 +1041,22 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAI
         queue[slot] = static_cast<unsigned short>(it | (js << 8));
       } else {
         if constexpr (PAIRED) {
-#pragma unroll
-          for (int a = 0; a < NBT; ++a)
-#pragma unroll
-            for (int b = 0; b < NBS; ++b) oim[a][b] = 0.0;  // real blocks
           // DL: (i, j) block here, (j, i) at the transposed entries; ADL: swapped
-          if (OP == kDL)
-            block_fp64_dl_pair<QT>(T, it, S, js, rule, ore, otr);
-          else
-            block_fp64_dl_pair<QT>(T, it, S, js, rule, otr, ore);
+          if constexpr (KER == kLaplace) {
+#pragma unroll
+            for (int a = 0; a < NBT; ++a)
+#pragma unroll
+              for (int b = 0; b < NBS; ++b) oim[a][b] = oti[a][b] = 0.0;  // real blocks
+            if (OP == kDL)
+              block_fp64_dl_pair<QT>(T, it, S, js, rule, ore, otr);
+            else
+              block_fp64_dl_pair<QT>(T, it, S, js, rule, otr, ore);
+          } else {
+            if (OP == kDL)
+              block_fp64_dl_pair_helmholtz<QT>(T, it, S, js, rule, k, ore, oim, otr, oti);
+            else
+              block_fp64_dl_pair_helmholtz<QT>(T, it, S, js, rule, k, otr, oti, ore, oim);
+          }
         } else if (MIXED) {
           block_fp32<QT, KER, OP, NBT, NBS, PH>(T, it, S, js, rule, k, ore, oim);
         } else {
@@ -985,12 +1081,13 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAI
       double* sr = stage_re + warp * (kTile * NBT * NBS);
       double* si = stage_im + warp * (kTile * NBT * NBS);
       double* acc = pass == 0 ? acc_re : acc_t;
+      double* acci = pass == 0 ? acc_im : acc_t + cap;
 #pragma unroll
       for (int a = 0; a < NBT; ++a)
 #pragma unroll
         for (int b = 0; b < NBS; ++b) {
           sr[(a * NBS + b) * kTile + it] = have ? (pass == 0 ? ore[a][b] : otr[a][b]) : 0.0;
-          if (kC) si[(a * NBS + b) * kTile + it] = have ? oim[a][b] : 0.0;
+          if (kC) si[(a * NBS + b) * kTile + it] = have ? (pass == 0 ? oim[a][b] : oti[a][b]) : 0.0;
         }
       __syncwarp();
       for (int d = it; d < ndt; d += kTile) {
@@ -1013,7 +1110,7 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAI
             acc[warp * cap + idx] += g_re[b];  // this warp's copy; distinct per lane
           } else {
             atomicAdd(acc + idx, g_re[b]);
-            if (kC) atomicAdd(acc_im + idx, g_im[b]);
+            if (kC) atomicAdd(acci + idx, g_im[b]);
           }
         }
       }
@@ -1068,7 +1165,18 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAI
       for (int w = 1; w < kAcc; ++w) re += acc_re[w * cap + idx];
       // symmetric, tx > sy: the same value at the transposed entry
       const int64_t om = static_cast<int64_t>(tdofs[a]) * ld + sdofs[b];
-      if (kC) {
+      if (kC && PAIRED) {
+        const double im = acc_im[idx];
+        if (re != 0.0 || im != 0.0) {
+          atomicAdd(out + 2 * o, re);
+          atomicAdd(out + 2 * o + 1, im);
+        }
+        const double tre = acc_t[idx], tim = acc_t[cap + idx];
+        if (mirror && (tre != 0.0 || tim != 0.0)) {
+          atomicAdd(out + 2 * om, tre);
+          atomicAdd(out + 2 * om + 1, tim);
+        }
+      } else if (kC) {
         const double im = acc_im[idx];
         if (re != 0.0 || im != 0.0) {
           atomicAdd(out + 2 * o, re);
@@ -1508,14 +1616,16 @@ cudaError_t launch_one(const CellSet& test, const SpaceTiles& tt, const CellSet&
   const int ty0 = a.trial_tile0, ty1 = a.trial_tile0 + ny;
   if constexpr (!MIXED) {
     if (a.symmetric == 2) {
-      // one P1 / DP1 space, Laplace DL / ADL: both orders of each pair from one kernel
-      // evaluation (the host asks for it only there)
-      if constexpr (KER == kLaplace && (OP == kDL || OP == kADL) && NBT == 3 && NBS == 3 &&
-                    !DIRECT && QT == 6)
+      // one P1 / DP1 space, DL / ADL: both orders of each pair from one kernel evaluation
+      // (the host asks for it only there, for Helmholtz only with phases referenced to the
+      // pair)
+      if constexpr ((OP == kDL || OP == kADL) && NBT == 3 && NBS == 3 && !DIRECT && QT == 6) {
+        if (KER == kHelmholtz && !a.small_phase) return cudaErrorInvalidValue;
         return launch_mode<QT, KER, OP, NBT, NBS, false, DIRECT, kPhaseSmall, kNearInKernel, true>(
             test, tt, trial, st, rule, a, ty0, ty1, stream);
-      else
+      } else {
         return cudaErrorInvalidValue;
+      }
     }
     // FP64 Helmholtz: phases referenced to the pair (kPhaseSmall) when the host's bound
     // allows it, else CUDA's sincos of every phase

@@ -186,12 +186,15 @@ def test_singular_csr_matches_dense():
     ("laplace", "adjoint_double_layer", 0.0, (1, True)),
     ("laplace", "double_layer", 0.0, (1, False)),
     ("laplace", "adjoint_double_layer", 0.0, (1, False)),
+    ("helmholtz", "double_layer", 5.0, (1, True)),
+    ("helmholtz", "adjoint_double_layer", 5.0, (1, True)),
 ])
 def test_one_space_symmetric_operators_match_oracle(kernel, op, k, sp):
     """Operators on one space object.  Single layer and hypersingular: only tile pairs
-    (tx >= sy) are computed and the rest is mirrored.  Laplace double layer and its adjoint
+    (tx >= sy) are computed and the rest is mirrored.  The double layer and its adjoint
     on P1 / DP1: tile pairs (tx >= sy), each integrated in both orders from one kernel
-    evaluation per point pair.  The matrix matches the oracle, which computes every pair."""
+    evaluation per point pair (Helmholtz: when the pair-referenced phase applies, as at
+    k = 5 here).  The matrix matches the oracle, which computes every pair."""
     pts, cells = shapes.icosphere(3)
     grid = Grid(shapes.radial_perturbation(pts, seed=11), cells)
     a = gpu_assemble(grid, kernel, op, k, test=sp, trial=sp, one_space=True)
