@@ -447,15 +447,14 @@ void assemble_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* d
                              (test.grid->max_circumradius() + trial.grid->max_circumradius()) *
                              (1.0 + 1e-6);
   ra.small_phase = phase_bound <= 0.8 ? 1 : 0;
-  // one P1 / DP1 space, double layer or its adjoint, FP64, 6-point rule (Helmholtz: with
-  // the phases referenced to the pair): the pair (i, j) and the pair (j, i) share their
+  // one P1 / DP1 space, double layer or its adjoint, 6-point rule (Helmholtz: with the
+  // phases referenced to the pair): the pair (i, j) and the pair (j, i) share their
   // kernel values, so both blocks of a tile pair come from one pass (one-launch assemblies
   // only: a chunked host-memory assembly keeps the full tile grid, whose columns finish
   // evenly through the chunks and go out by DMA meanwhile, where the tx >= sy half
   // finishes most columns only in its last chunks)
   if (&trial == &test && same_grid && (a.kernel == kLaplace || ra.small_phase) &&
-      (a.op == kDL || a.op == kADL) && a.options.precision != 1 && test.nbasis == 3 &&
-      rule.npts == 6 && nchunks == 1)
+      (a.op == kDL || a.op == kADL) && test.nbasis == 3 && rule.npts == 6 && nchunks == 1)
     ra.symmetric = 2;
   if (ra.precision == kRegularMixed && nt > 0 && ns > 0) {
     const NearField& nf = near_field(*test.grid, *trial.grid);

@@ -709,6 +709,135 @@ __device__ __forceinline__ void far_sums_x2(const Tile& T, int it, const Tile& S
   }
 }
 
+// The double layer of a far cell pair in both orders, mixed precision, for one P1 / DP1
+// space on both sides (the paired launch): the FP32 packed loop of far_sums_x2 with the
+// phase referenced to the pair (|k (r - r0)| <= 0.8, the launch's bound), one kernel value
+// per point pair for DL(test i, trial j) (the normal factor (x_p - y).n_j per test point)
+// and DL(test j, trial i) (the factor (y_q - x).n_i per point pair, folded per test point
+// like block_fp64_dl_pair); geometry, the reference phase e^{ik r0} and the blocks' final
+// scaling in FP64.  dij / dji as in block_fp64_dl_pair.
+template <int QT, int KER>
+__device__ __forceinline__ void block_fp32_dl_pair(const Tile& T, int it, const Tile& S, int js,
+                                                   const RegularRule& rule, double k,
+                                                   double dij_re[3][3], double dij_im[3][3],
+                                                   double dji_re[3][3], double dji_im[3][3]) {
+  static_assert(QT > 0 && QT % 2 == 0, "pairs of trial points");
+  constexpr bool kC = KER == kHelmholtz;
+  const double dcx = T.G(fCx, it) - S.G(fCx, js), dcy = T.G(fCy, it) - S.G(fCy, js),
+               dcz = T.G(fCz, it) - S.G(fCz, js);
+  const double njx = S.G(fNx, js), njy = S.G(fNy, js), njz = S.G(fNz, js);
+  const double nix = T.G(fNx, it), niy = T.G(fNy, it), niz = T.G(fNz, it);
+  // (x_p - y).n_j = fa0 + u_p fa1 + v_p fa2; (y_q - x).n_i = fb0 + u_q fb1 + v_q fb2
+  const float fa0 = static_cast<float>(dcx * njx + dcy * njy + dcz * njz);
+  const float fa1 = static_cast<float>(T.G(fT0x, it) * njx + T.G(fT0y, it) * njy + T.G(fT0z, it) * njz);
+  const float fa2 = static_cast<float>(T.G(fT1x, it) * njx + T.G(fT1y, it) * njy + T.G(fT1z, it) * njz);
+  const float fb0 = static_cast<float>(-(dcx * nix + dcy * niy + dcz * niz));
+  const float fb1 = static_cast<float>(S.G(fT0x, js) * nix + S.G(fT0y, js) * niy + S.G(fT0z, js) * niz);
+  const float fb2 = static_cast<float>(S.G(fT1x, js) * nix + S.G(fT1y, js) * niy + S.G(fT1z, js) * niz);
+  const float fdx = static_cast<float>(dcx), fdy = static_cast<float>(dcy),
+              fdz = static_cast<float>(dcz);
+  const double r0sq = dcx * dcx + dcy * dcy + dcz * dcz;
+  // s = r^2 - r0^2 (Helmholtz carries s' = ks s, ks = k or 1e-20 when k = 0), as in
+  // far_sums_x2
+  const float kf = static_cast<float>(k), ks = kf != 0.f ? kf : 1e-20f, ks_inv = 1.f / ks;
+  const float m2 = kC ? -2.f * ks : -2.f;
+  const float mx = (kC ? ks : 1.f) * (-2.f * fdx), my = (kC ? ks : 1.f) * (-2.f * fdy),
+              mz = (kC ? ks : 1.f) * (-2.f * fdz);
+  float r0f = 0.f, r0sqf = fmaf(fdx, fdx, fmaf(fdy, fdy, fdz * fdz));
+  double ph_c = 1.0, ph_s = 0.0;
+  if (kC) {
+    const double r0 = r0sq * rsqrt_refined(r0sq);
+    r0f = static_cast<float>(r0);
+    r0sqf = static_cast<float>(r0sq);
+    float pc, ps;
+    phase_cos_sin(k * r0, pc, ps);
+    ph_c = pc;
+    ph_s = ps;
+  }
+  const float2 r0sq2 = f2(r0sqf), r0f2 = f2(r0f), kf2 = f2(kf), nkf2 = f2(-kf);
+  const float2 ks2 = f2(ks), ksinv2 = f2(ks_inv);
+  float bij_re[3][3], bij_im[3][3], bji_re[3][3], bji_im[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) bij_re[a][b] = bij_im[a][b] = bji_re[a][b] = bji_im[a][b] = 0.f;
+#pragma unroll 1
+  for (int p = 0; p < QT; ++p) {
+    const float4 a = T.R4(p, it);
+    const float apf = fmaf(rule.uf[p], fa1, fmaf(rule.vf[p], fa2, fa0));
+    const float2 wx = f2(fmaf(m2, a.x, mx)), wy = f2(fmaf(m2, a.y, my)), wz = f2(fmaf(m2, a.z, mz));
+    const float2 Ap = f2(fmaf(-a.x, mx, fmaf(-a.y, my, fmaf(-a.z, mz, kC ? ks * a.w : a.w + r0sqf))));
+    float2 ur[3], ui[3], vr[3], vi[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) ur[b] = ui[b] = vr[b] = vi[b] = f2(0.f);
+#pragma unroll
+    for (int j = 0; j < QT / 2; ++j) {
+      const float4 A = S.RA(j, js), B = S.RB(j, js);
+      const float2 wq = make_float2(rule.wf[2 * j], rule.wf[2 * j + 1]);
+      const float2 sv = ffma2(wx, make_float2(A.x, A.y),
+                              ffma2(wy, make_float2(A.z, A.w),
+                                    ffma2(wz, make_float2(B.x, B.y),
+                                          kC ? ffma2(ks2, make_float2(B.z, B.w), Ap)
+                                             : fadd2(Ap, make_float2(B.z, B.w)))));
+      float2 kre, kim = f2(0.f);
+      if (!kC) {
+        const float2 rinv = rsqrt_approx2(sv);  // sv is r^2 here
+        kre = fmul2(wq, fmul2(fmul2(rinv, rinv), rinv));
+      } else {
+        const float2 r2 = ffma2(sv, ksinv2, r0sq2);
+        const float2 rinv = rsqrt_approx2(r2);
+        const float2 t = fmul2(sv, rcp_approx2(ffma2(r2, rinv, r0f2)));
+        float2 cs, ss;
+        poly_cos_sin2(t, cs, ss);
+        const float2 rr = fmul2(r2, rinv);
+        const float2 f = fmul2(wq, fmul2(fmul2(rinv, rinv), rinv));
+        // (1 - ik r) e^{ik (r - r0)} / r^3
+        kre = fmul2(f, ffma2(fmul2(kf2, rr), ss, cs));
+        kim = fmul2(f, ffma2(fmul2(nkf2, rr), cs, ss));
+      }
+      const float2 bq = ffma2(make_float2(rule.uf[2 * j], rule.uf[2 * j + 1]), f2(fb1),
+                              ffma2(make_float2(rule.vf[2 * j], rule.vf[2 * j + 1]), f2(fb2), f2(fb0)));
+      const float2 bre = fmul2(kre, bq), bim = kC ? fmul2(kim, bq) : f2(0.f);
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const float2 phi = make_float2(rule.phif[b][2 * j], rule.phif[b][2 * j + 1]);
+        ur[b] = ffma2(kre, phi, ur[b]);
+        vr[b] = ffma2(bre, phi, vr[b]);
+        if (kC) {
+          ui[b] = ffma2(kim, phi, ui[b]);
+          vi[b] = ffma2(bim, phi, vi[b]);
+        }
+      }
+    }
+    const float wp = rule.wf[p];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float c = wp * rule.phif[a][p], e = c * apf;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        bij_re[a][b] = fmaf(e, ur[b].x + ur[b].y, bij_re[a][b]);
+        bji_re[a][b] = fmaf(c, vr[b].x + vr[b].y, bji_re[a][b]);
+        if (kC) {
+          bij_im[a][b] = fmaf(e, ui[b].x + ui[b].y, bij_im[a][b]);
+          bji_im[a][b] = fmaf(c, vi[b].x + vi[b].y, bji_im[a][b]);
+        }
+      }
+    }
+  }
+  const double sc = T.G(fJdet, it) * S.G(fJdet, js) * kInv4Pi;
+  const double cr = ph_c * sc, ci = ph_s * sc;  // e^{ik r0} jdet_i jdet_j / (4 pi)
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      const double xr = bij_re[a][b], xi = bij_im[a][b], yr = bji_re[a][b], yi = bji_im[a][b];
+      dij_re[a][b] = xr * cr - xi * ci;
+      dij_im[a][b] = xr * ci + xi * cr;
+      dji_re[a][b] = yr * cr - yi * ci;
+      dji_im[a][b] = yr * ci + yi * cr;
+    }
+}
+
 // Phase handling of a launch (Helmholtz far pairs): kPhaseRuntime chooses per warp (the
 // unreduced polynomials of |t| <= 0.8 or, for even rules, of |t| <= 1.6 when the warp's
 // k (rad_x + rad_y) allows it, else the reduction), kPhaseSmall assumes |k (r - r0)| <= 0.8
@@ -887,10 +1016,11 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAI
     regular_tiles(CellSet test, SpaceTiles tt, CellSet trial, SpaceTiles st, RegularRule rule,
                   double k, int same_grid, double* __restrict__ out, int64_t ld, int tile_y0,
                   int tile_y1, NearArgs near, int symmetric, int acc_copies) {
-  static_assert(!PAIRED || ((OP == kDL || OP == kADL) && NBT == 3 && NBS == 3 && !MIXED &&
-                            !DIRECT && QT == 6 && (KER == kLaplace || PH == kPhaseSmall)),
-                "paired blocks: DL / ADL, FP64, P1 / DP1, 6-point rule (Helmholtz: phases "
-                "referenced to the pair)");
+  static_assert(!PAIRED || ((OP == kDL || OP == kADL) && NBT == 3 && NBS == 3 && !DIRECT &&
+                            QT == 6 && (KER == kLaplace || PH == kPhaseSmall) &&
+                            (!MIXED || NM == kNearMasked)),
+                "paired blocks: DL / ADL, P1 / DP1, 6-point rule (Helmholtz: phases "
+                "referenced to the pair; mixed: near pairs masked)");
   constexpr bool kC = KER == kHelmholtz;
   constexpr bool kQueue = MIXED && NM == kNearInKernel;
   constexpr bool kRel = MIXED;  // FP32 offsets staged
@@ -1040,7 +1170,13 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAI
         const int slot = atomicAdd(qcount, 1);
         queue[slot] = static_cast<unsigned short>(it | (js << 8));
       } else {
-        if constexpr (PAIRED) {
+        if constexpr (PAIRED && MIXED) {
+          // far pair, FP32 (near and vertex-sharing pairs are masked)
+          if (OP == kDL)
+            block_fp32_dl_pair<QT, KER>(T, it, S, js, rule, k, ore, oim, otr, oti);
+          else
+            block_fp32_dl_pair<QT, KER>(T, it, S, js, rule, k, otr, oti, ore, oim);
+        } else if constexpr (PAIRED) {
           // DL: (i, j) block here, (j, i) at the transposed entries; ADL: swapped
           if constexpr (KER == kLaplace) {
 #pragma unroll
@@ -1649,6 +1785,20 @@ cudaError_t launch_one(const CellSet& test, const SpaceTiles& tt, const CellSet&
     }
     if (a.near.trial_tiles != trial_tiles) return cudaErrorInvalidValue;
     cudaError_t e;
+    if (a.symmetric == 2) {
+      // one P1 / DP1 space, DL / ADL: both orders of each far pair from one kernel
+      // evaluation (Helmholtz only with phases within the polynomial range)
+      if constexpr ((OP == kDL || OP == kADL) && NBT == 3 && NBS == 3 && !DIRECT && QT == 6) {
+        if (KER == kHelmholtz && !a.small_phase) return cudaErrorInvalidValue;
+        e = launch_mode<QT, KER, OP, NBT, NBS, true, DIRECT, kPhaseSmall, kNearMasked, true>(
+            test, tt, trial, st, rule, a, ty0, ty1, stream);
+        if (e != cudaSuccess) return e;
+        return launch_near_pairs<QT, KER, OP, NBT, NBS, DIRECT>(test, trial, rule, a, ty0, ty1,
+                                                                stream);
+      } else {
+        return cudaErrorInvalidValue;
+      }
+    }
     // the launch-wide bound failed: each warp still takes the unreduced polynomial phase
     // when its own pairs allow it (most pairs of a mesh whose largest cells set the bound)
     if (KER == kHelmholtz && !a.small_phase)

@@ -73,9 +73,19 @@ def test_mixed_p1_matches_oracle(kernel, op, k):
 @pytest.mark.parametrize("kernel,op,k,sp", [
     ("helmholtz", "single_layer", 8.0, (0, False)),
     ("laplace", "hypersingular", 0.0, (1, True)),
+    ("laplace", "double_layer", 0.0, (1, True)),
+    ("laplace", "adjoint_double_layer", 0.0, (1, True)),
+    ("laplace", "double_layer", 0.0, (1, False)),
+    ("helmholtz", "double_layer", 5.0, (1, True)),
+    ("helmholtz", "adjoint_double_layer", 5.0, (1, True)),
+    ("helmholtz", "double_layer", 8.0, (1, True)),
 ])
 def test_mixed_one_space_symmetric(kernel, op, k, sp):
-    """The mixed path with the lower-triangle (mirrored) tile pairs of one space object."""
+    """The mixed path on one space object: lower-triangle (mirrored) tile pairs for the
+    single layer and the hypersingular operator; for the double layer and its adjoint on
+    P1 / DP1 the tile pairs tx >= sy, each far pair in both orders from one FP32 kernel
+    value (Helmholtz when every phase stays in the polynomial range: k = 5 here; k = 8
+    exceeds it on this mesh and takes the one-order launch)."""
     pts, cells = shapes.icosphere(3)
     grid = Grid(shapes.radial_perturbation(pts, seed=12), cells)
     a = gpu_assemble(grid, kernel, op, k, test=sp, trial=sp, precision=Precision.Mixed,
