@@ -199,7 +199,15 @@ def test_one_space_symmetric_operators_match_oracle(kernel, op, k, sp):
     grid = Grid(shapes.radial_perturbation(pts, seed=11), cells)
     a = gpu_assemble(grid, kernel, op, k, test=sp, trial=sp, one_space=True)
     o = oracle_assemble(grid, kernel, op, k, test=sp, trial=sp)
-    assert rel_err(a, o) <= FP64_TOL
+    err = rel_err(a, o)
+    if err > FP64_TOL:  # where the entries differ, for the failure message
+        bad = np.argwhere(np.abs(a - o) > 1e-9 * np.abs(o).max())
+        tiles = sorted({(int(i) // 32, int(j) // 32) for i, j in bad})
+        msg = (f"{len(bad)} entries differ; first {bad[:5].tolist()}; tile pairs {tiles[:20]}; "
+               f"zeros in the result {int((a == 0).sum())}")
+    else:
+        msg = ""
+    assert err <= FP64_TOL, msg
 
 
 
