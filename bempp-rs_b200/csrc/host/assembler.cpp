@@ -361,6 +361,8 @@ void assemble_quad_device(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, vo
   g.trial_dofs = trial.d_dofs.as<int>();
   g.rule = rule;
   g.same_grid = same_grid ? 1 : 0;
+  // one space and a symmetric operator: half of the regular pairs, mirrored
+  g.symmetric = (&trial == &test && same_grid && (a.op == kSL || a.op == kHS)) ? 1 : 0;
   g.out = out;
   g.ld = nt;
   if (!empty) {

@@ -63,8 +63,9 @@ struct RegularArgs {
   NearArgs near{};       // mixed: near field (null: near pairs found per pair in the kernel)
   int symmetric = 0;     // 1: test and trial are one space and the operator is symmetric
                          // (SL, HS): only tile pairs (tx >= sy) are computed, then mirrored;
-                         // 2: one P1 / DP1 space, Laplace DL or ADL, FP64, 6-point rule:
-                         // tile pairs (tx >= sy), each integrated in both orders
+                         // 2: one P1 / DP1 space, DL or ADL, 6-point rule (Helmholtz:
+                         // phases within the polynomial range): tile pairs (tx >= sy),
+                         // each integrated in both orders
   int trial_tile0 = 0;   // first trial tile of this launch
   int trial_tiles = 0;   // trial tiles of this launch (0: all from trial_tile0 on)
 };
@@ -152,6 +153,9 @@ struct GenericPairArgs {
   int64_t ld;
   int trial_lo = 0, trial_hi = 0x7fffffff;
   double* pair_values = nullptr;
+  // regular part, test and trial one space, symmetric operator (SL, HS): only the pairs
+  // with test cell >= trial cell, each also added at the transposed entries
+  int symmetric = 0;
 };
 cudaError_t launch_generic_pairs(const GenericPairArgs& g, cudaStream_t stream);
 
@@ -197,6 +201,7 @@ struct QuadPairArgs {
   int64_t ld;
   int trial_lo = 0, trial_hi = 0x7fffffff;
   double* pair_values = nullptr;
+  int symmetric = 0;  // as GenericPairArgs::symmetric
 };
 cudaError_t launch_quad_pairs(const QuadPairArgs& g, cudaStream_t stream);
 

@@ -99,7 +99,8 @@ __global__ void __launch_bounds__(kThreads)
     quad_pairs(QuadCells test, const int* __restrict__ tdofs, QuadCells trial,
                const int* __restrict__ sdofs, QuadGaussRule rule, SingularRules srules,
                SingularPairs pairs, int same_grid, double k, double* __restrict__ out,
-               int64_t ld, int trial_lo, int trial_hi, double* __restrict__ pair_values) {
+               int64_t ld, int trial_lo, int trial_hi, double* __restrict__ pair_values,
+               int symmetric) {
   constexpr bool kC = KER == kHelmholtz;
   const int lane = threadIdx.x & 31;
   const int64_t w = static_cast<int64_t>(blockIdx.x) * kWarpsPerBlock + (threadIdx.x >> 5);
@@ -116,6 +117,8 @@ __global__ void __launch_bounds__(kThreads)
     if (w >= span * test.ncells) return;
     tc = static_cast<int>(w % test.ncells);
     sc = trial_lo + static_cast<int>(w / test.ncells);
+    // one space and a symmetric operator: the pair (tc, sc) also gives (sc, tc)
+    if (symmetric && tc < sc) return;
     if (same_grid) {
       bool shared = false;
 #pragma unroll
@@ -284,11 +287,20 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
     for (int a = 0; a < NBT; ++a) {
       const int64_t o = col + __ldg(tdofs + static_cast<int64_t>(tc) * NBT + a);
+      // the transposed entry: test cell sc's function b against trial cell tc's function a
+      const int64_t om = static_cast<int64_t>(__ldg(sdofs + static_cast<int64_t>(tc) * NBS + a)) * ld +
+                         __ldg(tdofs + static_cast<int64_t>(sc) * NBT + b);
+      const bool mirror = !SING && symmetric && tc > sc;
       if (kC) {
         atomicAdd(out + 2 * o, acc_re[a][b] * kInv4Pi);
         atomicAdd(out + 2 * o + 1, acc_im[a][b] * kInv4Pi);
+        if (mirror) {
+          atomicAdd(out + 2 * om, acc_re[a][b] * kInv4Pi);
+          atomicAdd(out + 2 * om + 1, acc_im[a][b] * kInv4Pi);
+        }
       } else {
         atomicAdd(out + o, acc_re[a][b] * kInv4Pi);
+        if (mirror) atomicAdd(out + om, acc_re[a][b] * kInv4Pi);
       }
     }
   }
@@ -301,7 +313,7 @@ cudaError_t launch_pairs(const QuadPairArgs& g, cudaStream_t stream) {
     const int blocks = (g.pairs.npairs + kWarpsPerBlock - 1) / kWarpsPerBlock;
     quad_pairs<KER, OP, NBT, NBS, true><<<blocks, kThreads, 0, stream>>>(
         g.test, g.test_dofs, g.trial, g.trial_dofs, g.rule, g.rules, g.pairs, g.same_grid, g.k,
-        static_cast<double*>(g.out), g.ld, g.trial_lo, g.trial_hi, g.pair_values);
+        static_cast<double*>(g.out), g.ld, g.trial_lo, g.trial_hi, g.pair_values, 0);
     return cudaGetLastError();
   }
   const int lo = g.trial_lo, hi = g.trial_hi < g.trial.ncells ? g.trial_hi : g.trial.ncells;
@@ -311,7 +323,7 @@ cudaError_t launch_pairs(const QuadPairArgs& g, cudaStream_t stream) {
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
   quad_pairs<KER, OP, NBT, NBS, false><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(
       g.test, g.test_dofs, g.trial, g.trial_dofs, g.rule, g.rules, g.pairs, g.same_grid, g.k,
-      static_cast<double*>(g.out), g.ld, lo, hi, nullptr);
+      static_cast<double*>(g.out), g.ld, lo, hi, nullptr, g.symmetric);
   return cudaGetLastError();
 }
 

@@ -1996,6 +1996,7 @@ cudaError_t launch_regular_scatter(const CellSet& test, const SpaceTiles& tt,
     g.pairs = SingularPairs{};
     g.singular = false;
     g.same_grid = a.same_grid;
+    g.symmetric = a.symmetric == 1 ? 1 : 0;
     g.out = a.out;
     g.ld = a.ld;
     const int tiles = (trial.ncells + kTile - 1) / kTile;

@@ -123,10 +123,16 @@ def test_quad_other_rules(cube, q, order):
     assert rel_err(a, o) <= FP64_TOL
 
 
-def test_quad_one_space_object(cube):
-    sp = space(cube, Q1)
-    a = assembler("laplace", "hypersingular", 0.0, quad_options()).assemble(sp, sp)
-    o = oracle_quad(cube, "laplace", "hypersingular", test=Q1, trial=Q1)
+@pytest.mark.parametrize("kernel,op,sp", [("laplace", "hypersingular", Q1),
+                                          ("laplace", "single_layer", DP0),
+                                          ("helmholtz", "single_layer", DQ1),
+                                          ("helmholtz", "hypersingular", Q1)])
+def test_quad_one_space_object(cube, kernel, op, sp):
+    """One space object on both sides of a symmetric operator: only the regular pairs with
+    test cell >= trial cell are integrated, each also added at the transposed entries."""
+    s = space(cube, sp)
+    a = assembler(kernel, op, 2.0, quad_options()).assemble(s, s)
+    o = oracle_quad(cube, kernel, op, 2.0, test=sp, trial=sp)
     assert rel_err(a, o) <= FP64_TOL
 
 
