@@ -250,6 +250,9 @@ struct BoundaryAssemblerT {
   // host copy threads, ms of destination page prefaulting, device ms to the end of the
   // last chunk's kernels and to the end of the last DMA (page-locked destinations)
   std::array<double, 8> host_copy_stats{};
+  // the last assembly's regular launches covered the tile pairs tx >= sy only (a chunk's
+  // work then falls with its index)
+  bool tx_ge_sy = false;
   cudaEvent_t copy_timing[3] = {nullptr, nullptr, nullptr};  // start, compute end, DMA end
   DeviceBuffer convert;  // FP64 staging for F32 / C32 outputs
   DeviceBuffer pair_values;

@@ -24,6 +24,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
+#include <iterator>
 #include <thread>
 
 #include "core.h"
@@ -36,6 +37,7 @@ constexpr size_t kSlotBytes = size_t(64) << 20;
 constexpr size_t kChunkTargetBytes = size_t(48) << 20;  // device bytes per chunk (about)
 constexpr int kMaxChunks = 16;
 constexpr int64_t kMergeGap = 2;  // columns between two runs still copied as one DMA
+constexpr int64_t kMinRun = 16;   // shortest run of finished columns a tx >= sy chunk copies
 
 // Persistent pool running one parallel job at a time.
 class CopyPool {
@@ -137,6 +139,58 @@ struct Group {
   std::vector<Piece> pieces;
   size_t bytes = 0;
 };
+
+// The DMAs of each chunk into a page-locked destination, as (first column, columns).
+// Full tile grid (every chunk the same work): the runs of columns the chunk completes,
+// merged across gaps of at most kMergeGap columns (a gap column that is not final yet is
+// copied again by a later DMA on the same stream, which lands after this one; a final one
+// is copied twice with the same values), fewer, larger copies for ~17 % more bytes.
+// Tile pairs tx >= sy only (symmetric operators on one space): the first chunks hold
+// most of the work, so the copy stream has time to spare early and none late.  Only
+// finished columns are copied, and a run shorter than kMinRun columns waits for a later
+// chunk, where the columns beside it may have joined it (the last chunk takes the rest).
+ColumnRuns copy_plan(const ColumnRuns& runs, bool triangular) {
+  const int n = static_cast<int>(runs.size());
+  ColumnRuns plan(n);
+  if (!triangular) {
+    for (int c = 0; c < n; ++c) {
+      const auto& rc = runs[c];
+      for (size_t r = 0; r < rc.size();) {
+        const int64_t first = rc[r].first;
+        int64_t end = rc[r].first + rc[r].second;
+        size_t q = r + 1;
+        while (q < rc.size() && rc[q].first >= end && rc[q].first - end <= kMergeGap) {
+          end = rc[q].first + rc[q].second;
+          ++q;
+        }
+        plan[c].push_back({first, end - first});
+        r = q;
+      }
+    }
+    return plan;
+  }
+  std::vector<std::pair<int64_t, int64_t>> pending, all;
+  for (int c = 0; c < n; ++c) {
+    // the chunks' runs are disjoint: merge the deferred ones with this chunk's, joining
+    // runs that touch
+    all.clear();
+    std::merge(pending.begin(), pending.end(), runs[c].begin(), runs[c].end(),
+               std::back_inserter(all));
+    pending.clear();
+    for (size_t r = 0; r < all.size();) {
+      const int64_t first = all[r].first;
+      int64_t end = first + all[r].second;
+      size_t q = r + 1;
+      while (q < all.size() && all[q].first == end) end += all[q++].second;
+      if (end - first >= kMinRun || c + 1 == n)
+        plan[c].push_back({first, end - first});
+      else
+        pending.push_back({first, end - first});
+      r = q;
+    }
+  }
+  return plan;
+}
 
 std::vector<Group> plan_groups(const ColumnRuns& runs, size_t col_bytes) {
   std::vector<Group> groups;
@@ -312,28 +366,16 @@ void assemble_host(BoundaryAssemblerT& a, SpaceT& trial, SpaceT& test, void* dat
     BEMPP_CUDA(cudaEventRecord(a.copy_timing[1], a.stream));
     const char* src = static_cast<const char*>(a.work.ptr);
     size_t ncopies = 0;
-    // Runs of a chunk whose gap is at most kMergeGap columns go in one DMA: a gap column
-    // that is not final yet is copied again by a later chunk's DMA on the same stream
-    // (which lands after this one), one already final is copied twice with the same
-    // values.  Fewer, larger copies for ~17 % more bytes (P1 columns finish in short,
-    // scattered runs).
+    // P1 columns finish in short, scattered runs (copy_plan)
+    const ColumnRuns plan = copy_plan(runs, a.tx_ge_sy);
     for (int c = 0; c < nchunks; ++c) {
       BEMPP_CUDA(cudaStreamWaitEvent(a.copy_stream, a.chunk_ev[c], 0));
-      const auto& rc = runs[c];
-      for (size_t r = 0; r < rc.size();) {
-        const int64_t first = rc[r].first;
-        int64_t end = rc[r].first + rc[r].second;
-        size_t q = r + 1;
-        while (q < rc.size() && rc[q].first >= end && rc[q].first - end <= kMergeGap) {
-          end = rc[q].first + rc[q].second;
-          ++q;
-        }
-        const size_t off = static_cast<size_t>(first) * col_bytes;
+      for (const auto& run : plan[c]) {
+        const size_t off = static_cast<size_t>(run.first) * col_bytes;
         BEMPP_CUDA(cudaMemcpyAsync(static_cast<char*>(data) + off, src + off,
-                                   static_cast<size_t>(end - first) * col_bytes,
+                                   static_cast<size_t>(run.second) * col_bytes,
                                    cudaMemcpyDeviceToHost, a.copy_stream));
         ++ncopies;
-        r = q;
       }
     }
     BEMPP_CUDA(cudaEventRecord(a.copy_timing[2], a.copy_stream));

@@ -36,6 +36,7 @@ def output_memory(request, monkeypatch):
     return request.param
 
 OPS = {"single_layer": OperatorType.SingleLayer, "double_layer": OperatorType.DoubleLayer,
+       "adjoint_double_layer": OperatorType.AdjointDoubleLayer,
        "hypersingular": OperatorType.Hypersingular}
 
 
@@ -45,7 +46,7 @@ def boundary_pinned():
     return boundary.PINNED_OUTPUT_MIN_BYTES is not None
 
 
-def assemble_both(level, kernel, op, k, degree, dtype):
+def assemble_both(level, kernel, op, k, degree, dtype, precision=None):
     import torch
 
     pts, cells = shapes.icosphere(level)
@@ -56,6 +57,8 @@ def assemble_both(level, kernel, op, k, degree, dtype):
     sp = function_space(grid, fam)
     opts = BoundaryAssemblerOptions()
     opts.set_regular_quadrature_degree(ReferenceCellType.Triangle, 6)
+    if precision is not None:
+        opts.set_precision(precision)
     if kernel == "laplace":
         a = create_laplace_assembler(OPS[op], opts, dtype)
     else:
@@ -98,9 +101,24 @@ def test_chunked_p1_matches_device_and_oracle():
     assert rel_err(host[rows], o[rows]) <= 1e-12
 
 
-def test_chunked_p1_helmholtz_hypersingular():
-    # 2562^2 complex128 = 105 MB: 2 chunks
-    _, host, dev = assemble_both(4, "helmholtz", "hypersingular", 5.0, 1, np.complex128)
+@pytest.mark.parametrize("op", ["hypersingular", "double_layer", "adjoint_double_layer"])
+def test_chunked_p1_helmholtz(op):
+    # 2562^2 complex128 = 105 MB: 3 chunks (hypersingular: of tile pairs tx >= sy)
+    _, host, dev = assemble_both(4, "helmholtz", op, 5.0, 1, np.complex128)
+    assert rel_err(host, dev) <= 1e-13
+
+
+@pytest.mark.parametrize("kernel,k", [("laplace", 0.0), ("helmholtz", 5.0)])
+def test_chunked_p1_mixed_double_layer(kernel, k):
+    from bempp.assembly.boundary import Precision
+
+    dtype = np.float64 if kernel == "laplace" else np.complex128
+    _, host, dev = assemble_both(4, kernel, "double_layer", k, 1, dtype, Precision.Mixed)
+    assert rel_err(host, dev) <= 1e-12
+
+
+def test_chunked_p1_laplace_adjoint_double_layer():
+    _, host, dev = assemble_both(5, "laplace", "adjoint_double_layer", 0.0, 1, np.float64)
     assert rel_err(host, dev) <= 1e-13
 
 
