@@ -18,6 +18,7 @@ against the reference runs unchanged.  Beyond the reference:
 from __future__ import annotations
 
 import typing
+import weakref
 from enum import Enum
 
 import numpy as np
@@ -133,11 +134,9 @@ class BoundaryAssemblerOptions(object):
     def __init__(self):
         self._read_only = False
         self._rs_options = _lib.boundary_assembler_options_new()
-
-    def __del__(self):
-        if getattr(self, "_rs_options", None) is not None:
-            _lib.boundary_assembler_options_t_free(self._rs_options)
-            self._rs_options = None
+        # freed when the object goes, or at interpreter exit while the library is still
+        # loaded
+        weakref.finalize(self, _lib.boundary_assembler_options_t_free, self._rs_options)
 
     def set_regular_quadrature_degree(self, cell: ReferenceCellType, degree: int):
         """Number of points of the rule used on well-separated cell pairs of this cell
@@ -218,11 +217,8 @@ class BoundaryAssembler(object):
         self.options = options
         self.options._read_only = True
         self._rs_assembler = rs_assembler
-        self._owned = owned
-
-    def __del__(self):
-        if getattr(self, "_owned", False):
-            _lib.boundary_assembler_t_free(self._rs_assembler)
+        if owned:
+            weakref.finalize(self, _lib.boundary_assembler_t_free, rs_assembler)
 
     def _check_spaces(self, trial_space: FunctionSpace, test_space: FunctionSpace):
         ok = (trial_space.dtype, test_space.dtype)

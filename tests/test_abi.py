@@ -511,3 +511,36 @@ def test_p2_ndgrid_edge_numbering_is_kept():
         dofs = sp.cell_dofs(c)
         for i in range(3):
             assert sp.get_local_dof_numbers(1, int(t["cell_edges"][c, i])) == [dofs[3 + i]]
+
+
+def test_handles_alive_at_interpreter_exit_are_freed_quietly():
+    """Options, assemblers, grids and spaces still referenced by module globals at exit
+    are released by their finalizers while the library is still loaded."""
+    import subprocess
+    import sys
+
+    pkg = os.path.dirname(os.path.dirname(_lib.__file__))
+    # with torch loaded, the interpreter tears the modules down in an order in which a
+    # __del__ running late finds cffi's function lookup already gone
+    code = (
+        "import numpy as np\n"
+        "import torch\n"
+        "from bempp import shapes\n"
+        "from bempp.assembly.boundary import (BoundaryAssemblerOptions, OperatorType,\n"
+        "                                     create_laplace_assembler)\n"
+        "from bempp.function_space import function_space\n"
+        "from ndelement.ciarlet import Continuity, Family, create_family\n"
+        "from ndgrid.grid import Grid\n"
+        "opts = BoundaryAssemblerOptions()\n"
+        "asm = create_laplace_assembler(OperatorType.SingleLayer, opts, np.float64)\n"
+        "pts, cells = shapes.icosphere(1)\n"
+        "grid = Grid(pts, cells)\n"
+        "space = function_space(grid, create_family(Family.Lagrange, 1, Continuity.Standard,\n"
+        "                                           np.float64))\n"
+        "print(space.global_size)\n")
+    env = dict(os.environ, PYTHONPATH=pkg)
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip() == "42"
+    assert "Exception ignored" not in r.stderr, r.stderr
