@@ -8,15 +8,17 @@ radial perturbation U(-0.02, 0.02) (numpy default_rng(20480)); regular pairs use
 10,242 x 10,242 matrices (314.7 M entries).  The metric is dense entries per second.
 
 Other workloads: ``helmholtz_sl`` (Helmholtz single layer, k = 8, DP0, complex128, same
-perturbed 20,480-triangle sphere, 419 M entries) and ``laplace_sl`` (Laplace single layer,
-DP0, f64, 1,280-triangle icosphere).  The default run also measures the Helmholtz
+perturbed 20,480-triangle sphere, 419 M entries), ``helmholtz_p1`` (Helmholtz double
+layer, adjoint double layer and hypersingular, k = 8, P1, complex128, same sphere) and
+``laplace_sl`` (Laplace single layer, DP0, f64, 1,280-triangle icosphere).  The default run also measures the Helmholtz
 single-layer FP64 and mixed-precision assemblies and reports their speed ratio and the
 mixed result's relative Frobenius error against the FP64 result (``helmholtz_sl_fp64_vs_mixed``
 key, with the Helmholtz DL / ADL / HS P1 operators), the adjoint gradient against one
 forward assembly (``adjoint``) and the batched wavenumber sweep (``sweep``).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload p1|helmholtz_sl|laplace_sl] [--precision fp64|mixed]
+                  [--workload p1|helmholtz_sl|helmholtz_p1|laplace_sl]
+                  [--precision fp64|mixed]
                   [--level L] [--once]
 
 value: device-resident assembly (geometry cached, output in HBM), max over ranks.
@@ -81,6 +83,11 @@ WORKLOADS = {
                          level=5, perturb=True, k=8.0, ops=["single_layer"],
                          metric="dense entries/s (Helmholtz SL k=8, DP0, c128, 20480-triangle "
                                 "icosphere)"),
+    "helmholtz_p1": dict(name="helmholtz_dl_adl_hs_p1_ico5_k8_c128", kernel="helmholtz",
+                         space="p1", level=5, perturb=True, k=8.0,
+                         ops=["double_layer", "adjoint_double_layer", "hypersingular"],
+                         metric="dense entries/s (Helmholtz DL+ADL+HS k=8, P1, c128, "
+                                "20480-triangle icosphere)"),
     "laplace_sl": dict(name="laplace_sl_dp0_ico3_f64", kernel="laplace", space="dp0", level=3,
                        perturb=False, k=0.0, ops=["single_layer"],
                        metric="dense entries/s (Laplace SL, DP0, f64, 1280-triangle icosphere)"),
