@@ -498,8 +498,7 @@ size_t space_get_local_dof_numbers_size(SpaceT* s, size_t dim, size_t entity) {
 
 void space_get_local_dof_numbers(SpaceT* s, size_t dim, size_t entity, uintptr_t* dofs) {
   if (!s || !dofs || dim > 2 || entity >= s->entity_dofs[dim].size()) return;
-  const auto& v = s->entity_dofs[dim][entity];
-  for (size_t i = 0; i < v.size(); ++i) dofs[i] = static_cast<uintptr_t>(v[i]);
+  for (int64_t d : s->entity_dofs[dim][entity]) *dofs++ = static_cast<uintptr_t>(d);
 }
 
 size_t space_local_size(SpaceT* s) { return s ? static_cast<size_t>(s->ndofs) : 0; }

@@ -144,6 +144,23 @@ struct SingularPairList {
   bool uploaded = false;
 };
 
+// Rows of varying length in two flat arrays: row r is items[off[r] .. off[r + 1]).
+template <typename T>
+struct Rows {
+  std::vector<int64_t> off{0};
+  std::vector<T> items;
+  struct View {
+    const T* b;
+    const T* e;
+    const T* begin() const { return b; }
+    const T* end() const { return e; }
+    size_t size() const { return static_cast<size_t>(e - b); }
+  };
+  size_t size() const { return off.size() - 1; }
+  View operator[](size_t r) const { return {items.data() + off[r], items.data() + off[r + 1]}; }
+  bool empty() const { return off.size() == 1; }
+};
+
 }  // namespace bempp_b200
 
 // Handle types of the C-ABI (declared opaque in include/bempp_b200.h).
@@ -165,14 +182,14 @@ struct GridT {
   std::vector<int> topo;
   int64_t nvertices = 0;
   // ndgrid's cell -> edge connectivity (local edge i opposite local vertex i) and edge ->
-  // vertex connectivity, when given; build_topology then keeps ndgrid's edge numbering
+  // vertex connectivity, when given; build_edges then keeps ndgrid's edge numbering
   // (triangles; quadrilateral grids keep no edges, their spaces have no edge DOFs).
   std::vector<int> given_cell_edges;    // ncells x 3
   std::vector<int> given_edge_vertices; // nedges x 2
   const int* vtx() const { return topo.empty() ? cells.data() : topo.data(); }
   int64_t nverts() const { return topo.empty() ? npoints : nvertices; }
   uint8_t dtype = 1;
-  std::vector<std::vector<int>> vertex_cells;  // upward connectivity, increasing cell index
+  bempp_b200::Rows<int> vertex_cells;  // upward connectivity, increasing cell index
   std::vector<std::pair<int, int>> edges;      // unique edges (v0 < v1)
   std::vector<std::array<int, 3>> cell_edges;  // local edge i opposite local vertex i
   int device = -1;
@@ -186,7 +203,8 @@ struct GridT {
   // near fields with other grids (and itself), keyed by the trial grid's uid
   std::map<uint64_t, std::unique_ptr<bempp_b200::NearField>> near_fields;
   std::mutex mu;
-  void build_topology();
+  void build_topology();  // vertex_cells
+  void build_edges();     // edges and cell_edges (triangles)
   double max_circumradius();
 };
 
@@ -204,7 +222,7 @@ struct SpaceT {
   int nbasis = 1;
   int64_t ndofs = 0;
   std::vector<int64_t> cell_dofs;                  // ncells x nbasis
-  std::vector<std::vector<int64_t>> entity_dofs[3];  // [dim][entity] -> dofs
+  bempp_b200::Rows<int64_t> entity_dofs[3];  // [dim][entity] -> dofs
   // device mirrors
   int device = -1;
   DeviceBuffer d_dofs;                                   // int32 ncells x nbasis

@@ -24,10 +24,22 @@ void GridT::build_topology() {
   if (!vertex_cells.empty() || ncells == 0) return;
   const int* vx = vtx();
   const int n = nv();
-  vertex_cells.assign(nverts(), {});
+  // counts, offsets, then the cells in increasing order
+  auto& off = vertex_cells.off;
+  off.assign(static_cast<size_t>(nverts()) + 1, 0);
+  for (int64_t i = 0; i < n * ncells; ++i) ++off[vx[i] + 1];
+  for (size_t v = 1; v < off.size(); ++v) off[v] += off[v - 1];
+  vertex_cells.items.resize(static_cast<size_t>(n * ncells));
+  std::vector<int64_t> next(off.begin(), off.end() - 1);
   for (int64_t c = 0; c < ncells; ++c)
-    for (int i = 0; i < n; ++i) vertex_cells[vx[n * c + i]].push_back(static_cast<int>(c));
-  if (quads()) return;  // quadrilateral spaces (degree <= 1) have no edge DOFs
+    for (int i = 0; i < n; ++i) vertex_cells.items[next[vx[n * c + i]]++] = static_cast<int>(c);
+}
+
+// Edges of a triangle grid, built for the spaces with edge DOFs (degree 2) only; the
+// quadrilateral spaces (degree <= 1) have none.
+void GridT::build_edges() {
+  if (!cell_edges.empty() || ncells == 0 || quads()) return;
+  const int* vx = vtx();
   if (!given_cell_edges.empty()) {
     // ndgrid's own edge numbering (validated when the grid was created)
     const int64_t ne = static_cast<int64_t>(given_edge_vertices.size() / 2);
@@ -73,15 +85,18 @@ SpaceT* make_space(GridT* grid, const ElementFamilyT& fam) {
   if (grid->quads() && fam.degree > 1)
     throw Error(kUnsupported, "quadrilateral grids: Lagrange degree 0 and 1 spaces only");
   grid->build_topology();
+  if (fam.degree == 2) grid->build_edges();
   auto* s = new SpaceT();
   s->grid = grid;
   s->degree = fam.degree;
   s->continuous = fam.continuity == 0 && fam.degree >= 1;
   s->dtype = fam.dtype;
   const int64_t nc = grid->ncells;
-  s->entity_dofs[0].assign(grid->nverts(), {});
-  s->entity_dofs[1].assign(grid->edges.size(), {});
-  s->entity_dofs[2].assign(nc, {});
+  // DOF of each vertex and edge (-1: none yet); a cell's interior DOFs are
+  // [per_cell * c, per_cell * (c + 1))
+  std::vector<int64_t> vdof(static_cast<size_t>(grid->nverts()), -1),
+      edof(grid->edges.size(), -1);
+  int per_cell = 0;
   if (grid->quads() && fam.degree == 1) {
     // Q1 (one DOF per vertex, first visit) or DQ1 (four interior DOFs per cell)
     s->nbasis = 4;
@@ -90,23 +105,21 @@ SpaceT* make_space(GridT* grid, const ElementFamilyT& fam) {
     for (int64_t c = 0; c < nc; ++c)
       for (int i = 0; i < 4; ++i) {
         if (s->continuous) {
-          auto& ed = s->entity_dofs[0][grid->vtx()[4 * c + i]];
-          if (ed.empty()) ed.push_back(size++);
-          s->cell_dofs[4 * c + i] = ed[0];
+          int64_t& d = vdof[grid->vtx()[4 * c + i]];
+          if (d < 0) d = size++;
+          s->cell_dofs[4 * c + i] = d;
         } else {
-          s->cell_dofs[4 * c + i] = size;
-          s->entity_dofs[2][c].push_back(size++);
+          s->cell_dofs[4 * c + i] = size++;
         }
       }
+    if (!s->continuous) per_cell = 4;
     s->ndofs = size;
   } else if (fam.degree == 0) {
     // DP0: one DOF on the cell itself (Lagrange degree 0 is discontinuous)
     s->nbasis = 1;
     s->cell_dofs.resize(nc);
-    for (int64_t c = 0; c < nc; ++c) {
-      s->cell_dofs[c] = c;
-      s->entity_dofs[2][c] = {c};
-    }
+    for (int64_t c = 0; c < nc; ++c) s->cell_dofs[c] = c;
+    per_cell = 1;
     s->ndofs = nc;
   } else if (fam.degree == 1 && s->continuous) {
     s->nbasis = 3;
@@ -114,9 +127,9 @@ SpaceT* make_space(GridT* grid, const ElementFamilyT& fam) {
     int64_t size = 0;
     for (int64_t c = 0; c < nc; ++c)
       for (int i = 0; i < 3; ++i) {
-        auto& ed = s->entity_dofs[0][grid->vtx()[3 * c + i]];
-        if (ed.empty()) ed.push_back(size++);
-        s->cell_dofs[3 * c + i] = ed[0];
+        int64_t& d = vdof[grid->vtx()[3 * c + i]];
+        if (d < 0) d = size++;
+        s->cell_dofs[3 * c + i] = d;
       }
     s->ndofs = size;
   } else if (fam.degree == 2 && s->continuous) {
@@ -127,14 +140,14 @@ SpaceT* make_space(GridT* grid, const ElementFamilyT& fam) {
     int64_t size = 0;
     for (int64_t c = 0; c < nc; ++c) {
       for (int i = 0; i < 3; ++i) {
-        auto& ed = s->entity_dofs[0][grid->vtx()[3 * c + i]];
-        if (ed.empty()) ed.push_back(size++);
-        s->cell_dofs[6 * c + i] = ed[0];
+        int64_t& d = vdof[grid->vtx()[3 * c + i]];
+        if (d < 0) d = size++;
+        s->cell_dofs[6 * c + i] = d;
       }
       for (int i = 0; i < 3; ++i) {
-        auto& ed = s->entity_dofs[1][grid->cell_edges[c][i]];
-        if (ed.empty()) ed.push_back(size++);
-        s->cell_dofs[6 * c + 3 + i] = ed[0];
+        int64_t& d = edof[grid->cell_edges[c][i]];
+        if (d < 0) d = size++;
+        s->cell_dofs[6 * c + 3 + i] = d;
       }
     }
     s->ndofs = size;
@@ -143,14 +156,25 @@ SpaceT* make_space(GridT* grid, const ElementFamilyT& fam) {
     const int nb = fam.degree == 1 ? 3 : 6;
     s->nbasis = nb;
     s->cell_dofs.resize(nb * nc);
-    for (int64_t c = 0; c < nc; ++c) {
-      for (int i = 0; i < nb; ++i) {
-        s->cell_dofs[nb * c + i] = nb * c + i;
-        s->entity_dofs[2][c].push_back(nb * c + i);
-      }
-    }
+    for (int64_t i = 0; i < nb * nc; ++i) s->cell_dofs[i] = i;
+    per_cell = nb;
     s->ndofs = nb * nc;
   }
+  // entity -> DOFs rows: vertices and edges hold at most one DOF each
+  for (int dim = 0; dim < 2; ++dim) {
+    const std::vector<int64_t>& one = dim == 0 ? vdof : edof;
+    auto& r = s->entity_dofs[dim];
+    r.off.assign(one.size() + 1, 0);
+    for (size_t e = 0; e < one.size(); ++e) r.off[e + 1] = r.off[e] + (one[e] >= 0 ? 1 : 0);
+    r.items.reserve(static_cast<size_t>(r.off.back()));
+    for (int64_t d : one)
+      if (d >= 0) r.items.push_back(d);
+  }
+  auto& rc = s->entity_dofs[2];
+  rc.off.resize(static_cast<size_t>(nc) + 1);
+  for (int64_t c = 0; c <= nc; ++c) rc.off[c] = per_cell * c;
+  rc.items.resize(static_cast<size_t>(per_cell * nc));
+  for (int64_t i = 0; i < per_cell * nc; ++i) rc.items[i] = i;
   return s;
 }
 
