@@ -996,11 +996,14 @@ enum NearMode : int { kNearInKernel = 0, kNearMasked = 1 };
 // Resident CTAs per SM the register allocation must allow: 5 for the FP64 Laplace
 // hypersingular kernel (it fits in 96 registers without spills), 6 for the mixed
 // Helmholtz DP0 kernels (80 registers; with no FP64 points in their tiles six CTAs also
-// fit in shared memory), 4 elsewhere (the paired double layer too: at 128 registers it
-// spills 48 bytes).
+// fit in shared memory), 3 for the paired FP64 Helmholtz double layer (168 registers; at
+// 128 it spills 228 bytes, and four CTAs per SM ran 17 % slower), 4 elsewhere (the paired
+// Laplace double layer too: at 128 registers it spills 48 bytes; the paired mixed
+// Helmholtz one, which stages the real and imaginary parts of its blocks in turn to fit
+// four CTAs in shared memory, needs 127 registers without spills).
 template <int KER, int OP, bool MIXED, bool DIRECT, bool PAIRED = false>
 constexpr int min_ctas() {
-  return (PAIRED && KER == kHelmholtz)             ? 3
+  return (PAIRED && KER == kHelmholtz && !MIXED)   ? 3
          : (KER == kLaplace && OP == kHS && !MIXED) ? 5
          : (MIXED && DIRECT && KER == kHelmholtz)   ? 6
                                                     : 4;
@@ -1029,6 +1032,9 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAI
   // summed per test DOF (lane = DOF) before the accumulator, so that no two lanes of a
   // warp update the same entry (test cells share vertex DOFs)
   constexpr bool kGather = !DIRECT && NBT == 3;
+  // complex blocks gathered through one real stage, real parts first (paired mixed
+  // Helmholtz: four CTAs per SM fit in shared memory)
+  constexpr bool kSplitStage = kGather && kC && PAIRED && MIXED;
   // real FP64 P1 blocks (not the hypersingular kernel, which keeps 5 CTAs per SM; not the
   // mixed kernels, whose larger tiles would then limit the CTAs per SM): one accumulator
   // per warp, updated with plain adds, summed at the flush
@@ -1081,7 +1087,7 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAI
     constexpr int kStage = kWarps * kTile * NBT * NBS;
     stage_re = reinterpret_cast<double*>(cursor);
     stage_im = stage_re + kStage;
-    cursor += sizeof(double) * kStage * (kC ? 2 : 1);
+    cursor += sizeof(double) * kStage * ((kC && !kSplitStage) ? 2 : 1);
     inc_off = cursor;
     inc_ent = cursor + 3 * kTile + 1;
     cursor += 6 * kTile + 1;
@@ -1211,19 +1217,24 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAI
         }
       }
     }
-    // PAIRED off the diagonal: a second pass gathers the (sy, tx) blocks into acc_t
+    // PAIRED off the diagonal: a second block gathers the (sy, tx) blocks into acc_t;
+    // kSplitStage: each block in two passes, real then imaginary parts
+    constexpr int kParts = kSplitStage ? 2 : 1;
 #pragma unroll 1
-    for (int pass = 0; pass < ((PAIRED && mirror) ? 2 : (kGather ? 1 : 0)); ++pass) {
+    for (int pass = 0; pass < ((PAIRED && mirror) ? 2 : (kGather ? 1 : 0)) * kParts; ++pass) {
+      const int blk = pass / kParts, part = pass % kParts;
       double* sr = stage_re + warp * (kTile * NBT * NBS);
       double* si = stage_im + warp * (kTile * NBT * NBS);
-      double* acc = pass == 0 ? acc_re : acc_t;
-      double* acci = pass == 0 ? acc_im : acc_t + cap;
+      double* acc = blk == 0 ? (part == 0 ? acc_re : acc_im) : (part == 0 ? acc_t : acc_t + cap);
+      double* acci = blk == 0 ? acc_im : acc_t + cap;
 #pragma unroll
       for (int a = 0; a < NBT; ++a)
 #pragma unroll
         for (int b = 0; b < NBS; ++b) {
-          sr[(a * NBS + b) * kTile + it] = have ? (pass == 0 ? ore[a][b] : otr[a][b]) : 0.0;
-          if (kC) si[(a * NBS + b) * kTile + it] = have ? (pass == 0 ? oim[a][b] : oti[a][b]) : 0.0;
+          const double re = blk == 0 ? ore[a][b] : otr[a][b];
+          const double im = blk == 0 ? oim[a][b] : oti[a][b];
+          sr[(a * NBS + b) * kTile + it] = have ? (part == 0 ? re : im) : 0.0;
+          if (kC && !kSplitStage) si[(a * NBS + b) * kTile + it] = have ? im : 0.0;
         }
       __syncwarp();
       for (int d = it; d < ndt; d += kTile) {
@@ -1236,7 +1247,7 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAI
 #pragma unroll
           for (int b = 0; b < NBS; ++b) {
             g_re[b] += sr[(a * NBS + b) * kTile + c];
-            if (kC) g_im[b] += si[(a * NBS + b) * kTile + c];
+            if (kC && !kSplitStage) g_im[b] += si[(a * NBS + b) * kTile + c];
           }
         }
 #pragma unroll
@@ -1246,7 +1257,7 @@ __global__ void __launch_bounds__(kThreads, min_ctas<KER, OP, MIXED, DIRECT, PAI
             acc[warp * cap + idx] += g_re[b];  // this warp's copy; distinct per lane
           } else {
             atomicAdd(acc + idx, g_re[b]);
-            if (kC) atomicAdd(acci + idx, g_im[b]);
+            if (kC && !kSplitStage) atomicAdd(acci + idx, g_im[b]);
           }
         }
       }
@@ -1646,12 +1657,13 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 size_t smem_bytes(int q, bool rel, bool queue, bool direct, bool cplx, int max_t, int max_s,
-                  int nbt, int nbs, int acc_copies, bool mirror, bool pts) {
+                  int nbt, int nbs, int acc_copies, bool mirror, bool pts, bool split_stage) {
   size_t b = 16;  // the mbarrier
   if (!direct) b += sizeof(double) * static_cast<size_t>(max_t) * max_s * (cplx ? 2 : 1) * acc_copies;
   if (direct && mirror) b += sizeof(double) * kTile * (kTile + 1) * (cplx ? 2 : 1) + 16;
   if (!direct && nbt == 3)  // stage and DOF incidence of the gather
-    b += sizeof(double) * kWarps * kTile * nbt * nbs * (cplx ? 2 : 1) + 6 * kTile + 1;
+    b += sizeof(double) * kWarps * kTile * nbt * nbs * ((cplx && !split_stage) ? 2 : 1) +
+         6 * kTile + 1;
   for (int nb : {nbt, nbs}) {
     b = (b + 15) & ~size_t(15);
     b += sizeof(double) * tile_doubles(q, pts) + sizeof(float) * tile_floats(q, rel) +
@@ -1676,7 +1688,8 @@ cudaError_t launch_mode(const CellSet& test, const SpaceTiles& tt, const CellSet
   auto bytes = [&](int copies) {
     return smem_bytes(rule.npts, MIXED, MIXED && NM == kNearInKernel, DIRECT, KER == kHelmholtz,
                       tt.max_tile_dofs, st.max_tile_dofs, NBT, NBS, copies, a.symmetric != 0,
-                      !MIXED || NM == kNearInKernel);
+                      !MIXED || NM == kNearInKernel,
+                      !DIRECT && NBT == 3 && KER == kHelmholtz && PAIRED && MIXED);
   };
   int copies = kAcc;
   size_t smem = bytes(copies);
