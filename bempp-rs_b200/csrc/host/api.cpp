@@ -766,6 +766,7 @@ BemppStatus bempp_helmholtz_single_layer_dp0_gradient(GridT* grid,
     d_grad.alloc(sizeof(double) * 3 * np);
     BEMPP_CUDA(cudaMemcpy(d_lam.ptr, lambda, 16 * nc, cudaMemcpyHostToDevice));
     BEMPP_CUDA(cudaMemcpy(d_mu.ptr, mu, 16 * nc, cudaMemcpyHostToDevice));
+    BEMPP_CUDA(cudaStreamSynchronize(cudaStreamLegacy));  // the pageable copies have landed
     helmholtz_sl_gradient_device(*grid, options->options, k, d_lam.as<double>(),
                                  d_mu.as<double>(), d_out.as<double>(), d_grad.as<double>(),
                                  nullptr);

@@ -80,10 +80,16 @@ struct DeviceBuffer {
   T* as() const {
     return static_cast<T*>(ptr);
   }
+  // A copy from pageable host memory may return once the data is staged, before the DMA
+  // into the buffer has finished, and the legacy default stream it runs on does not order
+  // the library's non-blocking streams: wait for it, so that no kernel reads the buffer
+  // (possibly a recycled cache block holding older data) before the copy has landed.
   template <typename T>
   void upload(const std::vector<T>& v) {
     alloc(v.size() * sizeof(T));
-    if (!v.empty()) BEMPP_CUDA(cudaMemcpy(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    if (v.empty()) return;
+    BEMPP_CUDA(cudaMemcpy(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    BEMPP_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
   }
 };
 
